@@ -1,0 +1,805 @@
+// host.cpp -- C ABI, setup and quartet planning of the B200 Fock-build engine.
+//
+// Mirrors libERI's handle API (src/interface/liberi_interface.F90) and GAMESS
+// wrapper (src/interface/gms_liberi_wrapper.F90).  Setup restates the
+// reference's shell classification and pair classes
+// (src/liberi_shell_pair.F90:39-1283) and its per-kernel screening
+// (src/rhf/rot_axis/int*.F90 headers), then stores a device-resident plan per
+// kernel class: bra pairs sorted by Schwarz value, for each bra the number of
+// surviving kets, which form a prefix of the Schwarz-sorted ket list.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/liberi_b200.h"
+#include "engine.h"
+
+namespace liberi {
+
+// Driver order and per-kernel screening (src/liberi_driver.F90:69-102):
+// pre-screen (cross: int0001.F90:67-84; own: int2211_rysgen.F90:295-310),
+// product operator (int0000.F90:106-107 ">=", int0001.F90:120-121 ">",
+// int2222_rysgen.F90:428-436 none), tiles (int0000.F90:76-81 sqrt(3.75e9),
+// int0001.F90:90 3.75e9, int0002.F90:84 3.75e8), flat order
+// (int0001.F90:117 bra-major, int2211_rysgen.F90:351 bra-fastest), digestion
+// cut (cutoff_schwarz int0000.F90:246, literal 5e-11 int0002.F90:403) and
+// asymptotic thresholds (t_max=25, Rys 43/49/55).
+const KernelDesc KDESC[NKERN] = {
+    {"int0000", SS, SS, true, false, false, OP_GE, TILE_SQRT, false, true, 25.0, 0, 0, 0, 0},
+    {"int0001", SS, SP, false, false, true, OP_GT, TILE_E9, false, true, 25.0, 0, 0, 1, 0},
+    {"int0011", SS, PP, false, false, true, OP_GT, TILE_E9, false, true, 25.0, 0, 0, 1, 1},
+    {"int0111", SP, PP, false, false, true, OP_GT, TILE_E9, false, false, 25.0, 1, 0, 1, 1},
+    {"int0101", SP, SP, true, false, false, OP_GE, TILE_NONE, false, false, 25.0, 1, 0, 1, 0},
+    {"int1111", PP, PP, true, false, false, OP_GE, TILE_NONE, false, true, 25.0, 1, 1, 1, 1},
+    {"int0002", SS, SD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 0, 0, 2, 0},
+    {"int0012", SS, PD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 0, 0, 2, 1},
+    {"int0102", SP, SD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 1, 0, 2, 0},
+    {"int0112", SP, PD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 1, 0, 2, 1},
+    {"int0022", SS, DD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 0, 0, 2, 2},
+    {"int0122", SP, DD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 1, 0, 2, 2},
+    {"int1102", PP, SD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 1, 1, 2, 0},
+    {"int0202", SD, SD, true, false, false, OP_GT, TILE_NONE, false, false, 25.0, 2, 0, 2, 0},
+    {"int2211", DD, PP, false, true, false, OP_GT, TILE_E8, true, false, 49.0, 2, 2, 1, 1},
+    {"int2121", PD, PD, true, true, false, OP_GT, TILE_NONE, false, false, 49.0, 2, 1, 2, 1},
+    {"int2120", PD, SD, false, true, false, OP_GT, TILE_E8, true, false, 43.0, 2, 1, 2, 0},
+    {"int2111", PD, PP, false, true, false, OP_GT, TILE_E8, true, false, 43.0, 2, 1, 1, 1},
+    {"int2220", DD, SD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, 2, 2, 2, 0},
+    {"int2221", DD, PD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, 2, 2, 2, 1},
+    {"int2222", DD, DD, true, true, false, OP_NONE, TILE_NONE, false, false, 55.0, 2, 2, 2, 2},
+};
+
+static const int PC_L1[NPC] = {0, 0, 1, 0, 1, 2};  // reference pair order (first, second)
+static const int PC_L2[NPC] = {0, 1, 1, 2, 2, 2};
+static const double CUX = 50.0;                    // src/liberi_parameters.F90:44
+static const double SQRT_TWOPI52 = 5.9149671727956128778;  // sqrt(2 pi^(5/2))
+
+}  // namespace liberi
+
+using namespace liberi;
+
+// ---- error handling -------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? LIBERI_E_NOMEM : LIBERI_E_DEVICE, \
+                        "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+// ---- handle ------------------------------------------------------------------------
+struct liberi_handle_s {
+    // options (defaults reproduce the reference constants)
+    double schwarz_cut = 5.00000000000000018e-11;  // liberi_parameters.F90:38
+    double eri_cut = 5.0e-11;
+    double fp32_cut = 1.0e-7;
+    int precision = 0;
+    int device = 0;
+    uint32_t class_mask = (1u << NKERN) - 1;
+    bool timing = false;
+    cudaEvent_t ev[NKERN + 1][2] = {};
+    bool ev_recorded[NKERN] = {};
+    bool plan_dirty = false;
+
+    bool initialized = false;
+    int my_rank = 0, num_procs = 1;
+    BasisHost basis;
+    PairsHost pairs;
+    PlanHost plan[NKERN];
+    DeviceBuffers dev;
+    double *d_tab = nullptr;
+    unsigned long long *d_maxd = nullptr;
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    liberi_stats stats;
+    std::vector<void *> allocs;
+};
+
+template <typename T>
+static cudaError_t dev_upload(liberi_handle h, T **dst, const T *src, size_t n) {
+    *dst = nullptr;
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T));
+    if (e != cudaSuccess) return e;
+    h->allocs.push_back(*dst);
+    h->dev.bytes += n * sizeof(T);
+    return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+template <typename T>
+static cudaError_t dev_alloc(liberi_handle h, T **dst, size_t n) {
+    *dst = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T));
+    if (e != cudaSuccess) return e;
+    h->allocs.push_back(*dst);
+    h->dev.bytes += n * sizeof(T);
+    return cudaSuccess;
+}
+
+static void free_device(liberi_handle h) {
+    for (void *p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    h->dev = DeviceBuffers();
+    h->d_tab = nullptr;
+    h->d_maxd = nullptr;
+    for (int k = 0; k < NKERN; k++) h->plan[k] = PlanHost();
+    if (h->stream) {
+        cudaStreamDestroy(h->stream);
+        h->stream = nullptr;
+    }
+}
+
+// ---- basis validation and pair construction ------------------------------------
+static int validate_basis(const BasisHost &b) {
+    if (b.nsh <= 0 || b.natoms <= 0 || b.num_bas <= 0 || b.mxgtot <= 0)
+        return fail(LIBERI_E_ARG, "liberi_setup: non-positive size (nsh=%d natoms=%d num_bas=%d mxgtot=%d)",
+                    b.nsh, b.natoms, b.num_bas, b.mxgtot);
+    const long long ncoef = (long long)b.nsh * b.mxgtot;
+    for (int s = 0; s < b.nsh; s++) {
+        int l = b.ang_mom[s];
+        if (l == 4) return fail(LIBERI_E_UNSUPPORTED, "liberi_setup: shell %d is an f shell; f classes are not built", s + 1);
+        if (l < 1 || l > 3) return fail(LIBERI_E_ARG, "liberi_setup: ang_mom(%d)=%d out of range", s + 1, l);
+        if (b.contr_num[s] < 1 || b.contr_num[s] > b.mxgtot)
+            return fail(LIBERI_E_ARG, "liberi_setup: contr_num(%d)=%d out of range", s + 1, b.contr_num[s]);
+        if (b.sh_loc[s] < 1 || b.sh_loc[s] - 1 + b.contr_num[s] > ncoef)
+            return fail(LIBERI_E_ARG, "liberi_setup: sh_loc(%d)=%d out of range", s + 1, b.sh_loc[s]);
+        if (b.atom_num[s] < 1 || b.atom_num[s] > b.natoms)
+            return fail(LIBERI_E_ARG, "liberi_setup: atom_num(%d)=%d out of range", s + 1, b.atom_num[s]);
+        int nc = (l == 1) ? 1 : (l == 2 ? 3 : 6);
+        if (b.atom_loc[s] < 1 || b.atom_loc[s] - 1 + nc > b.num_bas)
+            return fail(LIBERI_E_ARG, "liberi_setup: atom_loc(%d)=%d out of range", s + 1, b.atom_loc[s]);
+    }
+    for (double x : b.schwrz)
+        if (!(x >= 0.0)) return fail(LIBERI_E_ARG, "liberi_setup: negative or NaN Schwarz value");
+    return LIBERI_OK;
+}
+
+static void build_pairs(const BasisHost &b, PairsHost &pr, std::vector<double4> &shell_xyz) {
+    shell_xyz.resize(b.nsh);
+    for (int s = 0; s < b.nsh; s++) {
+        int a = b.atom_num[s] - 1;
+        shell_xyz[s] = make_double4(b.coords[3 * a], b.coords[3 * a + 1], b.coords[3 * a + 2], 0.0);
+    }
+    // ascending per-L lists (classify_shells, liberi_shell_pair.F90:301-344)
+    std::vector<int> lst[3];
+    for (int s = 0; s < b.nsh; s++) lst[b.ang_mom[s] - 1].push_back(s);
+    for (int l = 0; l < 3; l++) pr.nl[l] = (int)lst[l].size();
+    const std::vector<double> *coef[3] = {&b.cs, &b.cp, &b.cd};
+    pr = PairsHost{};
+    for (int l = 0; l < 3; l++) pr.nl[l] = (int)lst[l].size();
+    for (int c = 0; c < NPC; c++) {
+        pr.class_off[c] = (int)pr.ish.size();
+        const int l1 = PC_L1[c], l2 = PC_L2[c];
+        const bool same = (l1 == l2);
+        for (size_t ii = 0; ii < lst[l1].size(); ii++) {
+            size_t jmax = same ? ii + 1 : lst[l2].size();
+            for (size_t jj = 0; jj < jmax; jj++) {
+                int is = lst[l1][ii], js = lst[l2][jj];
+                int hi = std::max(is, js) + 1, lo = std::min(is, js) + 1;
+                pr.ish.push_back(is);
+                pr.jsh.push_back(js);
+                pr.xint.push_back(b.schwrz[(size_t)hi * (hi - 1) / 2 + lo - 1]);
+                // engine orientation: higher L first (same L: reference order)
+                int A = is, B = js;
+                if (l2 > l1) std::swap(A, B);
+                pr.shell.push_back(make_int2(A, B));
+                pr.prim0.push_back((int)pr.K.size());
+                double r2 = 0.0;
+                for (int x = 0; x < 3; x++) {
+                    double d = b.coords[3 * (b.atom_num[js] - 1) + x] - b.coords[3 * (b.atom_num[is] - 1) + x];
+                    r2 += d * d;
+                }
+                const double4 RA = shell_xyz[is], RB = shell_xyz[js];
+                int kept = 0;
+                for (int i = 0; i < b.contr_num[is]; i++) {
+                    double a = b.exponents[b.sh_loc[is] - 1 + i];
+                    double ca = (*coef[l1])[b.sh_loc[is] - 1 + i];
+                    for (int j = 0; j < b.contr_num[js]; j++) {
+                        double bb = b.exponents[b.sh_loc[js] - 1 + j];
+                        double cb = (*coef[l2])[b.sh_loc[js] - 1 + j];
+                        double p = a + bb, ip = 1.0 / p;
+                        double mur2 = r2 * (a * ip) * bb;
+                        // mu R^2 > cux pairs are skipped by the reference's
+                        // rotated-axis kernels (int0000.F90:208-210) and
+                        // contribute < e^-50 in its Rys kernels
+                        if (mur2 > CUX) continue;
+                        pr.P.push_back(make_double4((a * RA.x + bb * RB.x) * ip, (a * RA.y + bb * RB.y) * ip,
+                                                    (a * RA.z + bb * RB.z) * ip, p));
+                        pr.K.push_back(SQRT_TWOPI52 * ca * cb * std::exp(-mur2) * ip);
+                        kept++;
+                    }
+                }
+                pr.nprim.push_back(kept);
+            }
+        }
+    }
+    pr.class_off[NPC] = (int)pr.ish.size();
+}
+
+// ---- per-kernel plan ----------------------------------------------------------
+static double class_max(const PairsHost &pr, int c) {
+    double m = -HUGE_VAL;
+    for (int i = pr.class_off[c]; i < pr.class_off[c + 1]; i++) m = std::max(m, pr.xint[i]);
+    return m;
+}
+
+static void build_plan(const PairsHost &pr, int k, double cut, PlanHost &ph) {
+    const KernelDesc &kd = KDESC[k];
+    ph = PlanHost();
+    const int nb_all = pr.class_off[kd.bra + 1] - pr.class_off[kd.bra];
+    const int nk_all = pr.class_off[kd.ket + 1] - pr.class_off[kd.ket];
+    if (nb_all == 0 || nk_all == 0) return;
+    const double sb = cut / class_max(pr, kd.cross ? kd.ket : kd.bra);
+    const double sk = cut / class_max(pr, kd.cross ? kd.bra : kd.ket);
+    std::vector<int> lb, lk;  // compacted lists, reference order (global ids)
+    for (int i = pr.class_off[kd.bra]; i < pr.class_off[kd.bra + 1]; i++)
+        if (pr.xint[i] >= sb) lb.push_back(i);
+    if (kd.tri) lk = lb;
+    else
+        for (int i = pr.class_off[kd.ket]; i < pr.class_off[kd.ket + 1]; i++)
+            if (pr.xint[i] >= sk) lk.push_back(i);
+    if (lb.empty() || lk.empty()) return;
+    ph.nbra_ref = (int)lb.size();
+    ph.nket_ref = (int)lk.size();
+    ph.ntot_ref = kd.tri ? (long long)lb.size() : (long long)lb.size() * (long long)lk.size();
+    auto sorted = [&](const std::vector<int> &l, std::vector<int> &ids, std::vector<int> &orig,
+                      std::vector<double> &x) {
+        std::vector<int> ord(l.size());
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return pr.xint[l[a]] > pr.xint[l[b]]; });
+        for (int o : ord) {
+            ids.push_back(l[o]);
+            orig.push_back(o);
+            x.push_back(pr.xint[l[o]]);
+        }
+    };
+    sorted(lb, ph.bra_ids, ph.bra_orig, ph.bra_x);
+    sorted(lk, ph.ket_ids, ph.ket_orig, ph.ket_x);
+    ph.nbra = (int)ph.bra_ids.size();
+    ph.nket = (int)ph.ket_ids.size();
+    ph.ncount.resize(ph.nbra);
+    ph.pref.assign(ph.nbra + 1, 0);
+    for (int i = 0; i < ph.nbra; i++) {
+        const double xb = ph.bra_x[i];
+        // surviving kets form a prefix of the descending ket list
+        int lo = 0, hi = ph.nket;
+        while (lo < hi) {
+            int mid = (lo + hi) / 2;
+            double t = xb * ph.ket_x[mid];
+            bool pass = kd.op == OP_GE ? (t >= cut) : (kd.op == OP_GT ? (t > cut) : true);
+            if (pass) lo = mid + 1; else hi = mid;
+        }
+        int n = lo;
+        if (kd.tri) n = std::min(n, i + 1);
+        ph.ncount[i] = n;
+        ph.pref[i + 1] = ph.pref[i] + n;
+    }
+    ph.total = ph.pref[ph.nbra];
+}
+
+static int upload_plans(liberi_handle h) {
+    for (int k = 0; k < NKERN; k++) {
+        PlanHost &ph = h->plan[k];
+        if (ph.nbra == 0) continue;
+        CUDA_TRY(dev_upload(h, &ph.d_bra, ph.bra_ids.data(), ph.bra_ids.size()));
+        CUDA_TRY(dev_upload(h, &ph.d_ket, ph.ket_ids.data(), ph.ket_ids.size()));
+        CUDA_TRY(dev_upload(h, &ph.d_bra_orig, ph.bra_orig.data(), ph.bra_orig.size()));
+        CUDA_TRY(dev_upload(h, &ph.d_ket_orig, ph.ket_orig.data(), ph.ket_orig.size()));
+        CUDA_TRY(dev_upload(h, &ph.d_pref, ph.pref.data(), ph.pref.size()));
+        CUDA_TRY(dev_upload(h, &ph.d_bra_x, ph.bra_x.data(), ph.bra_x.size()));
+        CUDA_TRY(dev_upload(h, &ph.d_ket_x, ph.ket_x.data(), ph.ket_x.size()));
+        CUDA_TRY(dev_upload(h, &ph.d_ncount, ph.ncount.data(), ph.ncount.size()));
+        CUDA_TRY(dev_alloc(h, &ph.d_pref64, ph.pref.size()));
+        CUDA_TRY(dev_alloc(h, &ph.d_pref32, ph.pref.size()));
+        CUDA_TRY(dev_alloc(h, &ph.d_split, ph.ncount.size()));
+    }
+    return LIBERI_OK;
+}
+
+static void compute_stats(liberi_handle h) {
+    for (int k = 0; k < NKERN; k++) {
+        const PlanHost &ph = h->plan[k];
+        h->stats.quartets[k] = ph.total;
+        // primitive quartets: sum_i nprim(bra_i) * sum_{j<n_i} nprim(ket_j)
+        std::vector<long long> kp(ph.nket + 1, 0);
+        for (int j = 0; j < ph.nket; j++) kp[j + 1] = kp[j] + h->pairs.nprim[ph.ket_ids[j]];
+        long long s = 0;
+        for (int i = 0; i < ph.nbra; i++) s += (long long)h->pairs.nprim[ph.bra_ids[i]] * kp[ph.ncount[i]];
+        h->stats.prim_quartets[k] = s;
+    }
+}
+
+static int copy_basis(BasisHost &b, int nsh, int natoms, int num_bas, int mxgtot, const int32_t *ang_mom,
+                      const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
+                      const int32_t *atom_loc, const int32_t *start_bas, const int32_t *end_bas,
+                      const double *exponents, const double *cs, const double *cp, const double *cd,
+                      const double *cf, const double *coords, const double *schwrz) {
+    if (nsh <= 0 || natoms <= 0 || num_bas <= 0 || mxgtot <= 0)
+        return fail(LIBERI_E_ARG, "liberi_setup: non-positive size (nsh=%d natoms=%d num_bas=%d mxgtot=%d)",
+                    nsh, natoms, num_bas, mxgtot);
+    if (!ang_mom || !contr_num || !sh_loc || !atom_num || !atom_loc || !exponents || !cs || !cp || !cd ||
+        !coords || !schwrz)
+        return fail(LIBERI_E_ARG, "liberi_setup: null array argument");
+    const size_t ncoef = (size_t)nsh * mxgtot;
+    b.nsh = nsh;
+    b.natoms = natoms;
+    b.num_bas = num_bas;
+    b.mxgtot = mxgtot;
+    b.ang_mom.assign(ang_mom, ang_mom + nsh);
+    b.contr_num.assign(contr_num, contr_num + nsh);
+    b.sh_loc.assign(sh_loc, sh_loc + nsh);
+    b.atom_num.assign(atom_num, atom_num + nsh);
+    b.atom_loc.assign(atom_loc, atom_loc + nsh);
+    if (start_bas) b.start_bas.assign(start_bas, start_bas + nsh);
+    if (end_bas) b.end_bas.assign(end_bas, end_bas + nsh);
+    b.exponents.assign(exponents, exponents + ncoef);
+    b.cs.assign(cs, cs + ncoef);
+    b.cp.assign(cp, cp + ncoef);
+    b.cd.assign(cd, cd + ncoef);
+    if (cf) b.cf.assign(cf, cf + ncoef);
+    b.coords.assign(coords, coords + 3 * (size_t)natoms);
+    b.schwrz.assign(schwrz, schwrz + (size_t)nsh * (nsh + 1) / 2);
+    return LIBERI_OK;
+}
+
+static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) {
+    const BasisHost &b = h->basis;
+    std::vector<int> bf0(b.nsh);
+    for (int s = 0; s < b.nsh; s++) bf0[s] = b.atom_loc[s] - 1;
+    CUDA_TRY(dev_upload(h, &h->dev.shell_xyz, shell_xyz.data(), shell_xyz.size()));
+    CUDA_TRY(dev_upload(h, &h->dev.shell_bf0, bf0.data(), bf0.size()));
+    CUDA_TRY(dev_upload(h, &h->dev.pair_shell, h->pairs.shell.data(), h->pairs.shell.size()));
+    CUDA_TRY(dev_upload(h, &h->dev.pair_prim0, h->pairs.prim0.data(), h->pairs.prim0.size()));
+    CUDA_TRY(dev_upload(h, &h->dev.pair_nprim, h->pairs.nprim.data(), h->pairs.nprim.size()));
+    CUDA_TRY(dev_upload(h, &h->dev.prim_P, h->pairs.P.data(), h->pairs.P.size()));
+    CUDA_TRY(dev_upload(h, &h->dev.prim_K, h->pairs.K.data(), h->pairs.K.size()));
+    const std::vector<double> &tab = rys_table_host();
+    CUDA_TRY(dev_upload(h, &h->d_tab, tab.data(), tab.size()));
+    const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
+    CUDA_TRY(dev_alloc(h, &h->dev.D, ntri));
+    CUDA_TRY(dev_alloc(h, &h->dev.F, ntri));
+    CUDA_TRY(dev_alloc(h, &h->d_maxd, 1));
+    return LIBERI_OK;
+}
+
+static DevBasis dev_basis(liberi_handle h) {
+    DevBasis d;
+    d.shell_xyz = h->dev.shell_xyz;
+    d.shell_bf0 = h->dev.shell_bf0;
+    d.pair_shell = h->dev.pair_shell;
+    d.pair_prim0 = h->dev.pair_prim0;
+    d.pair_nprim = h->dev.pair_nprim;
+    d.prim_P = h->dev.prim_P;
+    d.prim_K = h->dev.prim_K;
+    return d;
+}
+
+// ---- build ------------------------------------------------------------------------
+static int replan(liberi_handle h) {
+    for (int k = 0; k < NKERN; k++) {
+        PlanHost &ph = h->plan[k];
+        for (void *p : {(void *)ph.d_bra, (void *)ph.d_ket, (void *)ph.d_bra_orig, (void *)ph.d_ket_orig,
+                        (void *)ph.d_pref, (void *)ph.d_bra_x, (void *)ph.d_ket_x, (void *)ph.d_ncount,
+                        (void *)ph.d_pref64, (void *)ph.d_pref32, (void *)ph.d_split}) {
+            if (!p) continue;
+            cudaFree(p);
+            h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), p), h->allocs.end());
+        }
+    }
+    const BasisHost &b = h->basis;
+    for (int k = 0; k < NKERN; k++) {
+        const KernelDesc &kd = KDESC[k];
+        bool run = (k == 0 && h->pairs.nl[0] > 0) || (k >= 1 && k <= 5 && h->pairs.nl[1] > 0) ||
+                   (k >= 6 && h->pairs.nl[2] > 0);
+        (void)kd;
+        if (run) build_plan(h->pairs, k, h->schwarz_cut, h->plan[k]);
+        else h->plan[k] = PlanHost();
+    }
+    (void)b;
+    int rc = upload_plans(h);
+    if (rc) return rc;
+    compute_stats(h);
+    h->plan_dirty = false;
+    return LIBERI_OK;
+}
+
+static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaStream_t st) {
+    if (h->plan_dirty) {
+        int rc = replan(h);
+        if (rc) return rc;
+    }
+    const BasisHost &b = h->basis;
+    const long long ntri = (long long)b.num_bas * (b.num_bas + 1) / 2;
+    CUDA_TRY(cudaMemsetAsync(dF, 0, ntri * sizeof(double), st));  // liberi_driver.F90:64
+    LaunchCtx ctx;
+    ctx.basis = dev_basis(h);
+    ctx.rys_tab = h->d_tab;
+    ctx.D = dD;
+    ctx.F = dF;
+    ctx.schwarz_cut = h->schwarz_cut;
+    ctx.eri_cut = h->eri_cut;
+    ctx.stream = st;
+    ctx.num_sms = h->num_sms;
+    const bool mixed = h->precision == 1;
+    if (mixed) CUDA_TRY(launch_maxabs(dD, ntri, h->d_maxd, st));
+    for (int k = 0; k < NKERN; k++) h->ev_recorded[k] = false;
+    for (int k = 0; k < NKERN; k++) {
+        PlanHost &ph = h->plan[k];
+        if (ph.total == 0 || !((h->class_mask >> k) & 1u)) continue;
+        const KernelDesc &kd = KDESC[k];
+        if (h->timing) {
+            if (!h->ev[k][0]) {
+                CUDA_TRY(cudaEventCreate(&h->ev[k][0]));
+                CUDA_TRY(cudaEventCreate(&h->ev[k][1]));
+            }
+            CUDA_TRY(cudaEventRecord(h->ev[k][0], st));
+        }
+        RankSplit rs;
+        rs.rank = h->my_rank;
+        rs.nsize = h->num_procs;
+        rs.tile = kd.tile;
+        rs.ntot = ph.ntot_ref;
+        rs.nbra_ref = ph.nbra_ref;
+        rs.nket_ref = ph.nket_ref;
+        rs.tri = kd.tri;
+        rs.ketmajor = kd.ketmajor;
+        DevPlan dp;
+        dp.nbra = ph.nbra;
+        dp.nket = ph.nket;
+        dp.bra_ids = ph.d_bra;
+        dp.ket_ids = ph.d_ket;
+        dp.bra_orig = ph.d_bra_orig;
+        dp.ket_orig = ph.d_ket_orig;
+        dp.total = ph.total;
+        if (!mixed) {
+            dp.pref = ph.d_pref;
+            dp.split = nullptr;
+            CUDA_TRY(launch_class(k, ctx, dp, rs, 0));
+        } else {
+            CUDA_TRY(launch_split(ph.nbra, ph.d_bra_x, ph.d_ket_x, ph.d_ncount, h->d_maxd, h->fp32_cut,
+                                  ph.d_split, ph.d_pref64, ph.d_pref32, st));
+            dp.pref = ph.d_pref64;
+            dp.split = nullptr;
+            CUDA_TRY(launch_class(k, ctx, dp, rs, 0));
+            dp.pref = ph.d_pref32;
+            dp.split = ph.d_split;
+            CUDA_TRY(launch_class(k, ctx, dp, rs, 1));
+        }
+        if (h->timing) {
+            CUDA_TRY(cudaEventRecord(h->ev[k][1], st));
+            h->ev_recorded[k] = true;
+        }
+    }
+    return LIBERI_OK;
+}
+
+// ================================ C ABI ===========================================
+extern "C" {
+
+int liberi_c_last_error(char *buf, int32_t len) {
+    if (!buf || len <= 0) return LIBERI_E_ARG;
+    snprintf(buf, (size_t)len, "%s", g_err.c_str());
+    return LIBERI_OK;
+}
+
+const char *liberi_c_kernel_name(int32_t k) { return (k >= 0 && k < NKERN) ? KDESC[k].name : nullptr; }
+
+int liberi_c_rys_eval(int32_t n, double T, double thr, int32_t strict, double *u, double *w) {
+    if (n < 1 || n > MAXROOT || !u || !w || !(T >= 0.0)) return fail(LIBERI_E_ARG, "liberi_rys_eval: bad argument");
+    const std::vector<double> &tab = rys_table_host();
+    const bool asym = strict ? (T > thr) : (T >= thr);
+    if (asym || T >= RYS_TMAX) {
+        const double it = 1.0 / T, sq = std::sqrt(it);
+        for (int i = 0; i < n; i++) {
+            u[i] = tab[rys_herm_off(n) + i] * it;
+            w[i] = tab[rys_herm_off(n) + MAXROOT + i] * sq;
+        }
+        return LIBERI_OK;
+    }
+    const int k = (int)T;
+    const double x = 2.0 * (T - (double)k) - 1.0;
+    const double *base = tab.data() + rys_table_off(n) + (size_t)k * 2 * n * RYS_NCOEF;
+    for (int f = 0; f < 2 * n; f++) {
+        const double *cf = base + f * RYS_NCOEF;
+        double v = cf[RYS_DEG];
+        for (int j = RYS_DEG - 1; j >= 0; j--) v = std::fma(v, x, cf[j]);
+        if (f < n) u[f] = v; else w[f - n] = v;
+    }
+    return LIBERI_OK;
+}
+
+int liberi_c_create(liberi_handle *handle) {
+    if (!handle) return fail(LIBERI_E_ARG, "liberi_create: null handle pointer");
+    *handle = new (std::nothrow) liberi_handle_s();
+    if (!*handle) return fail(LIBERI_E_NOMEM, "liberi_create: out of host memory");
+    memset(&(*handle)->stats, 0, sizeof(liberi_stats));
+    return LIBERI_OK;
+}
+
+int liberi_c_cleanup(liberi_handle h) {
+    if (!h) return fail(LIBERI_E_ARG, "liberi_cleanup: null handle");
+    if (!h->initialized) return LIBERI_OK;  // liberi_interface.F90:236
+    cudaSetDevice(h->device);
+    for (int k = 0; k <= NKERN; k++)
+        for (int j = 0; j < 2; j++)
+            if (h->ev[k][j]) {
+                cudaEventDestroy(h->ev[k][j]);
+                h->ev[k][j] = nullptr;
+            }
+    free_device(h);
+    h->basis = BasisHost();
+    h->pairs = PairsHost();
+    h->initialized = false;
+    return LIBERI_OK;
+}
+
+int liberi_c_destroy(liberi_handle h) {
+    if (!h) return fail(LIBERI_E_ARG, "liberi_destroy: null handle");
+    liberi_c_cleanup(h);
+    delete h;
+    return LIBERI_OK;
+}
+
+int liberi_c_setup(liberi_handle h, int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot,
+                   const int32_t *ang_mom, const int32_t *contr_num, const int32_t *sh_loc,
+                   const int32_t *atom_num, const int32_t *atom_loc, const int32_t *start_bas,
+                   const int32_t *end_bas, const double *exponents, const double *contr_coef_s,
+                   const double *contr_coef_p, const double *contr_coef_d, const double *contr_coef_f,
+                   const double *coords, const double *schwrz_int, int32_t my_rank, int32_t num_procs) {
+    if (!h) return fail(LIBERI_E_ARG, "liberi_setup: null handle");
+    if (num_procs < 1 || my_rank < 0 || my_rank >= num_procs)
+        return fail(LIBERI_E_ARG, "liberi_setup: rank %d of %d is invalid", my_rank, num_procs);
+    if (h->initialized) liberi_c_cleanup(h);  // liberi_interface.F90:134-136
+    BasisHost b;
+    int rc = copy_basis(b, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num, atom_loc,
+                        start_bas, end_bas, exponents, contr_coef_s, contr_coef_p, contr_coef_d, contr_coef_f,
+                        coords, schwrz_int);
+    if (rc) return rc;
+    rc = validate_basis(b);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
+    h->num_sms = prop.multiProcessorCount;
+    h->basis = std::move(b);
+    h->my_rank = my_rank;
+    h->num_procs = num_procs;
+    std::vector<double4> shell_xyz;
+    build_pairs(h->basis, h->pairs, shell_xyz);
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    rc = upload_basis(h, shell_xyz);
+    if (!rc) rc = replan(h);
+    if (rc) {
+        free_device(h);
+        return rc;
+    }
+    h->stats.device_bytes = (int64_t)h->dev.bytes;
+    h->initialized = true;
+    return LIBERI_OK;
+}
+
+int liberi_c_fock_build_device(liberi_handle h, const double *d_density, double *d_fock, void *stream) {
+    if (!h) return fail(LIBERI_E_ARG, "liberi_fock_build: null handle");
+    if (!h->initialized) return fail(LIBERI_E_STATE, "liberi_fock_build called before liberi_setup");
+    if (!d_density || !d_fock) return fail(LIBERI_E_ARG, "liberi_fock_build: null device buffer");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    int rc = build_on_device(h, d_density, d_fock, st);
+    if (rc) return rc;
+    CUDA_TRY(cudaGetLastError());
+    return LIBERI_OK;
+}
+
+int liberi_c_fock_build(liberi_handle h, const double *density, double *fock, int32_t matrix_size) {
+    if (!h) return fail(LIBERI_E_ARG, "liberi_fock_build: null handle");
+    if (!h->initialized) return fail(LIBERI_E_STATE, "liberi_fock_build called before liberi_setup");
+    const long long n = h->basis.num_bas;
+    if ((long long)matrix_size != n * (n + 1) / 2)
+        return fail(LIBERI_E_SIZE, "liberi_fock_build: matrix_size %d != num_bas(num_bas+1)/2 = %lld",
+                    matrix_size, n * (n + 1) / 2);
+    if (!density || !fock) return fail(LIBERI_E_ARG, "liberi_fock_build: null buffer");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    CUDA_TRY(cudaEventRecord(e0, st));
+    CUDA_TRY(cudaMemcpyAsync(h->dev.D, density, (size_t)matrix_size * sizeof(double), cudaMemcpyHostToDevice, st));
+    int rc = build_on_device(h, h->dev.D, h->dev.F, st);
+    if (rc) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc;
+    }
+    CUDA_TRY(cudaMemcpyAsync(fock, h->dev.F, (size_t)matrix_size * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaEventRecord(e1, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    h->stats.build_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return LIBERI_OK;
+}
+
+int liberi_c_set_option(liberi_handle h, const char *name, double value) {
+    if (!h || !name) return fail(LIBERI_E_ARG, "liberi_set_option: null argument");
+    std::string n(name);
+    if (n == "schwarz_cut") {
+        if (!(value > 0)) return fail(LIBERI_E_ARG, "schwarz_cut must be > 0");
+        h->schwarz_cut = value;
+        h->plan_dirty = h->initialized;
+    } else if (n == "eri_cut") {
+        if (!(value >= 0)) return fail(LIBERI_E_ARG, "eri_cut must be >= 0");
+        h->eri_cut = value;
+    } else if (n == "fp32_cut") {
+        if (!(value >= 0)) return fail(LIBERI_E_ARG, "fp32_cut must be >= 0");
+        h->fp32_cut = value;
+    } else if (n == "precision") {
+        if (value != 0 && value != 1) return fail(LIBERI_E_ARG, "precision must be 0 or 1");
+        h->precision = (int)value;
+    } else if (n == "device") {
+        if (h->initialized) return fail(LIBERI_E_STATE, "device must be chosen before setup");
+        h->device = (int)value;
+    } else if (n == "class_mask") {
+        if (!(value >= 0 && value < (double)(1u << NKERN))) return fail(LIBERI_E_ARG, "class_mask out of range");
+        h->class_mask = (uint32_t)value;
+    } else if (n == "timing") {
+        h->timing = value != 0;
+    } else {
+        return fail(LIBERI_E_ARG, "unknown option '%s'", name);
+    }
+    return LIBERI_OK;
+}
+
+int liberi_c_get_option(liberi_handle h, const char *name, double *value) {
+    if (!h || !name || !value) return fail(LIBERI_E_ARG, "liberi_get_option: null argument");
+    std::string n(name);
+    if (n == "schwarz_cut") *value = h->schwarz_cut;
+    else if (n == "eri_cut") *value = h->eri_cut;
+    else if (n == "fp32_cut") *value = h->fp32_cut;
+    else if (n == "precision") *value = h->precision;
+    else if (n == "device") *value = h->device;
+    else if (n == "class_mask") *value = h->class_mask;
+    else if (n == "timing") *value = h->timing ? 1 : 0;
+    else return fail(LIBERI_E_ARG, "unknown option '%s'", name);
+    return LIBERI_OK;
+}
+
+int liberi_c_get_stats(liberi_handle h, liberi_stats *stats) {
+    if (!h || !stats) return fail(LIBERI_E_ARG, "liberi_get_stats: null argument");
+    for (int k = 0; k < NKERN; k++) {
+        h->stats.kernel_ms[k] = 0.0;
+        if (h->timing && h->ev_recorded[k]) {
+            float ms = 0.f;
+            if (cudaEventSynchronize(h->ev[k][1]) == cudaSuccess &&
+                cudaEventElapsedTime(&ms, h->ev[k][0], h->ev[k][1]) == cudaSuccess)
+                h->stats.kernel_ms[k] = ms;
+        }
+    }
+    *stats = h->stats;
+    return LIBERI_OK;
+}
+
+int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot, const int32_t *ang_mom,
+                     const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
+                     const int32_t *atom_loc, const double *exponents, const double *contr_coef_s,
+                     const double *contr_coef_p, const double *contr_coef_d, const double *coords,
+                     double *schwrz_out) {
+    if (!schwrz_out) return fail(LIBERI_E_ARG, "liberi_schwarz: null output");
+    liberi_handle_s tmp;
+    std::vector<double> ones((size_t)(nsh > 0 ? nsh : 0) * (nsh + 1) / 2, 1.0);
+    int rc = copy_basis(tmp.basis, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num,
+                        atom_loc, nullptr, nullptr, exponents, contr_coef_s, contr_coef_p, contr_coef_d,
+                        nullptr, coords, ones.data());
+    if (rc) return rc;
+    rc = validate_basis(tmp.basis);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(0));
+    std::vector<double4> shell_xyz;
+    build_pairs(tmp.basis, tmp.pairs, shell_xyz);
+    CUDA_TRY(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking));
+    rc = upload_basis(&tmp, shell_xyz);
+    double *d_out = nullptr;
+    const int npairs = tmp.pairs.class_off[NPC];
+    if (!rc) {
+        cudaError_t e = dev_alloc(&tmp, &d_out, (size_t)npairs);
+        if (e != cudaSuccess) rc = fail(LIBERI_E_NOMEM, "liberi_schwarz: %s", cudaGetErrorString(e));
+    }
+    if (!rc) {
+        DevBasis db = dev_basis(&tmp);
+        for (int c = 0; c < NPC && !rc; c++) {
+            int off = tmp.pairs.class_off[c], n = tmp.pairs.class_off[c + 1] - off;
+            cudaError_t e = launch_schwarz(c, n, off, db, tmp.d_tab, d_out + off, tmp.stream);
+            if (e != cudaSuccess) rc = fail(LIBERI_E_DEVICE, "liberi_schwarz: %s", cudaGetErrorString(e));
+        }
+    }
+    std::vector<double> per_pair(npairs);
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(per_pair.data(), d_out, npairs * sizeof(double), cudaMemcpyDeviceToHost,
+                                        tmp.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(tmp.stream);
+        if (e != cudaSuccess) rc = fail(LIBERI_E_DEVICE, "liberi_schwarz: %s", cudaGetErrorString(e));
+    }
+    if (!rc) {
+        const size_t ntri = (size_t)nsh * (nsh + 1) / 2;
+        std::fill(schwrz_out, schwrz_out + ntri, 0.0);
+        for (int p = 0; p < npairs; p++) {
+            int hi = std::max(tmp.pairs.ish[p], tmp.pairs.jsh[p]) + 1, lo = std::min(tmp.pairs.ish[p], tmp.pairs.jsh[p]) + 1;
+            schwrz_out[(size_t)hi * (hi - 1) / 2 + lo - 1] = per_pair[p];
+        }
+    }
+    free_device(&tmp);
+    return rc;
+}
+
+// ---- GAMESS direct-link wrapper (module-level saved handle) ------------------------
+static std::mutex g_wrap_mu;
+static liberi_handle g_wrap = nullptr;
+static long long g_wrap_size = 0;
+
+int liberi_c_init(int32_t natoms, int32_t num_bas, int32_t nsh, int32_t mxgtot, const int32_t *ang_mom,
+                  const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
+                  const int32_t *atom_loc, const int32_t *start_bas, const int32_t *end_bas,
+                  const double *exponents, const double *contr_coef_s, const double *contr_coef_p,
+                  const double *contr_coef_d, const double *contr_coef_f, const double *coords,
+                  const double *schwrz_int, int32_t my_rank, int32_t num_procs) {
+    std::lock_guard<std::mutex> lk(g_wrap_mu);
+    if (g_wrap) {  // gms_liberi_wrapper.F90:82-85
+        liberi_c_cleanup(g_wrap);
+        liberi_c_destroy(g_wrap);
+        g_wrap = nullptr;
+    }
+    int rc = liberi_c_create(&g_wrap);
+    if (rc) return rc;
+    rc = liberi_c_setup(g_wrap, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num, atom_loc,
+                        start_bas, end_bas, exponents, contr_coef_s, contr_coef_p, contr_coef_d, contr_coef_f,
+                        coords, schwrz_int, my_rank, num_procs);
+    if (rc) {
+        std::string msg = g_err;
+        liberi_c_destroy(g_wrap);
+        g_wrap = nullptr;
+        g_err = msg;
+        return rc;
+    }
+    g_wrap_size = (long long)num_bas * (num_bas + 1) / 2;
+    return LIBERI_OK;
+}
+
+int liberi_c_fock(const double *density, double *fock, int32_t n) {
+    std::lock_guard<std::mutex> lk(g_wrap_mu);
+    if (!g_wrap) return fail(LIBERI_E_STATE, "liberi_fock called before liberi_init");
+    if ((long long)n != g_wrap_size)  // gms_liberi_wrapper.F90:122-127
+        return fail(LIBERI_E_SIZE, "matrix size mismatch in liberi_fock: expected %lld, got %d", g_wrap_size, n);
+    return liberi_c_fock_build(g_wrap, density, fock, n);
+}
+
+int liberi_c_finalize(void) {
+    std::lock_guard<std::mutex> lk(g_wrap_mu);
+    if (g_wrap) {
+        liberi_c_cleanup(g_wrap);
+        liberi_c_destroy(g_wrap);
+        g_wrap = nullptr;
+    }
+    return LIBERI_OK;
+}
+
+}  // extern "C"

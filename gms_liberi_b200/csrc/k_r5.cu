@@ -1,0 +1,6 @@
+// k_r5.cu -- explicit instantiation of the int2221 quartet class (quartet.cuh).
+#include "quartet.cuh"
+
+namespace liberi {
+template cudaError_t launch_t<2, 2, 2, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
+}  // namespace liberi

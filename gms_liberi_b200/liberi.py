@@ -1,0 +1,264 @@
+"""Python front end of the B200 Fock-build engine (ctypes over the C ABI in
+include/liberi_b200.h).
+
+Mirrors libERI's Fortran API for this path:
+
+* handle API (src/interface/liberi_interface.F90): ``liberi_create``,
+  ``liberi_setup``, ``liberi_fock_build``, ``liberi_cleanup``,
+  ``liberi_destroy`` with the reference's argument lists and meanings;
+* GAMESS direct-link wrapper (src/interface/gms_liberi_wrapper.F90):
+  ``liberi_init`` (natoms first), ``liberi_fock``, ``liberi_finalize``.
+
+Where the reference stops with ``error stop 1`` these raise ``LiberiError``
+carrying the C status code and message.  There is no CPU fallback: importing
+this module fails if the CUDA library has not been built.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libliberi_b200.so")
+
+KERNELS = ["int0000", "int0001", "int0011", "int0111", "int0101", "int1111",
+           "int0002", "int0012", "int0102", "int0112", "int0022", "int0122",
+           "int1102", "int0202", "int2211", "int2121", "int2120", "int2111",
+           "int2220", "int2221", "int2222"]
+
+EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fock_build",
+           "liberi_c_cleanup", "liberi_c_init", "liberi_c_fock", "liberi_c_finalize",
+           "liberi_c_last_error", "liberi_c_set_option", "liberi_c_get_option",
+           "liberi_c_fock_build_device", "liberi_c_schwarz", "liberi_c_get_stats",
+           "liberi_c_kernel_name", "liberi_c_rys_eval"]
+
+_I32P = ctypes.POINTER(ctypes.c_int32)
+_F64P = ctypes.POINTER(ctypes.c_double)
+
+
+class LiberiError(RuntimeError):
+    """A failed C-ABI call; ``code`` is the negative LIBERI_E_* status."""
+
+    def __init__(self, code, msg):
+        super().__init__("liberi error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("quartets", ctypes.c_int64 * 21), ("fp32_quartets", ctypes.c_int64 * 21),
+                ("prim_quartets", ctypes.c_int64 * 21), ("kernel_ms", ctypes.c_double * 21),
+                ("build_ms", ctypes.c_double), ("device_bytes", ctypes.c_int64)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library; raises if it was not built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libliberi_b200.so not built at %s; run __graft_entry__.build()" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        H = ctypes.c_void_p
+        L.liberi_c_create.argtypes = [ctypes.POINTER(H)]
+        L.liberi_c_destroy.argtypes = [H]
+        L.liberi_c_cleanup.argtypes = [H]
+        L.liberi_c_setup.argtypes = [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                     _I32P, _I32P, _I32P, _I32P, _I32P, _I32P, _I32P,
+                                     _F64P, _F64P, _F64P, _F64P, _F64P, _F64P, _F64P,
+                                     ctypes.c_int32, ctypes.c_int32]
+        L.liberi_c_fock_build.argtypes = [H, _F64P, _F64P, ctypes.c_int32]
+        L.liberi_c_fock_build_device.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.liberi_c_init.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                    _I32P, _I32P, _I32P, _I32P, _I32P, _I32P, _I32P,
+                                    _F64P, _F64P, _F64P, _F64P, _F64P, _F64P, _F64P,
+                                    ctypes.c_int32, ctypes.c_int32]
+        L.liberi_c_fock.argtypes = [_F64P, _F64P, ctypes.c_int32]
+        L.liberi_c_finalize.argtypes = []
+        L.liberi_c_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int32]
+        L.liberi_c_set_option.argtypes = [H, ctypes.c_char_p, ctypes.c_double]
+        L.liberi_c_get_option.argtypes = [H, ctypes.c_char_p, _F64P]
+        L.liberi_c_schwarz.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                       _I32P, _I32P, _I32P, _I32P, _I32P,
+                                       _F64P, _F64P, _F64P, _F64P, _F64P, _F64P]
+        L.liberi_c_get_stats.argtypes = [H, ctypes.POINTER(Stats)]
+        L.liberi_c_rys_eval.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                                        _F64P, _F64P]
+        L.liberi_c_kernel_name.argtypes = [ctypes.c_int32]
+        L.liberi_c_kernel_name.restype = ctypes.c_char_p
+        for name in EXPORTS:
+            if name != "liberi_c_kernel_name":
+                getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        buf = ctypes.create_string_buffer(512)
+        lib().liberi_c_last_error(buf, 512)
+        raise LiberiError(rc, buf.value.decode(errors="replace"))
+
+
+def _i32(x, keep):
+    a = np.ascontiguousarray(x, dtype=np.int32)
+    keep.append(a)
+    return a.ctypes.data_as(_I32P)
+
+
+def _f64(x, keep):
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    keep.append(a)
+    return a.ctypes.data_as(_F64P)
+
+
+class LiberiHandle:
+    """Opaque handle (liberi_handle_t, liberi_interface.F90:30-43)."""
+
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+        _check(lib().liberi_c_create(ctypes.byref(self._h)))
+        self.num_bas = 0
+
+    @property
+    def ptr(self):
+        return self._h
+
+    def set_option(self, name, value):
+        _check(lib().liberi_c_set_option(self._h, name.encode(), float(value)))
+
+    def get_option(self, name):
+        v = ctypes.c_double()
+        _check(lib().liberi_c_get_option(self._h, name.encode(), ctypes.byref(v)))
+        return v.value
+
+    def stats(self):
+        s = Stats()
+        _check(lib().liberi_c_get_stats(self._h, ctypes.byref(s)))
+        return {"quartets": np.array(s.quartets[:]), "fp32_quartets": np.array(s.fp32_quartets[:]),
+                "prim_quartets": np.array(s.prim_quartets[:]), "kernel_ms": np.array(s.kernel_ms[:]),
+                "build_ms": s.build_ms, "device_bytes": s.device_bytes}
+
+    def destroy(self):
+        if self._h:
+            _check(lib().liberi_c_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().liberi_c_destroy(self._h)
+        except Exception:
+            pass
+
+
+# ---- reference-named handle API ------------------------------------------------
+def liberi_create():
+    """liberi_create(handle) -- liberi_interface.F90:46-55."""
+    return LiberiHandle()
+
+
+def liberi_destroy(handle):
+    """liberi_destroy(handle) -- cleans up if initialised (:57-70)."""
+    handle.destroy()
+
+
+def liberi_setup(handle, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num,
+                 atom_loc, start_bas, end_bas, exponents, contr_coef_s, contr_coef_p, contr_coef_d,
+                 contr_coef_f, coords, schwrz_int, my_rank, num_procs):
+    """liberi_setup(...) -- liberi_interface.F90:72-200 (deep copy, pairs, plan)."""
+    k = []
+    _check(lib().liberi_c_setup(handle.ptr, nsh, natoms, num_bas, mxgtot, _i32(ang_mom, k),
+                                _i32(contr_num, k), _i32(sh_loc, k), _i32(atom_num, k), _i32(atom_loc, k),
+                                _i32(start_bas, k), _i32(end_bas, k), _f64(exponents, k),
+                                _f64(contr_coef_s, k), _f64(contr_coef_p, k), _f64(contr_coef_d, k),
+                                _f64(contr_coef_f, k), _f64(coords, k), _f64(schwrz_int, k),
+                                my_rank, num_procs))
+    handle.num_bas = num_bas
+
+
+def liberi_fock_build(handle, density, fock, matrix_size):
+    """liberi_fock_build(handle, density, fock, matrix_size) -- :202-227.
+    ``fock`` (float64, C-contiguous) is overwritten with this rank's partial F."""
+    d = np.ascontiguousarray(density, dtype=np.float64)
+    if not (isinstance(fock, np.ndarray) and fock.dtype == np.float64 and fock.flags.c_contiguous):
+        raise TypeError("fock must be a C-contiguous float64 array")
+    if d.size < matrix_size or fock.size < matrix_size:
+        raise LiberiError(-3, "density/fock shorter than matrix_size")
+    _check(lib().liberi_c_fock_build(handle.ptr, d.ctypes.data_as(_F64P), fock.ctypes.data_as(_F64P),
+                                     matrix_size))
+
+
+def liberi_cleanup(handle):
+    """liberi_cleanup(handle) -- :229-260."""
+    _check(lib().liberi_c_cleanup(handle.ptr))
+
+
+# ---- GAMESS direct-link wrapper -------------------------------------------------
+def liberi_init(natoms, num_bas, nsh, mxgtot, ang_mom, contr_num, sh_loc, atom_num, atom_loc,
+                start_bas, end_bas, exponents, contr_coef_s, contr_coef_p, contr_coef_d,
+                contr_coef_f, coords, schwrz_int, my_rank, num_procs):
+    """liberi_init (natoms first) -- gms_liberi_wrapper.F90:29-100."""
+    k = []
+    _check(lib().liberi_c_init(natoms, num_bas, nsh, mxgtot, _i32(ang_mom, k), _i32(contr_num, k),
+                               _i32(sh_loc, k), _i32(atom_num, k), _i32(atom_loc, k), _i32(start_bas, k),
+                               _i32(end_bas, k), _f64(exponents, k), _f64(contr_coef_s, k),
+                               _f64(contr_coef_p, k), _f64(contr_coef_d, k), _f64(contr_coef_f, k),
+                               _f64(coords, k), _f64(schwrz_int, k), my_rank, num_procs))
+
+
+def liberi_fock(density, fock, n):
+    """liberi_fock(density, fock, n) with the wrapper's size check -- :103-131."""
+    d = np.ascontiguousarray(density, dtype=np.float64)
+    _check(lib().liberi_c_fock(d.ctypes.data_as(_F64P), fock.ctypes.data_as(_F64P), n))
+
+
+def liberi_finalize():
+    """liberi_finalize() -- :134-146."""
+    _check(lib().liberi_c_finalize())
+
+
+# ---- conveniences over a basis dict ---------------------------------------------
+def _basis_args(b):
+    nsh = int(b["nsh"])
+    mx = int(b["mxgtot"])
+    z = np.zeros(nsh * mx)
+    return (nsh, int(b["natoms"]), int(b["num_bas"]), mx, b["ang_mom"], b["contr_num"], b["sh_loc"],
+            b["atom_num"], b["atom_loc"], b.get("start_bas", b["atom_loc"]), b.get("end_bas", b["atom_loc"]),
+            b["exponents"], b["coef_s"], b["coef_p"], b["coef_d"], b.get("coef_f", z), b["coords"])
+
+
+def setup_from_basis(handle, basis, schwrz=None, my_rank=0, num_procs=1):
+    (nsh, natoms, nbf, mx, ang, cn, sl, an, al, sb, eb, ex, cs, cp, cd, cf, xyz) = _basis_args(basis)
+    sw = basis["schwrz"] if schwrz is None else schwrz
+    liberi_setup(handle, nsh, natoms, nbf, mx, ang, cn, sl, an, al, sb, eb, ex, cs, cp, cd, cf, xyz, sw,
+                 my_rank, num_procs)
+
+
+def fock(handle, density):
+    """Packed partial F for packed D through liberi_fock_build."""
+    n = handle.num_bas
+    ntri = n * (n + 1) // 2
+    out = np.zeros(ntri)
+    liberi_fock_build(handle, density, out, ntri)
+    return out
+
+
+def rys_eval(n, T, thr=60.0, strict=False):
+    """Engine Rys roots/weights (host evaluation of the device tables)."""
+    u = np.zeros(n)
+    w = np.zeros(n)
+    _check(lib().liberi_c_rys_eval(n, T, thr, int(strict), u.ctypes.data_as(_F64P), w.ctypes.data_as(_F64P)))
+    return u, w
+
+
+def schwarz(basis):
+    """Packed shell Schwarz table computed on the device."""
+    (nsh, natoms, nbf, mx, ang, cn, sl, an, al, sb, eb, ex, cs, cp, cd, cf, xyz) = _basis_args(basis)
+    k = []
+    out = np.zeros(nsh * (nsh + 1) // 2)
+    _check(lib().liberi_c_schwarz(nsh, natoms, nbf, mx, _i32(ang, k), _i32(cn, k), _i32(sl, k),
+                                  _i32(an, k), _i32(al, k), _f64(ex, k), _f64(cs, k), _f64(cp, k),
+                                  _f64(cd, k), _f64(xyz, k), out.ctypes.data_as(_F64P)))
+    return out

@@ -1,0 +1,150 @@
+/*
+ * liberi_b200.h -- C ABI of the B200 RHF Fock-build engine.
+ *
+ * Drop-in for libERI's handle API and its GAMESS direct-link wrapper.  Every
+ * entry point returns an int status: 0 on success, a negative LIBERI_E_* code
+ * otherwise; liberi_c_last_error() returns the message of the calling thread's
+ * last failure.  The reference aborts with `error stop 1` instead; the Fortran
+ * shim (gms_liberi_b200/fortran/liberi_b200_interface.F90) maps a non-zero
+ * status back to `error stop 1`.
+ *
+ * Layout conventions follow the reference exactly:
+ *   - density and Fock matrices are packed lower triangles of length
+ *     n(n+1)/2, element (i,j), i>=j, 1-based, at ia(i)+j with ia(i)=i(i-1)/2
+ *     (src/liberi_shell_pair.F90:131-133, src/rhf/rot_axis/int0000.F90:273-283);
+ *   - schwrz_int is packed the same way over shells;
+ *   - sh_loc, atom_num, atom_loc are 1-based; ang_mom 1=s 2=p 3=d;
+ *     Cartesian d order xx,yy,zz,xy,xz,yz with sqrt(3) on xy,xz,yz.
+ * All integer arguments are int32_t (the reference requires c_int at the
+ * boundary), all real arrays double.
+ */
+#ifndef LIBERI_B200_H
+#define LIBERI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct liberi_handle_s *liberi_handle;
+
+enum {
+    LIBERI_OK = 0,
+    LIBERI_E_ARG = -1,        /* bad pointer, size or option */
+    LIBERI_E_STATE = -2,      /* call before setup, after cleanup, ... */
+    LIBERI_E_SIZE = -3,       /* matrix_size != num_bas(num_bas+1)/2 */
+    LIBERI_E_DEVICE = -4,     /* CUDA error */
+    LIBERI_E_NOMEM = -5,      /* device allocation failed or over limit */
+    LIBERI_E_UNSUPPORTED = -6 /* f shells (ang_mom 4) are not built */
+};
+
+/* ---- handle API: src/interface/liberi_interface.F90 --------------------- */
+
+/* liberi_create(handle)                      liberi_interface.F90:46-55 */
+int liberi_c_create(liberi_handle *handle);
+
+/* liberi_destroy(handle): cleans up if still initialised.       :57-70 */
+int liberi_c_destroy(liberi_handle handle);
+
+/* liberi_setup(handle, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num,
+ * sh_loc, atom_num, atom_loc, start_bas, end_bas, exponents, contr_coef_s,
+ * contr_coef_p, contr_coef_d, contr_coef_f, coords, schwrz_int, my_rank,
+ * num_procs).  Deep-copies every input, builds shell pairs and the screened
+ * quartet plan on the device.  Calling it on an initialised handle cleans up
+ * first.                                                          :72-200 */
+int liberi_c_setup(liberi_handle handle, int32_t nsh, int32_t natoms, int32_t num_bas,
+                   int32_t mxgtot, const int32_t *ang_mom, const int32_t *contr_num,
+                   const int32_t *sh_loc, const int32_t *atom_num, const int32_t *atom_loc,
+                   const int32_t *start_bas, const int32_t *end_bas, const double *exponents,
+                   const double *contr_coef_s, const double *contr_coef_p,
+                   const double *contr_coef_d, const double *contr_coef_f, const double *coords,
+                   const double *schwrz_int, int32_t my_rank, int32_t num_procs);
+
+/* liberi_fock_build(handle, density, fock, matrix_size): overwrites fock
+ * with this rank's partial two-electron Fock contribution (host buffers).
+ * The caller reduces partials across ranks, as GAMESS does with DDI_GSUMF.
+ *                                                                 :202-227 */
+int liberi_c_fock_build(liberi_handle handle, const double *density, double *fock,
+                        int32_t matrix_size);
+
+/* liberi_cleanup(handle): frees device state; no-op if not set up. :229-260 */
+int liberi_c_cleanup(liberi_handle handle);
+
+/* ---- GAMESS direct-link wrapper: src/interface/gms_liberi_wrapper.F90 ---- */
+
+/* liberi_init(natoms, num_bas, nsh, mxgtot, ...): note natoms first.  :29-100 */
+int liberi_c_init(int32_t natoms, int32_t num_bas, int32_t nsh, int32_t mxgtot,
+                  const int32_t *ang_mom, const int32_t *contr_num, const int32_t *sh_loc,
+                  const int32_t *atom_num, const int32_t *atom_loc, const int32_t *start_bas,
+                  const int32_t *end_bas, const double *exponents, const double *contr_coef_s,
+                  const double *contr_coef_p, const double *contr_coef_d,
+                  const double *contr_coef_f, const double *coords, const double *schwrz_int,
+                  int32_t my_rank, int32_t num_procs);
+/* liberi_fock(density, fock, n) with the wrapper's size check.    :103-131 */
+int liberi_c_fock(const double *density, double *fock, int32_t n);
+/* liberi_finalize()                                               :134-146 */
+int liberi_c_finalize(void);
+
+/* ---- extensions without a reference counterpart ------------------------- */
+
+/* Message of the calling thread's last failure (NUL-terminated, truncated). */
+int liberi_c_last_error(char *buf, int32_t len);
+
+/* Runtime options; defaults reproduce the reference's compile-time constants.
+ *   "schwarz_cut"  (5e-11, cutoff_schwarz, src/liberi_parameters.F90:38)
+ *   "eri_cut"      (5e-11, the digestion literal, e.g. int0002.F90:403)
+ *   "fp32_cut"     (1e-7; quartets with xint_ab*xint_cd*max|D| below it run
+ *                   in FP32 when "precision" is 1)
+ *   "precision"    (0 = all FP64, 1 = mixed FP32/FP64)
+ *   "device"       (CUDA device ordinal used by the next setup, default 0)
+ *   "class_mask"   (bit k set = run class k of the driver order; default all 21)
+ *   "timing"       (1 = record per-class device times for liberi_c_get_stats)
+ * Options set before liberi_c_setup apply to it; cut options may also be
+ * changed between builds (the quartet plan is rebuilt on the next build). */
+int liberi_c_set_option(liberi_handle handle, const char *name, double value);
+int liberi_c_get_option(liberi_handle handle, const char *name, double *value);
+
+/* Fock build on device-resident packed buffers (no host copies), enqueued on
+ * `stream` (a cudaStream_t, NULL = the handle's own stream); does not
+ * synchronise.  Used for device-resident benchmarking and graph capture. */
+int liberi_c_fock_build_device(liberi_handle handle, const double *d_density, double *d_fock,
+                               void *stream);
+
+/* Schwarz table generator: schwrz_out[ia(max)+min] = sqrt(max_components
+ * |(ab|ab)|) over shell pairs, computed on the device (GAMESS supplies this
+ * table to the reference, liberi_interface.F90:128-129). */
+int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot,
+                     const int32_t *ang_mom, const int32_t *contr_num, const int32_t *sh_loc,
+                     const int32_t *atom_num, const int32_t *atom_loc, const double *exponents,
+                     const double *contr_coef_s, const double *contr_coef_p,
+                     const double *contr_coef_d, const double *coords, double *schwrz_out);
+
+/* Per-kernel statistics of the last build, 21 rows in the reference driver
+ * order (liberi_driver.F90:69-102):
+ *   quartets[k]     screened shell quartets owned by this rank
+ *   fp32_quartets[k] of those, evaluated in FP32
+ *   prim_quartets[k] primitive quartets (after mu*R^2 > 50 pair removal)
+ *   kernel_ms[k]    device time of the class (0 unless timing is enabled)  */
+typedef struct {
+    int64_t quartets[21];
+    int64_t fp32_quartets[21];
+    int64_t prim_quartets[21];
+    double kernel_ms[21];
+    double build_ms;
+    int64_t device_bytes;
+} liberi_stats;
+int liberi_c_get_stats(liberi_handle handle, liberi_stats *stats);
+
+/* Rys roots u_i = t_i^2 and weights w_i (sum w_i = F_0(T)) for n = 1..5 from
+ * the engine's piecewise tables, evaluated on the host exactly as the device
+ * does; the large-T limit is used for T > thr (strict) or T >= thr. */
+int liberi_c_rys_eval(int32_t n, double T, double thr, int32_t strict, double *u, double *w);
+
+/* Name of kernel class k (0..20), e.g. "int2222"; NULL if out of range. */
+const char *liberi_c_kernel_name(int32_t k);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

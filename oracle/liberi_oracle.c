@@ -63,7 +63,6 @@
 
 /* ---- reference parameters (src/liberi_parameters.F90) -------------------- */
 static const double CUX = 50.0;                   /* :44 */
-static const double T_MAX_ROT = 25.0;             /* liberi_boys.F90:22 */
 
 /* ---- Cartesian component tables: p = x,y,z ; d = xx,yy,zz,xy,xz,yz ------- */
 static const int NCART[3] = {1, 3, 6};
@@ -668,8 +667,10 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
  * (liberi_interface.F90:128-129); the oracle provides it for synthetic inputs. */
 int oracle_schwarz(const oracle_basis *b, double *schwrz_out) {
     init_tables();
-    /* evaluate with a dummy descriptor: exact roots, no primitive skipping */
-    kdesc_t kd = {"schwarz", 0, 0, 0, 1, 0, OP_NONE, TILE_NONE, 0, 0, 1e300};
+    /* evaluate with a Rys-style descriptor: no primitive skipping, the
+     * 35-point procedure below T = 60 and the large-T form above it (the
+     * 35-point grid integrates the Rys moments to ~1e-15 only up to T ~ 60) */
+    kdesc_t kd = {"schwarz", 0, 0, 0, 1, 0, OP_NONE, TILE_NONE, 0, 0, 60.0};
     oracle_basis bb = *b;
     int64_t ntri = (int64_t)b->nsh * (b->nsh + 1) / 2;
     double *dummy = malloc(sizeof(double) * (ntri > 0 ? ntri : 1));

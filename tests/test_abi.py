@@ -1,0 +1,95 @@
+"""C-ABI checks that need no GPU: the library loads, exports every entry point
+declared in include/liberi_b200.h, and rejects misuse before touching the
+device (the reference's `error stop 1` paths, liberi_interface.F90:219-222,
+gms_liberi_wrapper.F90:117-127)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from gms_liberi_b200 import liberi
+from conftest import ROOT
+
+
+def test_header_symbols_exported():
+    hdr = open(os.path.join(ROOT, "include", "liberi_b200.h")).read()
+    declared = set(re.findall(r"\b(liberi_c_\w+)\s*\(", hdr))
+    assert len(declared) >= 15
+    L = liberi.lib()
+    for name in declared:
+        assert hasattr(L, name), name
+    assert set(liberi.EXPORTS) == declared
+
+
+def test_kernel_names_in_driver_order():
+    L = liberi.lib()
+    names = [L.liberi_c_kernel_name(i).decode() for i in range(21)]
+    assert names == liberi.KERNELS
+    assert L.liberi_c_kernel_name(21) is None
+
+
+def test_fock_before_setup_is_state_error():
+    h = liberi.liberi_create()
+    with pytest.raises(liberi.LiberiError) as e:
+        liberi.liberi_fock_build(h, np.zeros(1), np.zeros(1), 1)
+    assert e.value.code == -2
+    liberi.liberi_cleanup(h)   # cleanup of an uninitialised handle is a no-op
+    liberi.liberi_cleanup(h)
+    liberi.liberi_destroy(h)
+
+
+def test_wrapper_before_init_is_state_error():
+    liberi.liberi_finalize()
+    with pytest.raises(liberi.LiberiError) as e:
+        liberi.liberi_fock(np.zeros(3), np.zeros(3), 3)
+    assert e.value.code == -2
+
+
+def test_options_validate():
+    h = liberi.liberi_create()
+    assert h.get_option("schwarz_cut") == pytest.approx(5e-11)
+    assert h.get_option("eri_cut") == pytest.approx(5e-11)
+    h.set_option("precision", 1)
+    assert h.get_option("precision") == 1
+    for name, val in [("nope", 1.0), ("precision", 2), ("schwarz_cut", -1.0)]:
+        with pytest.raises(liberi.LiberiError) as e:
+            h.set_option(name, val)
+        assert e.value.code == -1
+
+
+@pytest.mark.parametrize("bad", ["fshell", "rank", "sizes"])
+def test_setup_rejects_bad_input(bad):
+    h = liberi.liberi_create()
+    args = dict(nsh=1, natoms=1, num_bas=1, mxgtot=1, ang=[1], rank=0, nproc=1)
+    if bad == "fshell":
+        args["ang"] = [4]
+        code = -6
+    elif bad == "rank":
+        args["rank"] = 3
+        args["nproc"] = 2
+        code = -1
+    else:
+        args["nsh"] = 0
+        code = -1
+    with pytest.raises(liberi.LiberiError) as e:
+        liberi.liberi_setup(h, args["nsh"], args["natoms"], args["num_bas"], args["mxgtot"], args["ang"],
+                            [1], [1], [1], [1], [1], [1], [1.0], [1.0], [0.0], [0.0], [0.0],
+                            [0.0, 0.0, 0.0], [1.0], args["rank"], args["nproc"])
+    assert e.value.code == code
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5])
+def test_engine_rys_tables_match_oracle(n):
+    # the piecewise tables reproduce the reference's 35-point Stieltjes roots
+    from oracle import oracle
+    rng = np.random.default_rng(n)
+    for T in np.concatenate([[0.0, 1e-9, 0.5, 24.999, 25.0, 42.99, 59.9], rng.uniform(0, 60, 40)]):
+        ue, we = liberi.rys_eval(n, float(T), thr=60.0)
+        uo, wo = oracle.rys_roots(n, float(T), thr=60.0)
+        assert np.allclose(ue, uo, rtol=5e-13, atol=0), (n, T)
+        assert np.allclose(we, wo, rtol=5e-13, atol=0), (n, T)
+    for T in [25.5, 70.0, 300.0]:
+        ue, we = liberi.rys_eval(n, T, thr=25.0, strict=True)
+        uo, wo = oracle.rys_roots(n, T, thr=25.0, rot=True)
+        assert np.allclose(ue, uo, rtol=1e-14) and np.allclose(we, wo, rtol=1e-14)

@@ -1,0 +1,190 @@
+"""GPU parity: the CUDA Fock build (through the C ABI) against the reference's
+known-answer vectors and the CPU oracle.
+
+Tolerances are the ones the reference and its task state:
+  * known-answer vectors: max|dF| <= 1e-10 (tests/fortran/test_*.F90:25);
+  * plain FP64 path vs the oracle: max|dF| <= 1e-10 and |dE| <= 1e-9 Eh with
+    the same screened-quartet set (per-class counts equal);
+  * mixed FP32/FP64 path vs the oracle: |dE| <= 1e-6 Eh.
+E here is the two-electron energy functional 1/2 sum_ij D_ij G_ij of the
+symmetrised packed accumulation, identical for both sides.
+"""
+import numpy as np
+import pytest
+
+from gms_liberi_b200 import liberi
+from gms_liberi_b200 import molecules as M
+from oracle import oracle
+from conftest import KAT_NAMES, load_kat
+
+pytestmark = pytest.mark.gpu
+
+TOL_F = 1e-10
+TOL_E = 1e-9
+
+
+def energy(D, F):
+    # off-diagonal packed elements appear twice in the symmetric matrices
+    n = int((np.sqrt(8 * D.size + 1) - 1) / 2)
+    w = np.full(D.size, 2.0)
+    w[np.arange(1, n + 1) * np.arange(2, n + 2) // 2 - 1] = 1.0
+    return 0.5 * np.sum(w * D * F)
+
+
+def gpu_fock(basis, D, schwrz=None, rank=0, nproc=1, **opts):
+    h = liberi.liberi_create()
+    for k, v in opts.items():
+        h.set_option(k, v)
+    liberi.setup_from_basis(h, basis, schwrz=schwrz, my_rank=rank, num_procs=nproc)
+    F = liberi.fock(h, D)
+    st = h.stats()
+    liberi.liberi_cleanup(h)
+    liberi.liberi_destroy(h)
+    return F, st
+
+
+@pytest.mark.parametrize("name", KAT_NAMES)
+def test_reference_kat_handle_api(name):
+    # the reference test programs, step for step (test_h2o_ccpvdz.F90:636-705)
+    d = load_kat(name)
+    n = d["num_bas"]
+    tri = n * (n + 1) // 2
+    h = liberi.liberi_create()
+    liberi.liberi_setup(h, d["nsh"], d["natoms"], n, d["mxgtot"], d["ang_mom"], d["contr_num"],
+                        d["sh_loc"], d["atom_num"], d["atom_loc"], d["start_bas"], d["end_bas"],
+                        d["exponents"], d["coef_s"], d["coef_p"], d["coef_d"], d["coef_f"],
+                        d["coords"], d["schwrz"], 0, 1)
+    fa = np.zeros(tri)
+    liberi.liberi_fock_build(h, d["density"], fa, tri)
+    err = np.abs(fa - d["fa_ref"]).max()
+    liberi.liberi_cleanup(h)
+    liberi.liberi_destroy(h)
+    assert err <= d["tol"], err
+
+
+def test_reference_kat_gamess_wrapper():
+    d = load_kat("h2o_ccpvdz")
+    n = d["num_bas"]
+    tri = n * (n + 1) // 2
+    liberi.liberi_init(d["natoms"], n, d["nsh"], d["mxgtot"], d["ang_mom"], d["contr_num"], d["sh_loc"],
+                       d["atom_num"], d["atom_loc"], d["start_bas"], d["end_bas"], d["exponents"],
+                       d["coef_s"], d["coef_p"], d["coef_d"], d["coef_f"], d["coords"], d["schwrz"], 0, 1)
+    fa = np.zeros(tri)
+    liberi.liberi_fock(d["density"], fa, tri)
+    assert np.abs(fa - d["fa_ref"]).max() <= 1e-10
+    with pytest.raises(liberi.LiberiError) as e:  # gms_liberi_wrapper.F90:122-127
+        liberi.liberi_fock(d["density"], fa, tri - 1)
+    assert e.value.code == -3
+    liberi.liberi_finalize()
+    with pytest.raises(liberi.LiberiError):
+        liberi.liberi_fock(d["density"], fa, tri)
+
+
+def _molecule(name):
+    if name == "h2o_like":
+        b, nocc = M.h2o_like(), 5
+    elif name == "ethane":
+        b, nocc = M.ethane(), 9
+    else:
+        b = M.random_molecule(int(name.split("_")[1]), seed=11)
+        nocc = M.nocc_of(b)
+    b["schwrz"] = oracle.schwarz(b)
+    return b, nocc
+
+
+@pytest.mark.parametrize("mol", ["h2o_like", "ethane", "random_6", "random_9"])
+@pytest.mark.parametrize("cut", [1e-10, 5e-11])
+def test_fp64_parity_screened(mol, cut):
+    b, nocc = _molecule(mol)
+    D = M.density(b["num_bas"], nocc, seed=5)
+    Fo, cnt = oracle.fock_build(b, D, schwarz_cut=cut, return_counts=True)
+    Fg, st = gpu_fock(b, D, schwarz_cut=cut)
+    assert np.abs(Fg - Fo).max() <= TOL_F
+    assert abs(energy(D, Fg) - energy(D, Fo)) <= TOL_E
+    # the same screened-quartet set, class by class
+    assert (st["quartets"] == cnt[:, 0]).all(), (st["quartets"], cnt[:, 0])
+
+
+def test_identity_and_general_density_kat_basis():
+    d = load_kat("h2o_ccpvdz")
+    rng = np.random.default_rng(1)
+    n = d["num_bas"]
+    A = rng.standard_normal((n, n))
+    D = M.pack(A + A.T)
+    Fo = oracle.fock_build(d, D)
+    Fg, _ = gpu_fock(d, D)
+    assert np.abs(Fg - Fo).max() <= TOL_F
+
+
+def test_schwarz_generator_matches_oracle():
+    for b in (M.h2o_like(), M.ethane(), M.random_molecule(7, seed=2)):
+        sg = liberi.schwarz(b)
+        so = oracle.schwarz(b)
+        assert np.allclose(sg, so, rtol=1e-11, atol=1e-14)
+
+
+@pytest.mark.parametrize("nsize", [2, 3, 7])
+def test_rank_partials_match_reference_split(nsize):
+    b, nocc = _molecule("ethane")
+    D = M.density(b["num_bas"], nocc, seed=2)
+    full, _ = gpu_fock(b, D, schwarz_cut=1e-10)
+    acc = np.zeros_like(full)
+    for r in range(nsize):
+        Fg, _ = gpu_fock(b, D, rank=r, nproc=nsize, schwarz_cut=1e-10)
+        Fo = oracle.fock_build(b, D, schwarz_cut=1e-10, my_rank=r, num_procs=nsize)
+        assert np.abs(Fg - Fo).max() <= TOL_F, r
+        acc += Fg
+    assert np.abs(acc - full).max() <= 1e-11
+
+
+def test_repeated_builds_and_resetup():
+    b, nocc = _molecule("ethane")
+    D1 = M.density(b["num_bas"], nocc, seed=1)
+    D2 = M.density(b["num_bas"], nocc, seed=2)
+    h = liberi.liberi_create()
+    liberi.setup_from_basis(h, b)
+    F1 = liberi.fock(h, D1)
+    F2 = liberi.fock(h, D2)
+    F1b = liberi.fock(h, D1)
+    assert np.abs(F1 - F1b).max() <= 1e-12
+    # linearity in D (size independent)
+    F12 = liberi.fock(h, 0.5 * D1 + 2.0 * D2)
+    assert np.abs(F12 - (0.5 * F1 + 2.0 * F2)).max() <= 1e-11
+    # setup on an initialised handle cleans up first (liberi_interface.F90:134-136)
+    c = M.h2o_like()
+    c["schwrz"] = oracle.schwarz(c)
+    liberi.setup_from_basis(h, c)
+    Dc = M.density(c["num_bas"], 5)
+    assert np.abs(liberi.fock(h, Dc) - oracle.fock_build(c, Dc)).max() <= TOL_F
+    liberi.liberi_cleanup(h)
+    with pytest.raises(liberi.LiberiError):
+        liberi.fock(h, Dc)
+    liberi.liberi_destroy(h)
+
+
+def test_schwarz_cut_option_replans():
+    b, nocc = _molecule("ethane")
+    D = M.density(b["num_bas"], nocc, seed=4)
+    h = liberi.liberi_create()
+    liberi.setup_from_basis(h, b)
+    F_a = liberi.fock(h, D)
+    h.set_option("schwarz_cut", 1e-7)
+    F_b = liberi.fock(h, D)
+    q_b = h.stats()["quartets"]
+    Fo, cnt = oracle.fock_build(b, D, schwarz_cut=1e-7, return_counts=True)
+    assert (q_b == cnt[:, 0]).all()
+    assert np.abs(F_b - Fo).max() <= TOL_F
+    assert np.abs(F_a - oracle.fock_build(b, D)).max() <= TOL_F
+    liberi.liberi_destroy(h)
+
+
+@pytest.mark.parametrize("mol", ["ethane", "random_9"])
+def test_mixed_precision_error_bound(mol):
+    b, nocc = _molecule(mol)
+    D = M.density(b["num_bas"], nocc, seed=6)
+    Fo = oracle.fock_build(b, D, schwarz_cut=1e-10)
+    for cut in (1e-5, 1e-7):
+        Fm, _ = gpu_fock(b, D, schwarz_cut=1e-10, precision=1, fp32_cut=cut)
+        dE = abs(energy(D, Fm) - energy(D, Fo))
+        assert dE <= 1e-6, (cut, dE)
+        assert np.abs(Fm - Fo).max() <= 1e-5
