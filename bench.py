@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark: RHF two-electron Fock build of a C60-shaped molecule in a
+6-31G(d)-shaped basis (900 functions) on B200.
+
+One step = one full Fock build (all 21 s/p/d quartet classes, FP64) over the
+device-resident density, as libERI's liberi_fock_build / compute_integrals
+does per SCF iteration.  Inputs are seeded synthetic data: C60 truncated
+icosahedron with 2.65/2.74 bohr bonds, per-shell log-uniform exponents in
+[0.1, 3000], D = 2 C C^T with 180 orthonormal random columns, Schwarz cut
+1e-10 (the Schwarz table comes from the engine's own generator).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (under torchrun, one process per GPU): every rank builds its share of
+the quartets (the reference's rank split) into a private packed F, and one
+NCCL all-reduce sums F; the metric is ms per complete build (strong scaling).
+`--impl reference` times the reference algorithm's CPU restatement (oracle/,
+OpenMP on all host cores) on a bounded sample of the same quartets and
+extrapolates per class by the exact quartet counts.
+"""
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+from datetime import timedelta
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "C60 6-31G(d) Fock build ms"
+SCHWARZ_CUT = 1e-10
+MIXED_CUT = 1e-7
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work for cpu_baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--per-class", action="store_true", help="add per-class device ms to the JSON line")
+    return ap.parse_args()
+
+
+def workload():
+    from gms_liberi_b200 import molecules as M
+    b = M.c60()
+    return b, M.density(b["num_bas"], 180, seed=0)
+
+
+def config(n):
+    return {"workload": "C60 truncated icosahedron, 6-31G(d)-shaped basis (360 shells, 900 functions), "
+                        "RHF two-electron Fock build, Schwarz cut 1e-10",
+            "natoms": 60, "num_bas": 900, "nocc": 180, "schwarz_cut": SCHWARZ_CUT,
+            "l2": "flushed between timed steps (512 MB device write outside the step events)",
+            "parallelism": "single GPU" if n == 1 else "quartets split across %d ranks, NCCL all-reduce of packed F" % n}
+
+
+# ------------------------------------------------------------------ reference arm
+def oracle_extrapolated_ms(basis, D, budget_s, seed=0, nthreads=0):
+    """Time the oracle on a hashed uniform sample of every class's screened
+    quartets.  Per class the full-run estimate is the candidate-enumeration
+    wall time (paid once in a full run) plus the measured evaluation time
+    scaled by screened / evaluated quartets.  Returns (ms, info)."""
+    from oracle import oracle
+    _, c0, (tw, te, nth) = oracle.fock_build(basis, D, schwarz_cut=SCHWARZ_CUT, sample_mod=20000,
+                                             sample_seed=seed + 1000, nthreads=nthreads, return_times=True)
+    per_q = te.sum() / max(int(c0[:, 3].sum()), 1)  # thread-seconds per evaluated quartet
+    mod = int(np.clip(per_q * c0[:, 0].sum() / (budget_s * nth), 1, 2000000))
+    t0 = time.time()
+    _, c, (tw, te, nth) = oracle.fock_build(basis, D, schwarz_cut=SCHWARZ_CUT, sample_mod=mod, sample_seed=seed,
+                                            nthreads=nthreads, return_times=True)
+    wall = time.time() - t0
+    if mod == 1:
+        ms = float(tw.sum() * 1e3)
+    else:
+        mean_q = te.sum() / max(int(c[:, 3].sum()), 1)
+        ms = 0.0
+        for k in range(21):
+            if c[k, 0] == 0:
+                continue
+            enum = max(tw[k] - te[k] / nth, 0.0)
+            ev = te[k] / nth * c[k, 0] / c[k, 3] if c[k, 3] > 0 else mean_q / nth * c[k, 0]
+            ms += (enum + ev) * 1e3
+    return ms, {"sample_mod": mod, "evaluated_quartets": int(c[:, 3].sum()),
+                "screened_quartets": int(c[:, 0].sum()), "seconds": round(wall, 2), "threads": nth}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle
+    oracle.lib()
+    basis, D = workload()
+    from gms_liberi_b200 import liberi
+    try:
+        basis["schwrz"] = liberi.schwarz(basis)
+    except Exception:
+        basis["schwrz"] = oracle.schwarz(basis)
+    cores = os.cpu_count()
+    per_step = max(5.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    info = None
+    for s in range(args.warmup + args.steps):
+        ms, info = oracle_extrapolated_ms(basis, D, per_step, seed=s, nthreads=cores)
+        if s >= args.warmup:
+            vals.append(ms)
+    v = float(np.mean(vals))
+    line = {"metric": METRIC, "value": round(v, 3), "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config(1),
+            "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": cores, "kind": "port",
+                             "sample": "per step a hashed uniform 1/%d sample of each class's screened quartets "
+                                       "(%d of %d), extrapolated per class by exact counts; reference algorithm "
+                                       "restated in C (oracle/), OpenMP over quartets"
+                                       % (info["sample_mod"], info["evaluated_quartets"], info["screened_quartets"])},
+            "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.lines = []
+        self.proc = None
+        cmd = ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "200"]
+        if uuid:
+            cmd += ["-i", uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_per_launch(kernel):
+    """dram bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "%s_c60.txt" % kernel)
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def run_ours(args):
+    import torch
+    from gms_liberi_b200 import flops, liberi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+
+    basis, Dh = workload()
+    basis["schwrz"] = liberi.schwarz(basis)
+    h = liberi.liberi_create()
+    h.set_option("device", local)
+    h.set_option("schwarz_cut", SCHWARZ_CUT)
+    liberi.setup_from_basis(h, basis, my_rank=rank, num_procs=world)
+    st0 = h.stats()
+    ntri = Dh.size
+    D = torch.from_numpy(Dh).to(dev)
+    F = torch.zeros(ntri, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    # a dedicated stream: the engine's kernels, the flush, the copies, the
+    # all-reduce and the timing events are all ordered on it
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    launched = int(sum(1 for k in range(21) if st0["quartets"][k] > 0))
+
+    def step():
+        liberi.fock_build_device(h, D.data_ptr(), F.data_ptr(), stream.cuda_stream)
+        if world > 1:
+            dist.all_reduce(F)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed_loop(nsteps, per_class=False):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+        cls = np.zeros(21)
+        barrier()
+        for s in range(nsteps):
+            flush.zero_()
+            ev[s][0].record(stream)
+            step()
+            ev[s][1].record(stream)
+            if per_class:
+                cls += h.stats()["kernel_ms"]
+        barrier()
+        ms = [a.elapsed_time(b) for a, b in ev]
+        return float(np.mean(ms)), cls / max(1, nsteps)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    assert stream.cuda_stream != 0
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+
+    # warm-up, then the timed region (clocks sampled, per-class events on)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    h.set_option("timing", 1)
+    clk = ClockSampler(uuid)
+    ms_local, cls_ms = timed_loop(args.steps, per_class=True)
+    clocks = clk.stop()
+    h.set_option("timing", 0)
+    ms = max_over_ranks(ms_local)
+    F_fp64 = F.detach().clone()
+
+    # roofline of the dominant class kernel
+    k_dom = int(np.argmax(cls_ms))
+    kname = liberi.KERNELS[k_dom]
+    fl = flops.class_flops(k_dom, int(st0["prim_quartets"][k_dom]), int(st0["quartets"][k_dom]))
+    peak_fp64 = liberi.microbench(0)
+    achieved = fl / (cls_ms[k_dom] * 1e-3) / 1e12
+    build_tf = flops.build_flops(st0) / (ms_local * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "kernel": "class_kernel<%s>" % kname, "achieved": round(achieved, 3),
+                "peak": round(peak_fp64, 3), "unit": "TFLOP/s", "frac": round(achieved / peak_fp64, 4),
+                "peak_source": "measured FP64 FMA throughput on this GPU (liberi_c_microbench 0)",
+                "traffic": traffic_per_launch(kname), "share": round(float(cls_ms[k_dom] / cls_ms.sum()), 3),
+                "build_achieved_tflops": round(build_tf, 3)}
+
+    # end to end through the public API with host buffers
+    pin_D = torch.from_numpy(Dh).pin_memory()
+    pin_F = torch.zeros(ntri, dtype=torch.float64).pin_memory()
+    e2e_vals = []
+    if world == 1:
+        Fh = pin_F.numpy()
+        Dp = pin_D.numpy()
+        for s in range(args.warmup + args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            liberi.liberi_fock_build(h, Dp, Fh, ntri)  # host buffers, the handle's own stream
+            if s >= args.warmup:
+                e2e_vals.append(h.stats()["build_ms"])
+        e2e_ms = float(np.mean(e2e_vals))
+    else:
+        ev = []
+        barrier()
+        for s in range(args.warmup + args.steps):
+            flush.zero_()
+            a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            D.copy_(pin_D, non_blocking=True)
+            step()
+            pin_F.copy_(F, non_blocking=True)
+            b2.record(stream)
+            if s >= args.warmup:
+                ev.append((a, b2))
+        barrier()
+        e2e_ms = max_over_ranks(float(np.mean([a.elapsed_time(b2) for a, b2 in ev])))
+
+    # mixed precision at the serving cut, and the accuracy sweep of config 3
+    mixed = None
+    if not args.no_mixed:
+        h.set_option("precision", 1)
+        sweep = []
+        for cut in (1e-5, 1e-6, 1e-7, 1e-8):
+            h.set_option("fp32_cut", cut)
+            for _ in range(2):
+                step()
+            m_ms = max_over_ranks(timed_loop(max(3, args.steps // 2))[0])
+            dF = (F - F_fp64).abs().max().item()
+            dE = 0.5 * abs(float(torch.dot(F - F_fp64, _weights(D))))
+            sweep.append({"fp32_cut": cut, "ms": round(m_ms, 3), "speedup_vs_fp64": round(ms / m_ms, 3),
+                          "max_dF_vs_fp64": dF, "dE_vs_fp64": dE})
+        h.set_option("precision", 0)
+        mixed = {"reference_path": "plain FP64 GPU build (parity-tested against the oracle to 1e-10)",
+                 "sweep": sweep}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count()
+        cpu_ms, info = oracle_extrapolated_ms(basis, Dh, args.cpu_budget, nthreads=cores)
+        cpu = {"value": round(cpu_ms, 1), "unit": "ms", "cores": cores, "kind": "port",
+               "sample": "hashed uniform 1/%d sample of each class's screened quartets (%d of %d), "
+                         "%.1f s of CPU time, extrapolated per class by exact counts"
+                         % (info["sample_mod"], info["evaluated_quartets"], info["screened_quartets"],
+                            info["seconds"])}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded C60 geometry, 6-31G(d)-shaped exponents, D = 2CC^T)",
+                "config": config(world), "clocks": clocks,
+                "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 8 * ntri,
+                        "d2h_bytes_per_step": 8 * ntri},
+                "gpu_launches": launched * args.steps, "roofline": roofline, "cpu_baseline": cpu,
+                "mixed": mixed,
+                "quartets": int(st0["quartets"].sum()), "prim_quartets": int(st0["prim_quartets"].sum())}
+        if args.per_class:
+            line["per_class_ms"] = {liberi.KERNELS[k]: round(float(cls_ms[k]), 3) for k in range(21)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    liberi.liberi_destroy(h)
+    return 0
+
+
+def _weights(D):
+    import torch
+    n = int((np.sqrt(8 * D.numel() + 1) - 1) / 2)
+    w = torch.full_like(D, 2.0)
+    idx = torch.arange(1, n + 1, device=D.device)
+    w[idx * (idx + 1) // 2 - 1] = 1.0
+    return w * D
+
+
+def main():
+    args = parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -39,7 +39,7 @@ enum Tile { TILE_SQRT = 0, TILE_E9 = 1, TILE_E8 = 2, TILE_NONE = 3 };
 // One reference kernel (intABCD) and its screening / digestion behaviour.
 struct KernelDesc {
     const char *name;
-    int bra, ket;        // pair classes
+    int bra, ket;        // reference pair classes (bra, ket)
     bool tri;            // same-class triangle (kkll <= iijj)
     bool rys;            // generated Rys kernel (else rotated-axis)
     bool cross;          // pre-screen against the other class's maximum
@@ -48,7 +48,8 @@ struct KernelDesc {
     bool ketmajor;       // flat index runs bra-fastest (Rys product kernels)
     bool digest_schwarz; // digestion skip uses cutoff_schwarz (else eri_cut)
     double asym;         // asymptotic-root threshold (rot: T > 25; Rys: T >= x)
-    int la, lb, lc, ld;  // shell angular momenta in the engine's orientation
+    bool swap;           // engine rows = the reference's ket class (larger block)
+    int la, lb, lc, ld;  // engine orientation: rows (A,B), kets (C,D), L_A >= L_B
 };
 extern const KernelDesc KDESC[NKERN];
 
@@ -60,18 +61,18 @@ struct DevBasis {
     const int *pair_prim0;     // first primitive pair
     const int *pair_nprim;     // number of kept primitive pairs
     const double4 *prim_P;     // Px, Py, Pz, p
-    const double *prim_K;      // sqrt(2 pi^2.5) c_a c_b exp(-mu R^2) / p
+    const double2 *prim_X;     // sqrt(2 pi^2.5) c_a c_b exp(-mu R^2) / p, 0.5 / p
 };
 
+// One launch of a class: a list of CTA tasks (bra position, first ket
+// position, ket count) over the plan's sorted lists.
 struct DevPlan {
-    int nbra, nket;
     const int *bra_ids, *ket_ids;    // global pair ids, sorted by xint desc
     const int *bra_orig, *ket_orig;  // positions in the reference's compacted lists
-    const long long *pref;           // nbra+1 exclusive prefix of work items
-    long long total;
-    // fp32 split: items [pref[i], pref[i]+n64[i]) of bra i are FP64, the rest
-    // FP32.  n64 == nullptr means everything is FP64.
-    const int *split;                // per bra: first FP32 ket position
+    const int4 *tasks;
+    const int *ntasks_dev;           // task count on the device (per-build lists) or null
+    int ntasks;                      // static count, or capacity for per-build lists
+    bool swapped;
 };
 
 struct RankSplit {
@@ -86,20 +87,23 @@ struct RankSplit {
 struct PlanHost {
     int nbra = 0, nket = 0;
     std::vector<int> bra_ids, ket_ids, bra_orig, ket_orig, ncount;
+    std::vector<int4> items;  // (bra position, ket segment start, surviving count, -)
     std::vector<double> bra_x, ket_x;
     std::vector<long long> pref;
     long long total = 0;
     long long ntot_ref = 0;  // reference iteration count (rank split)
     int nbra_ref = 0, nket_ref = 0;
+    int chunk = 512;         // kets per CTA task
+    std::vector<int4> tasks; // static FP64 task list
+    int task_cap = 0;        // capacity of the per-build (mixed) lists
     // device copies
     int *d_bra = nullptr, *d_ket = nullptr, *d_bra_orig = nullptr, *d_ket_orig = nullptr;
-    long long *d_pref = nullptr;
     double *d_bra_x = nullptr, *d_ket_x = nullptr;
-    int *d_ncount = nullptr;
-    // mixed precision: per build
-    long long *d_pref64 = nullptr, *d_pref32 = nullptr;
-    int *d_split = nullptr;
-    long long total64 = 0, total32 = 0;
+    int4 *d_items = nullptr;
+    int4 *d_tasks = nullptr;
+    // mixed precision: per-build task lists
+    int4 *d_tasks64 = nullptr, *d_tasks32 = nullptr;
+    int *d_ntasks = nullptr;  // [0] fp64 count, [1] fp32 count, [2] fp32 quartets (lo), [3] (hi)
 };
 
 struct BasisHost {
@@ -115,8 +119,9 @@ struct PairsHost {
     std::vector<double> xint;
     std::vector<int2> shell;      // engine orientation
     std::vector<int> prim0, nprim;
+    std::vector<int> kab;         // contraction-pattern key K_a * K_b
     std::vector<double4> P;
-    std::vector<double> K;
+    std::vector<double2> X;
     int nl[3] = {0, 0, 0};
 };
 
@@ -126,7 +131,7 @@ struct DeviceBuffers {
     int2 *pair_shell = nullptr;
     int *pair_prim0 = nullptr, *pair_nprim = nullptr;
     double4 *prim_P = nullptr;
-    double *prim_K = nullptr;
+    double2 *prim_X = nullptr;
     double *D = nullptr, *F = nullptr;
     long long *scratch_total = nullptr;  // device counters (mixed split)
     size_t bytes = 0;
@@ -147,12 +152,12 @@ struct LaunchCtx {
 };
 
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
-                         int precision);  // precision 0: fp64 items, 1: fp32 items
+                         int precision, int nbf, int tile_rows);  // precision 0: FP64, 1: FP32
 cudaError_t launch_maxabs(const double *x, long long n, unsigned long long *out,
                           cudaStream_t stream);
-cudaError_t launch_split(int nbra, const double *bra_x, const double *ket_x, const int *ncount,
-                         const unsigned long long *maxd, double fp32_cut, int *split,
-                         long long *pref64, long long *pref32, cudaStream_t stream);
+cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_x, const double *ket_x,
+                               const unsigned long long *maxd, double fp32_cut, int chunk,
+                               int4 *tasks64, int4 *tasks32, int *counts, cudaStream_t stream);
 cudaError_t launch_schwarz(int pair_class, int npairs, int pair_off, const DevBasis &b,
                            const double *rys_tab, double *out_per_pair, cudaStream_t stream);
 

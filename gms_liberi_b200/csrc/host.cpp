@@ -30,34 +30,50 @@ namespace liberi {
 // (int0001.F90:117 bra-major, int2211_rysgen.F90:351 bra-fastest), digestion
 // cut (cutoff_schwarz int0000.F90:246, literal 5e-11 int0002.F90:403) and
 // asymptotic thresholds (t_max=25, Rys 43/49/55).
+// Engine orientation: the "rows" pair (A,B) is the class with the larger
+// Cartesian block (its rows of F are staged in shared memory), the kets (C,D)
+// the smaller; `swap` marks classes whose rows are the reference's ket list.
 const KernelDesc KDESC[NKERN] = {
-    {"int0000", SS, SS, true, false, false, OP_GE, TILE_SQRT, false, true, 25.0, 0, 0, 0, 0},
-    {"int0001", SS, SP, false, false, true, OP_GT, TILE_E9, false, true, 25.0, 0, 0, 1, 0},
-    {"int0011", SS, PP, false, false, true, OP_GT, TILE_E9, false, true, 25.0, 0, 0, 1, 1},
-    {"int0111", SP, PP, false, false, true, OP_GT, TILE_E9, false, false, 25.0, 1, 0, 1, 1},
-    {"int0101", SP, SP, true, false, false, OP_GE, TILE_NONE, false, false, 25.0, 1, 0, 1, 0},
-    {"int1111", PP, PP, true, false, false, OP_GE, TILE_NONE, false, true, 25.0, 1, 1, 1, 1},
-    {"int0002", SS, SD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 0, 0, 2, 0},
-    {"int0012", SS, PD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 0, 0, 2, 1},
-    {"int0102", SP, SD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 1, 0, 2, 0},
-    {"int0112", SP, PD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 1, 0, 2, 1},
-    {"int0022", SS, DD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 0, 0, 2, 2},
-    {"int0122", SP, DD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 1, 0, 2, 2},
-    {"int1102", PP, SD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, 1, 1, 2, 0},
-    {"int0202", SD, SD, true, false, false, OP_GT, TILE_NONE, false, false, 25.0, 2, 0, 2, 0},
-    {"int2211", DD, PP, false, true, false, OP_GT, TILE_E8, true, false, 49.0, 2, 2, 1, 1},
-    {"int2121", PD, PD, true, true, false, OP_GT, TILE_NONE, false, false, 49.0, 2, 1, 2, 1},
-    {"int2120", PD, SD, false, true, false, OP_GT, TILE_E8, true, false, 43.0, 2, 1, 2, 0},
-    {"int2111", PD, PP, false, true, false, OP_GT, TILE_E8, true, false, 43.0, 2, 1, 1, 1},
-    {"int2220", DD, SD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, 2, 2, 2, 0},
-    {"int2221", DD, PD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, 2, 2, 2, 1},
-    {"int2222", DD, DD, true, true, false, OP_NONE, TILE_NONE, false, false, 55.0, 2, 2, 2, 2},
+    //  name      bra ket  tri    rys    cross  op      tile       kmaj   dsch   asym  swap   la lb lc ld
+    {"int0000", SS, SS, true, false, false, OP_GE, TILE_SQRT, false, true, 25.0, false, 0, 0, 0, 0},
+    {"int0001", SS, SP, false, false, true, OP_GT, TILE_E9, false, true, 25.0, true, 1, 0, 0, 0},
+    {"int0011", SS, PP, false, false, true, OP_GT, TILE_E9, false, true, 25.0, true, 1, 1, 0, 0},
+    {"int0111", SP, PP, false, false, true, OP_GT, TILE_E9, false, false, 25.0, true, 1, 1, 1, 0},
+    {"int0101", SP, SP, true, false, false, OP_GE, TILE_NONE, false, false, 25.0, false, 1, 0, 1, 0},
+    {"int1111", PP, PP, true, false, false, OP_GE, TILE_NONE, false, true, 25.0, false, 1, 1, 1, 1},
+    {"int0002", SS, SD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, true, 2, 0, 0, 0},
+    {"int0012", SS, PD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, true, 2, 1, 0, 0},
+    {"int0102", SP, SD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, true, 2, 0, 1, 0},
+    {"int0112", SP, PD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, true, 2, 1, 1, 0},
+    {"int0022", SS, DD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, true, 2, 2, 0, 0},
+    {"int0122", SP, DD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, true, 2, 2, 1, 0},
+    {"int1102", PP, SD, false, false, true, OP_GT, TILE_E8, false, false, 25.0, false, 1, 1, 2, 0},
+    {"int0202", SD, SD, true, false, false, OP_GT, TILE_NONE, false, false, 25.0, false, 2, 0, 2, 0},
+    {"int2211", DD, PP, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 2, 2, 1, 1},
+    {"int2121", PD, PD, true, true, false, OP_GT, TILE_NONE, false, false, 49.0, false, 2, 1, 2, 1},
+    {"int2120", PD, SD, false, true, false, OP_GT, TILE_E8, true, false, 43.0, false, 2, 1, 2, 0},
+    {"int2111", PD, PP, false, true, false, OP_GT, TILE_E8, true, false, 43.0, false, 2, 1, 1, 1},
+    {"int2220", DD, SD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 2, 2, 2, 0},
+    {"int2221", DD, PD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 2, 2, 2, 1},
+    {"int2222", DD, DD, true, true, false, OP_NONE, TILE_NONE, false, false, 55.0, false, 2, 2, 2, 2},
 };
 
 static const int PC_L1[NPC] = {0, 0, 1, 0, 1, 2};  // reference pair order (first, second)
 static const int PC_L2[NPC] = {0, 1, 1, 2, 2, 2};
 static const double CUX = 50.0;                    // src/liberi_parameters.F90:44
 static const double SQRT_TWOPI52 = 5.9149671727956128778;  // sqrt(2 pi^(5/2))
+static const size_t TILE_MAX_BYTES = 160 * 1024;            // shared-memory F rows per CTA
+static const int CLASS_CTA_THREADS = 128;
+
+static int ncart_l(int l) { return (l + 1) * (l + 2) / 2; }
+
+// default kets per CTA task (the autotuner may override per class)
+static int default_chunk(int k) {
+    const KernelDesc &d = KDESC[k];
+    const int nc = ncart_l(d.la) * ncart_l(d.lb) * ncart_l(d.lc) * ncart_l(d.ld);
+    const int qpt = nc >= 216 ? 1 : (nc >= 54 ? 2 : 4);
+    return CLASS_CTA_THREADS * qpt;
+}
 
 }  // namespace liberi
 
@@ -93,6 +109,7 @@ struct liberi_handle_s {
     int precision = 0;
     int device = 0;
     uint32_t class_mask = (1u << NKERN) - 1;
+    int chunk[NKERN] = {};  // kets per CTA task per class (0 = default)
     bool timing = false;
     cudaEvent_t ev[NKERN + 1][2] = {};
     bool ev_recorded[NKERN] = {};
@@ -169,6 +186,8 @@ static int validate_basis(const BasisHost &b) {
     }
     for (double x : b.schwrz)
         if (!(x >= 0.0)) return fail(LIBERI_E_ARG, "liberi_setup: negative or NaN Schwarz value");
+    if (b.num_bas > 46340)  // packed indices are 32-bit on the device
+        return fail(LIBERI_E_UNSUPPORTED, "liberi_setup: num_bas %d exceeds 46340", b.num_bas);
     return LIBERI_OK;
 }
 
@@ -201,7 +220,8 @@ static void build_pairs(const BasisHost &b, PairsHost &pr, std::vector<double4> 
                 int A = is, B = js;
                 if (l2 > l1) std::swap(A, B);
                 pr.shell.push_back(make_int2(A, B));
-                pr.prim0.push_back((int)pr.K.size());
+                pr.prim0.push_back((int)pr.X.size());
+                pr.kab.push_back(b.contr_num[is] * b.contr_num[js]);
                 double r2 = 0.0;
                 for (int x = 0; x < 3; x++) {
                     double d = b.coords[3 * (b.atom_num[js] - 1) + x] - b.coords[3 * (b.atom_num[is] - 1) + x];
@@ -223,7 +243,7 @@ static void build_pairs(const BasisHost &b, PairsHost &pr, std::vector<double4> 
                         if (mur2 > CUX) continue;
                         pr.P.push_back(make_double4((a * RA.x + bb * RB.x) * ip, (a * RA.y + bb * RB.y) * ip,
                                                     (a * RA.z + bb * RB.z) * ip, p));
-                        pr.K.push_back(SQRT_TWOPI52 * ca * cb * std::exp(-mur2) * ip);
+                        pr.X.push_back(make_double2(SQRT_TWOPI52 * ca * cb * std::exp(-mur2) * ip, 0.5 * ip));
                         kept++;
                     }
                 }
@@ -241,9 +261,10 @@ static double class_max(const PairsHost &pr, int c) {
     return m;
 }
 
-static void build_plan(const PairsHost &pr, int k, double cut, PlanHost &ph) {
+static void build_plan(const PairsHost &pr, int k, double cut, int chunk, PlanHost &ph) {
     const KernelDesc &kd = KDESC[k];
     ph = PlanHost();
+    ph.chunk = chunk;
     const int nb_all = pr.class_off[kd.bra + 1] - pr.class_off[kd.bra];
     const int nk_all = pr.class_off[kd.ket + 1] - pr.class_off[kd.ket];
     if (nb_all == 0 || nk_all == 0) return;
@@ -260,11 +281,21 @@ static void build_plan(const PairsHost &pr, int k, double cut, PlanHost &ph) {
     ph.nbra_ref = (int)lb.size();
     ph.nket_ref = (int)lk.size();
     ph.ntot_ref = kd.tri ? (long long)lb.size() : (long long)lb.size() * (long long)lk.size();
+    // engine rows: the reference's ket list for swapped classes (the
+    // surviving partners of any element still form a prefix of the other
+    // Schwarz-sorted list, and the quartet set is symmetric)
+    if (kd.swap) std::swap(lb, lk);
     auto sorted = [&](const std::vector<int> &l, std::vector<int> &ids, std::vector<int> &orig,
                       std::vector<double> &x) {
         std::vector<int> ord(l.size());
         std::iota(ord.begin(), ord.end(), 0);
-        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return pr.xint[l[a]] > pr.xint[l[b]]; });
+        // contraction-pattern groups (uniform primitive loops per CTA), each
+        // sorted by Schwarz value: the partners of any pair are a prefix of
+        // every group
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+            if (pr.kab[l[a]] != pr.kab[l[b]]) return pr.kab[l[a]] > pr.kab[l[b]];
+            return pr.xint[l[a]] > pr.xint[l[b]];
+        });
         for (int o : ord) {
             ids.push_back(l[o]);
             orig.push_back(o);
@@ -275,24 +306,46 @@ static void build_plan(const PairsHost &pr, int k, double cut, PlanHost &ph) {
     sorted(lk, ph.ket_ids, ph.ket_orig, ph.ket_x);
     ph.nbra = (int)ph.bra_ids.size();
     ph.nket = (int)ph.ket_ids.size();
-    ph.ncount.resize(ph.nbra);
+    ph.ncount.assign(ph.nbra, 0);
     ph.pref.assign(ph.nbra + 1, 0);
+    // ket segments of equal contraction pattern
+    std::vector<int> seg{0};
+    for (int j = 1; j < ph.nket; j++)
+        if (pr.kab[ph.ket_ids[j]] != pr.kab[ph.ket_ids[j - 1]]) seg.push_back(j);
+    seg.push_back(ph.nket);
+    ph.items.clear();
     for (int i = 0; i < ph.nbra; i++) {
         const double xb = ph.bra_x[i];
-        // surviving kets form a prefix of the descending ket list
-        int lo = 0, hi = ph.nket;
-        while (lo < hi) {
-            int mid = (lo + hi) / 2;
-            double t = xb * ph.ket_x[mid];
-            bool pass = kd.op == OP_GE ? (t >= cut) : (kd.op == OP_GT ? (t > cut) : true);
-            if (pass) lo = mid + 1; else hi = mid;
+        int n_i = 0;
+        for (size_t g = 0; g + 1 < seg.size(); g++) {
+            const int s = seg[g], e = seg[g + 1];
+            if (kd.tri && s > i) break;  // triangle: partners at positions <= i
+            int lo = s, hi = e;
+            while (lo < hi) {
+                int mid = (lo + hi) / 2;
+                double t = xb * ph.ket_x[mid];
+                bool pass = kd.op == OP_GE ? (t >= cut) : (kd.op == OP_GT ? (t > cut) : true);
+                if (pass) lo = mid + 1; else hi = mid;
+            }
+            int n = lo - s;
+            if (kd.tri) n = std::min(n, i - s + 1);
+            if (n > 0) {
+                ph.items.push_back(make_int4(i, s, n, 0));
+                n_i += n;
+            }
         }
-        int n = lo;
-        if (kd.tri) n = std::min(n, i + 1);
-        ph.ncount[i] = n;
-        ph.pref[i + 1] = ph.pref[i] + n;
+        ph.ncount[i] = n_i;
+        ph.pref[i + 1] = ph.pref[i] + n_i;
     }
     ph.total = ph.pref[ph.nbra];
+    if (ph.chunk <= 0) ph.chunk = default_chunk(k);
+    ph.tasks.clear();
+    ph.task_cap = 0;
+    for (const int4 &it : ph.items) {
+        for (int k0 = 0; k0 < it.z; k0 += ph.chunk)
+            ph.tasks.push_back(make_int4(it.x, it.y + k0, std::min(ph.chunk, it.z - k0), 0));
+        ph.task_cap += (it.z + ph.chunk - 1) / ph.chunk + 1;
+    }
 }
 
 static int upload_plans(liberi_handle h) {
@@ -303,13 +356,13 @@ static int upload_plans(liberi_handle h) {
         CUDA_TRY(dev_upload(h, &ph.d_ket, ph.ket_ids.data(), ph.ket_ids.size()));
         CUDA_TRY(dev_upload(h, &ph.d_bra_orig, ph.bra_orig.data(), ph.bra_orig.size()));
         CUDA_TRY(dev_upload(h, &ph.d_ket_orig, ph.ket_orig.data(), ph.ket_orig.size()));
-        CUDA_TRY(dev_upload(h, &ph.d_pref, ph.pref.data(), ph.pref.size()));
         CUDA_TRY(dev_upload(h, &ph.d_bra_x, ph.bra_x.data(), ph.bra_x.size()));
         CUDA_TRY(dev_upload(h, &ph.d_ket_x, ph.ket_x.data(), ph.ket_x.size()));
-        CUDA_TRY(dev_upload(h, &ph.d_ncount, ph.ncount.data(), ph.ncount.size()));
-        CUDA_TRY(dev_alloc(h, &ph.d_pref64, ph.pref.size()));
-        CUDA_TRY(dev_alloc(h, &ph.d_pref32, ph.pref.size()));
-        CUDA_TRY(dev_alloc(h, &ph.d_split, ph.ncount.size()));
+        CUDA_TRY(dev_upload(h, &ph.d_items, ph.items.data(), ph.items.size()));
+        CUDA_TRY(dev_upload(h, &ph.d_tasks, ph.tasks.data(), ph.tasks.size()));
+        CUDA_TRY(dev_alloc(h, &ph.d_tasks64, (size_t)ph.task_cap));
+        CUDA_TRY(dev_alloc(h, &ph.d_tasks32, (size_t)ph.task_cap));
+        CUDA_TRY(dev_alloc(h, &ph.d_ntasks, 4));
     }
     return LIBERI_OK;
 }
@@ -322,7 +375,8 @@ static void compute_stats(liberi_handle h) {
         std::vector<long long> kp(ph.nket + 1, 0);
         for (int j = 0; j < ph.nket; j++) kp[j + 1] = kp[j] + h->pairs.nprim[ph.ket_ids[j]];
         long long s = 0;
-        for (int i = 0; i < ph.nbra; i++) s += (long long)h->pairs.nprim[ph.bra_ids[i]] * kp[ph.ncount[i]];
+        for (const int4 &it : ph.items)
+            s += (long long)h->pairs.nprim[ph.bra_ids[it.x]] * (kp[it.y + it.z] - kp[it.y]);
         h->stats.prim_quartets[k] = s;
     }
 }
@@ -370,7 +424,7 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
     CUDA_TRY(dev_upload(h, &h->dev.pair_prim0, h->pairs.prim0.data(), h->pairs.prim0.size()));
     CUDA_TRY(dev_upload(h, &h->dev.pair_nprim, h->pairs.nprim.data(), h->pairs.nprim.size()));
     CUDA_TRY(dev_upload(h, &h->dev.prim_P, h->pairs.P.data(), h->pairs.P.size()));
-    CUDA_TRY(dev_upload(h, &h->dev.prim_K, h->pairs.K.data(), h->pairs.K.size()));
+    CUDA_TRY(dev_upload(h, &h->dev.prim_X, h->pairs.X.data(), h->pairs.X.size()));
     const std::vector<double> &tab = rys_table_host();
     CUDA_TRY(dev_upload(h, &h->d_tab, tab.data(), tab.size()));
     const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
@@ -388,7 +442,7 @@ static DevBasis dev_basis(liberi_handle h) {
     d.pair_prim0 = h->dev.pair_prim0;
     d.pair_nprim = h->dev.pair_nprim;
     d.prim_P = h->dev.prim_P;
-    d.prim_K = h->dev.prim_K;
+    d.prim_X = h->dev.prim_X;
     return d;
 }
 
@@ -397,8 +451,8 @@ static int replan(liberi_handle h) {
     for (int k = 0; k < NKERN; k++) {
         PlanHost &ph = h->plan[k];
         for (void *p : {(void *)ph.d_bra, (void *)ph.d_ket, (void *)ph.d_bra_orig, (void *)ph.d_ket_orig,
-                        (void *)ph.d_pref, (void *)ph.d_bra_x, (void *)ph.d_ket_x, (void *)ph.d_ncount,
-                        (void *)ph.d_pref64, (void *)ph.d_pref32, (void *)ph.d_split}) {
+                        (void *)ph.d_bra_x, (void *)ph.d_ket_x, (void *)ph.d_items, (void *)ph.d_tasks,
+                        (void *)ph.d_tasks64, (void *)ph.d_tasks32, (void *)ph.d_ntasks}) {
             if (!p) continue;
             cudaFree(p);
             h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), p), h->allocs.end());
@@ -410,7 +464,7 @@ static int replan(liberi_handle h) {
         bool run = (k == 0 && h->pairs.nl[0] > 0) || (k >= 1 && k <= 5 && h->pairs.nl[1] > 0) ||
                    (k >= 6 && h->pairs.nl[2] > 0);
         (void)kd;
-        if (run) build_plan(h->pairs, k, h->schwarz_cut, h->plan[k]);
+        if (run) build_plan(h->pairs, k, h->schwarz_cut, h->chunk[k], h->plan[k]);
         else h->plan[k] = PlanHost();
     }
     (void)b;
@@ -462,26 +516,29 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
         rs.tri = kd.tri;
         rs.ketmajor = kd.ketmajor;
         DevPlan dp;
-        dp.nbra = ph.nbra;
-        dp.nket = ph.nket;
         dp.bra_ids = ph.d_bra;
         dp.ket_ids = ph.d_ket;
         dp.bra_orig = ph.d_bra_orig;
         dp.ket_orig = ph.d_ket_orig;
-        dp.total = ph.total;
+        dp.swapped = kd.swap;
+        const int nbf = b.num_bas;
+        const size_t tile_bytes = (size_t)(ncart_l(kd.la) + ncart_l(kd.lb)) * nbf * sizeof(double);
+        const int tile_rows = tile_bytes <= TILE_MAX_BYTES ? 1 : 0;
         if (!mixed) {
-            dp.pref = ph.d_pref;
-            dp.split = nullptr;
-            CUDA_TRY(launch_class(k, ctx, dp, rs, 0));
+            dp.tasks = ph.d_tasks;
+            dp.ntasks_dev = nullptr;
+            dp.ntasks = (int)ph.tasks.size();
+            CUDA_TRY(launch_class(k, ctx, dp, rs, 0, nbf, tile_rows));
         } else {
-            CUDA_TRY(launch_split(ph.nbra, ph.d_bra_x, ph.d_ket_x, ph.d_ncount, h->d_maxd, h->fp32_cut,
-                                  ph.d_split, ph.d_pref64, ph.d_pref32, st));
-            dp.pref = ph.d_pref64;
-            dp.split = nullptr;
-            CUDA_TRY(launch_class(k, ctx, dp, rs, 0));
-            dp.pref = ph.d_pref32;
-            dp.split = ph.d_split;
-            CUDA_TRY(launch_class(k, ctx, dp, rs, 1));
+            CUDA_TRY(launch_split_tasks((int)ph.items.size(), ph.d_items, ph.d_bra_x, ph.d_ket_x, h->d_maxd,
+                                        h->fp32_cut, ph.chunk, ph.d_tasks64, ph.d_tasks32, ph.d_ntasks, st));
+            dp.ntasks = ph.task_cap;
+            dp.tasks = ph.d_tasks64;
+            dp.ntasks_dev = ph.d_ntasks;
+            CUDA_TRY(launch_class(k, ctx, dp, rs, 0, nbf, tile_rows));
+            dp.tasks = ph.d_tasks32;
+            dp.ntasks_dev = ph.d_ntasks + 1;
+            CUDA_TRY(launch_class(k, ctx, dp, rs, 1, nbf, tile_rows));
         }
         if (h->timing) {
             CUDA_TRY(cudaEventRecord(h->ev[k][1], st));
@@ -686,6 +743,14 @@ int liberi_c_get_option(liberi_handle h, const char *name, double *value) {
 
 int liberi_c_get_stats(liberi_handle h, liberi_stats *stats) {
     if (!h || !stats) return fail(LIBERI_E_ARG, "liberi_get_stats: null argument");
+    for (int k = 0; k < NKERN; k++) {
+        h->stats.fp32_quartets[k] = 0;
+        if (h->initialized && h->precision == 1 && h->plan[k].d_ntasks) {
+            int cnt[4] = {0, 0, 0, 0};
+            if (cudaMemcpy(cnt, h->plan[k].d_ntasks, sizeof(cnt), cudaMemcpyDeviceToHost) == cudaSuccess)
+                h->stats.fp32_quartets[k] = (int64_t)(unsigned)cnt[2] | ((int64_t)(unsigned)cnt[3] << 32);
+        }
+    }
     for (int k = 0; k < NKERN; k++) {
         h->stats.kernel_ms[k] = 0.0;
         if (h->timing && h->ev_recorded[k]) {

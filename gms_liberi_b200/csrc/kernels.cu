@@ -1,115 +1,105 @@
-// kernels.cu -- class dispatch, Schwarz generator and mixed-precision split
-// kernels of the Fock-build engine; the class kernels themselves are
+// kernels.cu -- class dispatch, Schwarz generator and mixed-precision task
+// builder of the Fock-build engine; the class kernels themselves are
 // instantiated in k_*.cu from quartet.cuh.
 #include "quartet.cuh"
 
 namespace liberi {
 
-extern template cudaError_t launch_t<0, 0, 0, 0>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<0, 0, 1, 0>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<0, 0, 1, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<1, 0, 1, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<1, 0, 1, 0>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<1, 1, 1, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<0, 0, 2, 0>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<0, 0, 2, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<1, 0, 2, 0>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<1, 0, 2, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<0, 0, 2, 2>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<1, 0, 2, 2>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<1, 1, 2, 0>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<2, 0, 2, 0>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<2, 2, 1, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<2, 1, 2, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<2, 1, 2, 0>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<2, 1, 1, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<2, 2, 2, 0>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<2, 2, 2, 1>(const ClassArgs &, long long, int, int, cudaStream_t);
-extern template cudaError_t launch_t<2, 2, 2, 2>(const ClassArgs &, long long, int, int, cudaStream_t);
+#define LIBERI_CLASSES(X)                                                                    \
+    X(0, 0, 0, 0, 0) X(1, 1, 0, 0, 0) X(2, 1, 1, 0, 0) X(3, 1, 1, 1, 0) X(4, 1, 0, 1, 0)         \
+    X(5, 1, 1, 1, 1) X(6, 2, 0, 0, 0) X(7, 2, 1, 0, 0) X(8, 2, 0, 1, 0) X(9, 2, 1, 1, 0)         \
+    X(10, 2, 2, 0, 0) X(11, 2, 2, 1, 0) X(12, 1, 1, 2, 0) X(13, 2, 0, 2, 0) X(14, 2, 2, 1, 1)    \
+    X(15, 2, 1, 2, 1) X(16, 2, 1, 2, 0) X(17, 2, 1, 1, 1) X(18, 2, 2, 2, 0) X(19, 2, 2, 2, 1)    \
+    X(20, 2, 2, 2, 2)
+
+#define LIBERI_EXTERN(k, a, b, c, d) \
+    extern template cudaError_t launch_t<a, b, c, d>(const ClassArgs &, int, cudaStream_t);
+LIBERI_CLASSES(LIBERI_EXTERN)
 
 // Schwarz table: sqrt(max |(ab|ab)|) per pair of one class
 template <int LA, int LB>
 __global__ void __launch_bounds__(64) schwarz_kernel(DevBasis b, int pair_off, int npairs,
                                                      const double *tab, double *out) {
-    using Q = Quartet<LA, LB, LA, LB, double>;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= npairs) return;
-    int P = pair_off + t;
-    double acc[Q::NCART];
-    Q::eval(b, P, P, RYS_TMAX, false, tab, acc);
-    double m = 0.0;
-    for (int ia = 0; ia < Q::NA; ia++)
-        for (int ib = 0; ib < Q::NB; ib++) {
-            double v = fabs(acc[((ia * Q::NB + ib) * Q::NA + ia) * Q::NB + ib]);
-            int n3 = 2 * (cs3(LA, ia) + cs3(LB, ib));
-            if (n3 == 2) v *= 3.0; else if (n3 == 4) v *= 9.0;
-            m = v > m ? v : m;
-        }
-    out[t] = sqrt(m);
+    out[t] = schwarz_diag<LA, LB>(b, pair_off + t, tab);
 }
 
-// ---- mixed-precision split --------------------------------------------------------
 __global__ void maxabs_kernel(const double *x, long long n, unsigned long long *out) {
     double m = 0.0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
         m = fmax(m, fabs(x[i]));
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, __double_as_longlong(m));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
-// per bra: split = #kets (of its prefix) with x_bra*x_ket*max|D| >= fp32_cut,
-// then exclusive scans of the FP64 and FP32 counts (one CTA per plan)
-__global__ void __launch_bounds__(1024) split_kernel(int nbra, const double *bra_x,
-                                                     const double *ket_x, const int *ncount,
-                                                     const unsigned long long *maxd_bits,
-                                                     double fp32_cut, int *split,
-                                                     long long *pref64, long long *pref32) {
-    __shared__ long long s64[1024], s32[1024];
+// Per plan item (bra, ket segment, surviving count): split = number of its
+// kets with x_bra*x_ket*max|D| >= fp32_cut (a prefix, the segment is sorted
+// by x); FP64 tasks cover [0, split), FP32 tasks [split, count).  One CTA
+// builds both task lists; counts[0..1] are the task counts, counts[2..3] the
+// FP32 quartet count (low, high word).
+__device__ __forceinline__ int item_split(const int4 &it, const double *bra_x, const double *ket_x, double maxd,
+                                          double fp32_cut) {
+    const double xb = bra_x[it.x];
+    int lo = 0, hi = it.z;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (xb * ket_x[it.y + mid] * maxd >= fp32_cut) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(1024) split_tasks_kernel(int nitems, const int4 *items, const double *bra_x,
+                                                           const double *ket_x, const unsigned long long *maxd_bits,
+                                                           double fp32_cut, int chunk, int4 *tasks64,
+                                                           int4 *tasks32, int *counts) {
+    __shared__ int s64[1024], s32[1024];
+    __shared__ unsigned long long sq32[1024];
     const double maxd = __longlong_as_double((long long)*maxd_bits);
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int per = (nbra + nt - 1) / nt;
-    const int i0 = tid * per, i1 = min(nbra, i0 + per);
-    long long c64 = 0, c32 = 0;
+    const int per = (nitems + nt - 1) / nt;
+    const int i0 = min(nitems, tid * per), i1 = min(nitems, i0 + per);
+    int c64 = 0, c32 = 0;
+    unsigned long long q32 = 0;
     for (int i = i0; i < i1; i++) {
-        const int n = ncount[i];
-        const double xb = bra_x[i];
-        int lo = 0, hi = n;  // first position failing the FP64 test
-        while (lo < hi) {
-            int mid = (lo + hi) >> 1;
-            if (xb * ket_x[mid] * maxd >= fp32_cut) lo = mid + 1; else hi = mid;
-        }
-        split[i] = lo;
-        c64 += lo;
-        c32 += n - lo;
+        const int4 it = items[i];
+        const int s = item_split(it, bra_x, ket_x, maxd, fp32_cut);
+        c64 += (s + chunk - 1) / chunk;
+        c32 += (it.z - s + chunk - 1) / chunk;
+        q32 += (unsigned long long)(it.z - s);
     }
     s64[tid] = c64;
     s32[tid] = c32;
+    sq32[tid] = q32;
     __syncthreads();
     for (int off = 1; off < nt; off <<= 1) {
-        long long a = tid >= off ? s64[tid - off] : 0, b2 = tid >= off ? s32[tid - off] : 0;
+        int a = tid >= off ? s64[tid - off] : 0, b2 = tid >= off ? s32[tid - off] : 0;
+        unsigned long long c = tid >= off ? sq32[tid - off] : 0ull;
         __syncthreads();
         s64[tid] += a;
         s32[tid] += b2;
+        sq32[tid] += c;
         __syncthreads();
     }
-    long long r64 = tid > 0 ? s64[tid - 1] : 0, r32 = tid > 0 ? s32[tid - 1] : 0;
+    int o64 = tid > 0 ? s64[tid - 1] : 0, o32 = tid > 0 ? s32[tid - 1] : 0;
     for (int i = i0; i < i1; i++) {
-        pref64[i] = r64;
-        pref32[i] = r32;
-        r64 += split[i];
-        r32 += ncount[i] - split[i];
+        const int4 it = items[i];
+        const int s = item_split(it, bra_x, ket_x, maxd, fp32_cut);
+        for (int k = 0; k < s; k += chunk) tasks64[o64++] = make_int4(it.x, it.y + k, min(chunk, s - k), 0);
+        for (int k = s; k < it.z; k += chunk) tasks32[o32++] = make_int4(it.x, it.y + k, min(chunk, it.z - k), 0);
     }
     if (tid == nt - 1) {
-        pref64[nbra] = s64[nt - 1];
-        pref32[nbra] = s32[nt - 1];
+        counts[0] = s64[nt - 1];
+        counts[1] = s32[nt - 1];
+        counts[2] = (int)(sq32[nt - 1] & 0xffffffffull);
+        counts[3] = (int)(sq32[nt - 1] >> 32);
     }
 }
 
 // ---- launchers -------------------------------------------------------------------
-
-cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
-                         int precision) {
+cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs, int precision,
+                         int nbf, int tile_rows) {
     const KernelDesc &kd = KDESC[k];
     ClassArgs a;
     a.b = ctx.basis;
@@ -119,43 +109,26 @@ cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const
     a.cut = kd.digest_schwarz ? ctx.schwarz_cut : ctx.eri_cut;
     a.thr = kd.asym;
     a.strict = !kd.rys;
-    a.nbra = plan.nbra;
+    a.tasks = plan.tasks;
+    a.ntasks_dev = plan.ntasks_dev;
+    a.ntasks = plan.ntasks;
+    a.nbf = nbf;
+    a.tile_rows = tile_rows;
     a.bra_ids = plan.bra_ids;
     a.ket_ids = plan.ket_ids;
     a.bra_orig = plan.bra_orig;
     a.ket_orig = plan.ket_orig;
-    a.pref = plan.pref;
-    a.koff = plan.split;
+    a.swapped = plan.swapped ? 1 : 0;
     a.rs = rs;
-    const long long w = plan.total;
-    switch (k) {
-        case 0: return launch_t<0, 0, 0, 0>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 1: return launch_t<0, 0, 1, 0>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 2: return launch_t<0, 0, 1, 1>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 3: return launch_t<1, 0, 1, 1>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 4: return launch_t<1, 0, 1, 0>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 5: return launch_t<1, 1, 1, 1>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 6: return launch_t<0, 0, 2, 0>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 7: return launch_t<0, 0, 2, 1>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 8: return launch_t<1, 0, 2, 0>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 9: return launch_t<1, 0, 2, 1>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 10: return launch_t<0, 0, 2, 2>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 11: return launch_t<1, 0, 2, 2>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 12: return launch_t<1, 1, 2, 0>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 13: return launch_t<2, 0, 2, 0>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 14: return launch_t<2, 2, 1, 1>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 15: return launch_t<2, 1, 2, 1>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 16: return launch_t<2, 1, 2, 0>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 17: return launch_t<2, 1, 1, 1>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 18: return launch_t<2, 2, 2, 0>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 19: return launch_t<2, 2, 2, 1>(a, w, precision, ctx.num_sms, ctx.stream);
-        case 20: return launch_t<2, 2, 2, 2>(a, w, precision, ctx.num_sms, ctx.stream);
-    }
+#define LIBERI_CASE(kk, A, B, C, D) \
+    case kk: return launch_t<A, B, C, D>(a, precision, ctx.stream);
+    switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
+#undef LIBERI_CASE
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_schwarz(int pc, int npairs, int pair_off, const DevBasis &b,
-                           const double *tab, double *out, cudaStream_t st) {
+cudaError_t launch_schwarz(int pc, int npairs, int pair_off, const DevBasis &b, const double *tab, double *out,
+                           cudaStream_t st) {
     if (npairs <= 0) return cudaSuccess;
     const int threads = 64;
     const unsigned blocks = (unsigned)((npairs + threads - 1) / threads);
@@ -181,14 +154,13 @@ cudaError_t launch_maxabs(const double *x, long long n, unsigned long long *out,
     return cudaGetLastError();
 }
 
-cudaError_t launch_split(int nbra, const double *bra_x, const double *ket_x, const int *ncount,
-                         const unsigned long long *maxd, double fp32_cut, int *split,
-                         long long *pref64, long long *pref32, cudaStream_t st) {
-    if (nbra <= 0) return cudaSuccess;
-    split_kernel<<<1, 1024, 0, st>>>(nbra, bra_x, ket_x, ncount, maxd, fp32_cut, split, pref64,
-                                     pref32);
+cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_x, const double *ket_x,
+                               const unsigned long long *maxd, double fp32_cut, int chunk, int4 *tasks64,
+                               int4 *tasks32, int *counts, cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    split_tasks_kernel<<<1, 1024, 0, st>>>(nitems, items, bra_x, ket_x, maxd, fp32_cut, chunk, tasks64, tasks32,
+                                           counts);
     return cudaGetLastError();
 }
-
 
 }  // namespace liberi

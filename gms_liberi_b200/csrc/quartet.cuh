@@ -3,22 +3,27 @@
 //
 // One templated kernel per reference quartet class intABCD
 // (src/rhf/rot_axis/int*.F90, driver order src/liberi_driver.F90:69-102).
-// A thread owns one screened shell quartet (bra pair P, ket pair Q):
-//   1. decode the flat work index into (P, Q) from the class plan: bra pairs
-//      sorted by Schwarz value, per bra a prefix of the sorted ket list;
-//   2. loop over kept primitive pairs (ket outer, bra inner, as the
-//      reference does, e.g. int0001.F90:220-287), evaluate Rys roots and
-//      weights from the piecewise tables, build 2D integrals with the
-//      vertical and horizontal recurrences in registers and contract the
-//      Cartesian block;
-//   3. digest the block into the packed Fock matrix with the reference's
-//      DIRFCK rules (unique components for identical shells, 0.5 factors,
-//      skip |v| < cut, six updates; int0000.F90:241-311,
-//      int2222_rysgen.F90:11176-11338) using FP64 atomics.
-// The FP32 instantiation evaluates steps 2's recurrences and contraction in
-// single precision (roots, weights and pair prefactors stay FP64) for the
-// quartets whose Schwarz bound falls below the mixed-precision cut; its
-// integrals are digested into the same FP64 Fock matrix.
+//
+// Work unit: a CTA owns one "row" shell pair P = (A, B) and a chunk of its
+// surviving ket pairs Q = (C, D) (the kets of a bra form a prefix of the
+// Schwarz-sorted ket list).  Each thread evaluates whole quartets:
+//   1. loop over kept primitive pairs (ket outer, bra inner, as the reference
+//      does, e.g. int0001.F90:220-287), evaluate Rys roots and weights from
+//      the piecewise tables, build 2D integrals with the vertical and
+//      horizontal recurrences in registers and contract the Cartesian block;
+//      large classes run the primitive loop in register-bounded passes over
+//      the components of shell A;
+//   2. digest with the reference's DIRFCK rules (unique components for
+//      identical shells, 0.5 factors, skip |v| < cut, the six updates of
+//      int0000.F90:241-311 / int2222_rysgen.F90:11176-11338), pre-reduced in
+//      registers per quartet:
+//        K updates into rows A and B of F -> shared-memory tile of the CTA
+//        J update of the row pair (A,B)   -> warp-reduced, then the tile
+//        J update of the ket pair (C,D)   -> FP64 global atomics
+//      and the tile is flushed to F with FP64 atomics when the CTA ends.
+// The FP32 instantiation evaluates step 1 in single precision (roots,
+// weights and pair prefactors stay FP64) for the quartets whose Schwarz bound
+// falls below the mixed-precision cut; step 2 always accumulates in FP64.
 #pragma once
 #include <cstdio>
 
@@ -131,134 +136,239 @@ __device__ __forceinline__ void hrr(const R (&g)[LA + LB + 1][LC + LD + 1], R ab
 }
 
 // ---- contracted Cartesian block of one shell quartet -------------------------
-template <int LA, int LB, int LC, int LD, typename R>
-struct Quartet {
-    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    static constexpr int NCART = NA * NB * NC * ND;
-    static constexpr int LAB = LA + LB, LCD = LC + LD;
-    static constexpr int NR = (LAB + LCD) / 2 + 1;
+// Component tables as runtime values (used to select one A component).
+__device__ __forceinline__ int cx_rt(int l, int c) { return l == 0 ? 0 : (l == 1 ? (c == 0) : (c == 0 ? 2 : ((c == 3 || c == 4) ? 1 : 0))); }
+__device__ __forceinline__ int cy_rt(int l, int c) { return l == 0 ? 0 : (l == 1 ? (c == 1) : (c == 1 ? 2 : ((c == 3 || c == 5) ? 1 : 0))); }
+__device__ __forceinline__ int cz_rt(int l, int c) { return l == 0 ? 0 : (l == 1 ? (c == 2) : (c == 2 ? 2 : ((c == 4 || c == 5) ? 1 : 0))); }
 
-    __device__ __forceinline__ static int64_t eval(const DevBasis &b, int P, int Q, double thr,
-                                                    bool strict, const double *__restrict__ tab,
-                                                    R (&acc)[NCART]) {
-        const int2 sab = b.pair_shell[P], scd = b.pair_shell[Q];
-        const double4 A = b.shell_xyz[sab.x], B = b.shell_xyz[sab.y];
-        const double4 C = b.shell_xyz[scd.x], D = b.shell_xyz[scd.y];
-        const R abx = R(A.x - B.x), aby = R(A.y - B.y), abz = R(A.z - B.z);
-        const R cdx = R(C.x - D.x), cdy = R(C.y - D.y), cdz = R(C.z - D.z);
+// slice[b][c][d] = I[e][b][c][d] for a runtime e <= LA (register selects)
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void select_slice(const R (&I)[LA + 1][LB + 1][LC + 1][LD + 1], int e,
+                                             R (&s)[LB + 1][LC + 1][LD + 1]) {
 #pragma unroll
-        for (int i = 0; i < NCART; i++) acc[i] = R(0);
-        const int p0 = b.pair_prim0[P], np = b.pair_nprim[P];
-        const int q0 = b.pair_prim0[Q], nq = b.pair_nprim[Q];
-        for (int kq = q0; kq < q0 + nq; kq++) {
-            const double4 Qp = b.prim_P[kq];
-            const double Kq = b.prim_K[kq];
-            const double q = Qp.w;
-            const double hq = 0.5 / q;
-            for (int kp = p0; kp < p0 + np; kp++) {
-                const double4 Pp = b.prim_P[kp];
-                const double Kp = b.prim_K[kp];
-                const double p = Pp.w;
-                const double hp = 0.5 / p;
-                const double rs = rsqrt(p + q);
-                const double ipq = rs * rs;
-                const double pqx = Pp.x - Qp.x, pqy = Pp.y - Qp.y, pqz = Pp.z - Qp.z;
-                const double rho = p * q * ipq;
-                const double T = rho * (pqx * pqx + pqy * pqy + pqz * pqz);
-                double u[NR], w[NR];
-                rys_eval<NR>(T, thr, strict, tab, u, w);
-                const double pref = Kp * Kq * rs;
+    for (int b = 0; b <= LB; b++)
 #pragma unroll
-                for (int r = 0; r < NR; r++) {
-                    const double ui = u[r] * ipq;
-                    const double fq = q * ui, fp = p * ui;
-                    const R b00 = R(0.5 * ui);
-                    const R b10 = R(hp * (1.0 - fq));
-                    const R b01 = R(hq * (1.0 - fp));
-                    R gx[LAB + 1][LCD + 1], gy[LAB + 1][LCD + 1], gz[LAB + 1][LCD + 1];
-                    vrr<LAB, LCD, R>(gx, R((Pp.x - A.x) - fq * pqx), R((Qp.x - C.x) + fp * pqx),
-                                     b10, b01, b00, R(1));
-                    vrr<LAB, LCD, R>(gy, R((Pp.y - A.y) - fq * pqy), R((Qp.y - C.y) + fp * pqy),
-                                     b10, b01, b00, R(1));
-                    vrr<LAB, LCD, R>(gz, R((Pp.z - A.z) - fq * pqz), R((Qp.z - C.z) + fp * pqz),
-                                     b10, b01, b00, R(w[r] * pref));
-                    R ix[LA + 1][LB + 1][LC + 1][LD + 1], iy[LA + 1][LB + 1][LC + 1][LD + 1],
-                        iz[LA + 1][LB + 1][LC + 1][LD + 1];
-                    hrr<LA, LB, LC, LD, R>(gx, abx, cdx, ix);
-                    hrr<LA, LB, LC, LD, R>(gy, aby, cdy, iy);
-                    hrr<LA, LB, LC, LD, R>(gz, abz, cdz, iz);
-#pragma unroll(NCART > 81 ? 1 : NA)
-                    for (int ia = 0; ia < NA; ia++)
+        for (int c = 0; c <= LC; c++)
 #pragma unroll
-                        for (int ib = 0; ib < NB; ib++)
+            for (int d = 0; d <= LD; d++) {
+                R v = I[0][b][c][d];
 #pragma unroll
-                            for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-                                for (int id = 0; id < ND; id++) {
-                                    const int n = ((ia * NB + ib) * NC + ic) * ND + id;
-                                    acc[n] += ix[cxp(LA, ia)][cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)] *
-                                              iy[cyp(LA, ia)][cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)] *
-                                              iz[czp(LA, ia)][czp(LB, ib)][czp(LC, ic)][czp(LD, id)];
-                                }
-                }
+                for (int x = 1; x <= LA; x++) v = (e == x) ? I[x][b][c][d] : v;
+                s[b][c][d] = v;
             }
-        }
-        return (int64_t)np * nq;
-    }
-};
+}
 
-// ---- DIRFCK digestion ----------------------------------------------------------
-template <int LA, int LB, int LC, int LD, typename R>
-__device__ __forceinline__ void digest(const R *acc, int bfA, int bfB, int bfC, int bfD,
-                                       bool iandj, bool kandl, bool same, double cut,
-                                       const double *__restrict__ Dm, double *F) {
+// acc[m][ib][ic][id] for A components ia = mu0 + m (m < NMU, ia < NA), all of
+// B, C, D.  mu0 is a runtime value, so one copy of the primitive loop serves
+// every pass.
+template <int LA, int LB, int LC, int LD, typename R, int NMU>
+__device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, int q0, int nq,
+                                           const double4 &A, const double4 &C, R abx, R aby, R abz,
+                                           R cdx, R cdy, R cdz, double thr, bool strict,
+                                           const double *__restrict__ tab, int mu0,
+                                           R (&acc)[NMU][ncart(LB)][ncart(LC)][ncart(LD)]) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    constexpr bool can_same = (LA == LC) && (LB == LD);
-    const double s3 = 1.7320508075688772935;
-#pragma unroll(NA * NB * NC * ND > 81 ? 1 : NA)
-    for (int ia = 0; ia < NA; ia++)
+    constexpr int LAB = LA + LB, LCD = LC + LD;
+    constexpr int NR = (LAB + LCD) / 2 + 1;
+    constexpr bool FULL = (NMU == NA);  // one pass: compile-time components
+    int ex[NMU], ey[NMU], ez[NMU];
 #pragma unroll
-        for (int ib = 0; ib < NB; ib++) {
-            if (LA == LB && iandj && ib > ia) continue;
+    for (int m = 0; m < NMU; m++) {
+        const int ia = mu0 + m < NA ? mu0 + m : NA - 1;
+        ex[m] = cx_rt(LA, ia);
+        ey[m] = cy_rt(LA, ia);
+        ez[m] = cz_rt(LA, ia);
+    }
+#pragma unroll
+    for (int m = 0; m < NMU; m++)
+#pragma unroll
+        for (int ib = 0; ib < NB; ib++)
 #pragma unroll
             for (int ic = 0; ic < NC; ic++)
 #pragma unroll
-                for (int id = 0; id < ND; id++) {
-                    if (LC == LD && kandl && id > ic) continue;
-                    if (can_same && same) {
-                        const int oij = iandj ? ia * (ia + 1) / 2 + ib : ia * NB + ib;
-                        const int okl = kandl ? ic * (ic + 1) / 2 + id : ic * ND + id;
-                        if (okl > oij) continue;
+                for (int id = 0; id < ND; id++) acc[m][ib][ic][id] = R(0);
+    for (int kq = q0; kq < q0 + nq; kq++) {
+        const double4 Qp = b.prim_P[kq];
+        const double2 Qx = b.prim_X[kq];
+        const double q = Qp.w, hq = Qx.y;
+        for (int kp = p0; kp < p0 + np; kp++) {
+            const double4 Pp = b.prim_P[kp];
+            const double2 Px = b.prim_X[kp];
+            const double p = Pp.w, hp = Px.y;
+            const double rs = rsqrt(p + q);
+            const double ipq = rs * rs;
+            const double pqx = Pp.x - Qp.x, pqy = Pp.y - Qp.y, pqz = Pp.z - Qp.z;
+            const double T = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
+            double u[NR], w[NR];
+            rys_eval<NR>(T, thr, strict, tab, u, w);
+            const double pref = Px.x * Qx.x * rs;
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                const double ui = u[r] * ipq;
+                const double fq = q * ui, fp = p * ui;
+                const R b00 = R(0.5 * ui);
+                const R b10 = R(hp * (1.0 - fq));
+                const R b01 = R(hq * (1.0 - fp));
+                R gx[LAB + 1][LCD + 1], gy[LAB + 1][LCD + 1], gz[LAB + 1][LCD + 1];
+                vrr<LAB, LCD, R>(gx, R((Pp.x - A.x) - fq * pqx), R((Qp.x - C.x) + fp * pqx), b10, b01, b00, R(1));
+                vrr<LAB, LCD, R>(gy, R((Pp.y - A.y) - fq * pqy), R((Qp.y - C.y) + fp * pqy), b10, b01, b00, R(1));
+                vrr<LAB, LCD, R>(gz, R((Pp.z - A.z) - fq * pqz), R((Qp.z - C.z) + fp * pqz), b10, b01, b00,
+                                 R(w[r] * pref));
+                R ix[LA + 1][LB + 1][LC + 1][LD + 1], iy[LA + 1][LB + 1][LC + 1][LD + 1],
+                    iz[LA + 1][LB + 1][LC + 1][LD + 1];
+                hrr<LA, LB, LC, LD, R>(gx, abx, cdx, ix);
+                hrr<LA, LB, LC, LD, R>(gy, aby, cdy, iy);
+                hrr<LA, LB, LC, LD, R>(gz, abz, cdz, iz);
+#pragma unroll
+                for (int m = 0; m < NMU; m++) {
+                    R sx[LB + 1][LC + 1][LD + 1], sy[LB + 1][LC + 1][LD + 1], sz[LB + 1][LC + 1][LD + 1];
+                    if constexpr (FULL) {
+#pragma unroll
+                        for (int b2 = 0; b2 <= LB; b2++)
+#pragma unroll
+                            for (int c2 = 0; c2 <= LC; c2++)
+#pragma unroll
+                                for (int d2 = 0; d2 <= LD; d2++) {
+                                    sx[b2][c2][d2] = ix[cxp(LA, m)][b2][c2][d2];
+                                    sy[b2][c2][d2] = iy[cyp(LA, m)][b2][c2][d2];
+                                    sz[b2][c2][d2] = iz[czp(LA, m)][b2][c2][d2];
+                                }
+                    } else {
+                        select_slice<LA, LB, LC, LD, R>(ix, ex[m], sx);
+                        select_slice<LA, LB, LC, LD, R>(iy, ey[m], sy);
+                        select_slice<LA, LB, LC, LD, R>(iz, ez[m], sz);
                     }
-                    const int n3 = cs3(LA, ia) + cs3(LB, ib) + cs3(LC, ic) + cs3(LD, id);
-                    double v = (double)acc[((ia * NB + ib) * NC + ic) * ND + id];
-                    if (n3 == 1) v *= s3;
-                    else if (n3 == 2) v *= 3.0;
-                    else if (n3 == 3) v *= 3.0 * s3;
-                    else if (n3 == 4) v *= 9.0;
-                    if (fabs(v) < cut) continue;
-                    long long i1 = bfA + ia + 1, j1 = bfB + ib + 1, k1 = bfC + ic + 1, l1 = bfD + id + 1;
-                    long long i2 = i1, j2 = j1, k2 = k1, l2 = l1;
-                    if (i1 < j1) { i2 = j1; j2 = i1; }
-                    if (k1 < l1) { k2 = l1; l2 = k1; }
-                    long long ii = i2, jj = j2, kk = k2, ll = l2;
-                    if (ii < kk) { ii = k2; jj = l2; kk = i2; ll = j2; }
-                    else if (ii == kk && jj < ll) { jj = l2; ll = j2; }
-                    if (ii == jj) v *= 0.5;
-                    if (kk == ll) v *= 0.5;
-                    if (ii == kk && jj == ll) v *= 0.5;
-                    const long long ij = tri1(ii, jj) - 1, kl = tri1(kk, ll) - 1;
-                    const long long ik = tri1(ii, kk) - 1, jl = tri1(jj, ll) - 1;
-                    const long long il = tri1(ii, ll) - 1, jk = tri1(jj, kk) - 1;
-                    const double v4 = 4.0 * v;
-                    atomicAdd(F + ij, v4 * __ldg(Dm + kl));
-                    atomicAdd(F + kl, v4 * __ldg(Dm + ij));
-                    atomicAdd(F + ik, -v * __ldg(Dm + jl));
-                    atomicAdd(F + jl, -v * __ldg(Dm + ik));
-                    atomicAdd(F + il, -v * __ldg(Dm + jk));
-                    atomicAdd(F + jk, -v * __ldg(Dm + il));
+#pragma unroll
+                    for (int ib = 0; ib < NB; ib++)
+#pragma unroll
+                        for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                            for (int id = 0; id < ND; id++)
+                                acc[m][ib][ic][id] += sx[cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)] *
+                                                      sy[cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)] *
+                                                      sz[czp(LB, ib)][czp(LC, ic)][czp(LD, id)];
                 }
+            }
         }
+    }
+}
+
+// normalisation of a component product: sqrt(3)^n3
+__device__ __forceinline__ double s3pow(int n3) {
+    return n3 == 0 ? 1.0 : n3 == 1 ? 1.7320508075688772935 : n3 == 2 ? 3.0 : n3 == 3 ? 5.196152422706632 : 9.0;
+}
+__device__ __forceinline__ int cs3_rt(int l, int c) { return (l == 2 && c >= 3) ? 1 : 0; }
+
+// 0-based packed index of (i, j): max(i,j)(max+1)/2 + min, 32-bit (nbf < 65536)
+__device__ __forceinline__ int tri0(int i, int j) {
+    const int hi = i > j ? i : j, lo = i > j ? j : i;
+    return ((hi * (hi + 1)) >> 1) + lo;
+}
+
+// target of a K or J update: the CTA's shared tile (rows of A and B of F) or,
+// when the tile does not fit, the packed matrix itself
+struct Rows {
+    double *tile;  // rows x nbf, or null
+    double *F;
+    int nbf;
+    __device__ __forceinline__ void add(int r, int bf_row, int col, double v) const {
+        if (v == 0.0) return;
+        if (tile) atomicAdd(tile + r * nbf + col, v);
+        else atomicAdd(F + tri0(bf_row, col), v);
+    }
+};
+
+struct QuartetCtx {
+    int bfA, bfB, bfC, bfD;
+    bool iandj, kandl, same;
+    double cut;
+    const double *__restrict__ Dm;
+};
+
+__device__ __forceinline__ double dget(const double *__restrict__ Dm, int i, int j) {
+    return __ldg(Dm + tri0(i, j));
+}
+
+// register budget per pass: at most ~40 contracted integrals in flight
+template <int LA, int LB, int LC, int LD>
+struct PassShape {
+    static constexpr int PER_MU = ncart(LB) * ncart(LC) * ncart(LD);
+    static constexpr int NA = ncart(LA);
+    static constexpr int NMU0 = PER_MU >= 40 ? 1 : (40 / PER_MU);
+    static constexpr int NMU = NMU0 > NA ? NA : NMU0;
+    static constexpr int NPASS = (NA + NMU - 1) / NMU;
+};
+
+// Runtime loop over passes of NMU A components; digestion of each pass.
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, int q0, int nq, const double4 &A,
+                                           const double4 &C, R abx, R aby, R abz, R cdx, R cdy, R cdz,
+                                           double thr, bool strict, const double *__restrict__ tab,
+                                           const QuartetCtx &qc, const Rows &rows,
+                                           double (&kbc)[ncart(LB)][ncart(LC)], double (&kbd)[ncart(LB)][ncart(LD)],
+                                           double (&jcd)[ncart(LC)][ncart(LD)]) {
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    using PS = PassShape<LA, LB, LC, LD>;
+    constexpr int M = PS::NMU;
+    constexpr bool can_same = (LA == LC) && (LB == LD);
+#pragma unroll 1
+    for (int pass = 0; pass < PS::NPASS; pass++) {
+        const int mu0 = pass * M;
+        R acc[M][NB][NC][ND];
+        eval_block<LA, LB, LC, LD, R, M>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict, tab,
+                                         mu0, acc);
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            const int ia = mu0 + m;
+            if (ia >= NA) break;
+            const int mu = qc.bfA + ia;
+            const int n3a = cs3_rt(LA, ia);
+            double kac[NC], kad[ND], jab[NB];
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++) kac[ic] = 0.0;
+#pragma unroll
+            for (int id = 0; id < ND; id++) kad[id] = 0.0;
+#pragma unroll
+            for (int ib = 0; ib < NB; ib++) {
+                jab[ib] = 0.0;
+                if (LA == LB && qc.iandj && ib > ia) continue;
+                const int nu = qc.bfB + ib;
+                const double dmn = dget(qc.Dm, mu, nu);
+#pragma unroll
+                for (int ic = 0; ic < NC; ic++) {
+                    const int la = qc.bfC + ic;
+#pragma unroll
+                    for (int id = 0; id < ND; id++) {
+                        if (LC == LD && qc.kandl && id > ic) continue;
+                        if (can_same && qc.same) {
+                            const int oij = qc.iandj ? ia * (ia + 1) / 2 + ib : ia * NB + ib;
+                            const int okl = qc.kandl ? ic * (ic + 1) / 2 + id : ic * ND + id;
+                            if (okl > oij) continue;
+                        }
+                        double v = (double)acc[m][ib][ic][id] * s3pow(n3a + cs3(LB, ib) + cs3(LC, ic) + cs3(LD, id));
+                        if (fabs(v) < qc.cut) continue;
+                        const int si = qc.bfD + id;
+                        // 0.5 factors for coinciding function indices (int0000.F90:288-292)
+                        if (mu == nu) v *= 0.5;
+                        if (la == si) v *= 0.5;
+                        if ((mu == la && nu == si) || (mu == si && nu == la)) v *= 0.5;
+                        jab[ib] += 4.0 * v * dget(qc.Dm, la, si);
+                        jcd[ic][id] += 4.0 * v * dmn;
+                        kac[ic] += v * dget(qc.Dm, nu, si);
+                        kad[id] += v * dget(qc.Dm, nu, la);
+                        kbc[ib][ic] += v * dget(qc.Dm, mu, si);
+                        kbd[ib][id] += v * dget(qc.Dm, mu, la);
+                    }
+                }
+            }
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++) rows.add(ia, mu, qc.bfC + ic, -kac[ic]);
+#pragma unroll
+            for (int id = 0; id < ND; id++) rows.add(ia, mu, qc.bfD + id, -kad[id]);
+#pragma unroll
+            for (int ib = 0; ib < NB; ib++) rows.add(ia, mu, qc.bfB + ib, jab[ib]);
+        }
+    }
 }
 
 // ---- reference rank ownership (int0000.F90:76-91, int0001.F90:89-104) ---------
@@ -291,56 +401,144 @@ struct ClassArgs {
     double cut;
     double thr;
     bool strict;
-    int nbra;
+    const int4 *tasks;       // (bra position, first ket position, ket count, -)
+    const int *ntasks_dev;   // device task count (per-build task lists) or null
+    int ntasks;              // static task count / grid bound
+    int nbf;
+    int tile_rows;           // 1: stage rows of A and B of F in shared memory
     const int *bra_ids, *ket_ids, *bra_orig, *ket_orig;
-    const long long *pref;   // nbra+1
-    const int *koff;         // per-bra first ket position (FP32 items) or null
+    int swapped;             // plan bra list is the reference's ket list
     RankSplit rs;
 };
 
+constexpr int CLASS_THREADS = 128;
+
 template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(128) class_kernel(ClassArgs a) {
-    using Q = Quartet<LA, LB, LC, LD, R>;
-    const long long total = a.pref[a.nbra];
-    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
-         g += (long long)gridDim.x * blockDim.x) {
-        int lo = 0, hi = a.nbra;
-        while (hi - lo > 1) {
-            int mid = (lo + hi) >> 1;
-            if (__ldg(a.pref + mid) <= g) lo = mid; else hi = mid;
-        }
-        const int i = lo;
-        const int j = (int)(g - __ldg(a.pref + i)) + (a.koff ? __ldg(a.koff + i) : 0);
+__global__ void __launch_bounds__(CLASS_THREADS, 3) class_kernel(ClassArgs a) {
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    extern __shared__ double tile[];
+    const int ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
+    if ((int)blockIdx.x >= ntasks) return;
+    const int4 t = a.tasks[blockIdx.x];
+    const int ibra = t.x, k0 = t.y, cnt = t.z;
+    const int P = __ldg(a.bra_ids + ibra);
+    const int2 sab = a.b.pair_shell[P];
+    const double4 A = a.b.shell_xyz[sab.x], B = a.b.shell_xyz[sab.y];
+    const int bfA = a.b.shell_bf0[sab.x], bfB = a.b.shell_bf0[sab.y];
+    const int nrow = NA + NB;
+    const bool use_tile = a.tile_rows != 0;
+    if (use_tile) {
+        for (int i = threadIdx.x; i < nrow * a.nbf; i += CLASS_THREADS) tile[i] = 0.0;
+        __syncthreads();
+    }
+    Rows rowsA{use_tile ? tile : nullptr, a.F, a.nbf};
+    Rows rowsB{use_tile ? tile + NA * a.nbf : nullptr, a.F, a.nbf};
+    const R abx = R(A.x - B.x), aby = R(A.y - B.y), abz = R(A.z - B.z);
+    const int p0 = a.b.pair_prim0[P], np = a.b.pair_nprim[P];
+    for (int qi = threadIdx.x; qi < cnt; qi += CLASS_THREADS) {
+        const int j = k0 + qi;
         if (a.rs.nsize > 1) {
-            const long long bo = a.bra_orig[i], ko = a.ket_orig[j];
+            long long bo = a.bra_orig[ibra], ko = a.ket_orig[j];
+            if (a.swapped) { long long tmp = bo; bo = ko; ko = tmp; }
             long long it;
             if (a.rs.tri) it = (bo > ko ? bo : ko) + 1;
             else if (a.rs.ketmajor) it = ko * a.rs.nbra_ref + bo + 1;
             else it = bo * a.rs.nket_ref + ko + 1;
             if (!rank_owns(a.rs, it)) continue;
         }
-        const int P = __ldg(a.bra_ids + i), Qd = __ldg(a.ket_ids + j);
-        R acc[Q::NCART];
-        Q::eval(a.b, P, Qd, a.thr, a.strict, a.tab, acc);
-        const int2 sab = a.b.pair_shell[P], scd = a.b.pair_shell[Qd];
-        digest<LA, LB, LC, LD, R>(acc, a.b.shell_bf0[sab.x], a.b.shell_bf0[sab.y],
-                                  a.b.shell_bf0[scd.x], a.b.shell_bf0[scd.y], sab.x == sab.y,
-                                  scd.x == scd.y, P == Qd, a.cut, a.Dm, a.F);
+        const int Qd = __ldg(a.ket_ids + j);
+        const int2 scd = a.b.pair_shell[Qd];
+        const double4 C = a.b.shell_xyz[scd.x], D = a.b.shell_xyz[scd.y];
+        const R cdx = R(C.x - D.x), cdy = R(C.y - D.y), cdz = R(C.z - D.z);
+        QuartetCtx qc;
+        qc.bfA = bfA; qc.bfB = bfB;
+        qc.bfC = a.b.shell_bf0[scd.x]; qc.bfD = a.b.shell_bf0[scd.y];
+        qc.iandj = sab.x == sab.y; qc.kandl = scd.x == scd.y; qc.same = P == Qd;
+        qc.cut = a.cut; qc.Dm = a.Dm;
+        double kbc[NB][NC], kbd[NB][ND], jcd[NC][ND];
+#pragma unroll
+        for (int ib = 0; ib < NB; ib++) {
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++) kbc[ib][ic] = 0.0;
+#pragma unroll
+            for (int id = 0; id < ND; id++) kbd[ib][id] = 0.0;
+        }
+#pragma unroll
+        for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+            for (int id = 0; id < ND; id++) jcd[ic][id] = 0.0;
+        run_passes<LA, LB, LC, LD, R>(a.b, p0, np, a.b.pair_prim0[Qd], a.b.pair_nprim[Qd], A, C, abx, aby, abz,
+                                      cdx, cdy, cdz, a.thr, a.strict, a.tab, qc, rowsA, kbc, kbd, jcd);
+#pragma unroll
+        for (int ib = 0; ib < NB; ib++) {
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++) rowsB.add(ib, bfB + ib, qc.bfC + ic, -kbc[ib][ic]);
+#pragma unroll
+            for (int id = 0; id < ND; id++) rowsB.add(ib, bfB + ib, qc.bfD + id, -kbd[ib][id]);
+        }
+#pragma unroll
+        for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+            for (int id = 0; id < ND; id++) {
+                const double v = jcd[ic][id];
+                if (v != 0.0) atomicAdd(a.F + tri0(qc.bfC + ic, qc.bfD + id), v);
+            }
+    }
+    if (use_tile) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < nrow * a.nbf; i += CLASS_THREADS) {
+            const double v = tile[i];
+            if (v == 0.0) continue;
+            const int r = i / a.nbf, col = i - r * a.nbf;
+            const int bf = r < NA ? bfA + r : bfB + (r - NA);
+            atomicAdd(a.F + tri0(bf, col), v);
+        }
     }
 }
 
+// sqrt(max |(ab|ab)|) over the components of one pair, for the Schwarz table.
+template <int LA, int LB>
+__device__ __forceinline__ double schwarz_diag(const DevBasis &b, int P, const double *tab) {
+    constexpr int NA = ncart(LA), NB = ncart(LB);
+    const int2 sab = b.pair_shell[P];
+    const double4 A = b.shell_xyz[sab.x], B = b.shell_xyz[sab.y];
+    const double abx = A.x - B.x, aby = A.y - B.y, abz = A.z - B.z;
+    const int p0 = b.pair_prim0[P], np = b.pair_nprim[P];
+    double m = 0.0;
+#pragma unroll 1
+    for (int ia = 0; ia < NA; ia++) {
+        double acc[1][NB][NA][NB];
+        eval_block<LA, LB, LA, LB, double, 1>(b, p0, np, p0, np, A, A, abx, aby, abz, abx, aby, abz, RYS_TMAX,
+                                              false, tab, ia, acc);
+#pragma unroll
+        for (int ib = 0; ib < NB; ib++) {
+            double v = 0.0;
+#pragma unroll
+            for (int ic = 0; ic < NA; ic++) v = (ic == ia) ? acc[0][ib][ic][ib] : v;
+            v = fabs(v) * s3pow(2 * (cs3_rt(LA, ia) + cs3(LB, ib)));
+            m = v > m ? v : m;
+        }
+    }
+    return sqrt(m);
+}
 
 template <int LA, int LB, int LC, int LD>
-cudaError_t launch_t(const ClassArgs &a, long long work, int precision, int num_sms, cudaStream_t st) {
-    if (work <= 0) return cudaSuccess;
-    const int threads = 128;
-    long long blocks = (work + threads - 1) / threads;
-    long long cap = (long long)num_sms * 32;
-    if (blocks > cap) blocks = cap;
-    if (precision == 0)
-        class_kernel<LA, LB, LC, LD, double><<<(unsigned)blocks, threads, 0, st>>>(a);
-    else
-        class_kernel<LA, LB, LC, LD, float><<<(unsigned)blocks, threads, 0, st>>>(a);
+cudaError_t launch_t(const ClassArgs &a, int precision, cudaStream_t st) {
+    if (a.ntasks <= 0) return cudaSuccess;
+    constexpr int NA = ncart(LA), NB = ncart(LB);
+    const size_t smem = a.tile_rows ? (size_t)(NA + NB) * a.nbf * sizeof(double) : 0;
+    cudaError_t e;
+    if (precision == 0) {
+        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, double>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        class_kernel<LA, LB, LC, LD, double><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(a);
+    } else {
+        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, float>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        class_kernel<LA, LB, LC, LD, float><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(a);
+    }
     return cudaGetLastError();
 }
 

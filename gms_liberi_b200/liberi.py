@@ -30,7 +30,7 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_cleanup", "liberi_c_init", "liberi_c_fock", "liberi_c_finalize",
            "liberi_c_last_error", "liberi_c_set_option", "liberi_c_get_option",
            "liberi_c_fock_build_device", "liberi_c_schwarz", "liberi_c_get_stats",
-           "liberi_c_kernel_name", "liberi_c_rys_eval"]
+           "liberi_c_kernel_name", "liberi_c_rys_eval", "liberi_c_microbench"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -85,6 +85,7 @@ def lib():
         L.liberi_c_get_stats.argtypes = [H, ctypes.POINTER(Stats)]
         L.liberi_c_rys_eval.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                         _F64P, _F64P]
+        L.liberi_c_microbench.argtypes = [ctypes.c_int32, _F64P]
         L.liberi_c_kernel_name.argtypes = [ctypes.c_int32]
         L.liberi_c_kernel_name.restype = ctypes.c_char_p
         for name in EXPORTS:
@@ -243,6 +244,19 @@ def fock(handle, density):
     out = np.zeros(ntri)
     liberi_fock_build(handle, density, out, ntri)
     return out
+
+
+def microbench(kind):
+    """0: FP64 FMA TFLOP/s, 1: FP32 FMA TFLOP/s, 2: FP64 atomicAdd Gatomic/s."""
+    v = ctypes.c_double()
+    _check(lib().liberi_c_microbench(kind, ctypes.byref(v)))
+    return v.value
+
+
+def fock_build_device(handle, d_density_ptr, d_fock_ptr, stream_ptr=0):
+    """liberi_c_fock_build_device on raw device pointers (enqueued, async)."""
+    _check(lib().liberi_c_fock_build_device(handle.ptr, ctypes.c_void_p(d_density_ptr),
+                                            ctypes.c_void_p(d_fock_ptr), ctypes.c_void_p(stream_ptr)))
 
 
 def rys_eval(n, T, thr=60.0, strict=False):

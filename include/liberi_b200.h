@@ -141,6 +141,15 @@ int liberi_c_get_stats(liberi_handle handle, liberi_stats *stats);
  * does; the large-T limit is used for T > thr (strict) or T >= thr. */
 int liberi_c_rys_eval(int32_t n, double T, double thr, int32_t strict, double *u, double *w);
 
+/* Device microbenchmarks on the current device (roofline denominators):
+ *   kind 0: FP64 FMA throughput, TFLOP/s
+ *   kind 1: FP32 FMA throughput, TFLOP/s
+ *   kind 2: FP64 atomicAdd throughput into a 405,450-element (3.2 MB,
+ *           L2-resident) array at random addresses, Gatomic/s
+ *   kind 3: shared-memory FP64 atomicAdd throughput (3,600-element block
+ *           array, random addresses), Gatomic/s */
+int liberi_c_microbench(int32_t kind, double *result);
+
 /* Name of kernel class k (0..20), e.g. "int2222"; NULL if out of range. */
 const char *liberi_c_kernel_name(int32_t k);
 

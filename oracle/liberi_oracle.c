@@ -97,8 +97,10 @@ typedef struct {
 } oracle_opts;
 
 /* per kernel: [0] screened shell quartets, [1] primitive quartets evaluated,
- * [2] integrals digested (|v| >= cut), [3] evaluated shell quartets (sample) */
-typedef struct { int64_t c[21][4]; } oracle_counts;
+ * [2] integrals digested (|v| >= cut), [3] evaluated shell quartets (sample);
+ * t_wall[k]: wall seconds of the kernel, t_eval[k]: seconds spent evaluating
+ * and digesting quartets summed over threads */
+typedef struct { int64_t c[21][4]; double t_wall[21]; double t_eval[21]; int32_t nthreads; } oracle_counts;
 
 /* ---- pair classes ---------------------------------------------------------- */
 enum { SS = 0, SP, PP, SD, PD, DD, NPC };
@@ -573,6 +575,14 @@ int oracle_rank_owns(int tile, int64_t ntot, int64_t it, int rank, int nsize) {
     return it >= s && it <= e;
 }
 
+static double now_s(void) {
+#ifdef _OPENMP
+    return omp_get_wtime();
+#else
+    return 0.0;
+#endif
+}
+
 static uint64_t mix64(uint64_t x) {
     x ^= x >> 33; x *= 0xff51afd7ed558ccdULL; x ^= x >> 33;
     x *= 0xc4ceb9fe1a85ec53ULL; x ^= x >> 33;
@@ -615,7 +625,8 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
         double dcut = kd->digest_schwarz ? o->schwarz_cut : o->eri_cut;
         int64_t niter = kd->tri ? nbl : nbl * nkl;
         int64_t c_scr = 0, c_prim = 0, c_dig = 0, c_eval = 0;
-#pragma omp parallel num_threads(nth) reduction(+ : c_scr, c_prim, c_dig, c_eval)
+        double t_eval = 0.0, t_k0 = now_s();
+#pragma omp parallel num_threads(nth) reduction(+ : c_scr, c_prim, c_dig, c_eval, t_eval)
         {
             int tid = 0;
 #ifdef _OPENMP
@@ -643,15 +654,20 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
                         if (h % (uint64_t)o->sample_mod) continue;
                     }
                     c_eval++;
+                    double tq = o->sample_mod > 1 ? now_s() : 0.0;
                     int A = pb->ish[bi], B = pb->jsh[bi], C = pk->ish[ki], D = pk->jsh[ki];
                     c_prim += eri_quartet(&c, A, B, C, D, pb, bi, pk, ki, kd, vbuf);
                     c_dig += dirfck(&c, A, B, C, D, vbuf, dcut, Dm, Ft);
+                    if (o->sample_mod > 1) t_eval += now_s() - tq;
                 }
             }
         }
         if (cnt) {
             cnt->c[kk][0] = c_scr; cnt->c[kk][1] = c_prim;
             cnt->c[kk][2] = c_dig; cnt->c[kk][3] = c_eval;
+            cnt->t_wall[kk] = now_s() - t_k0;
+            cnt->t_eval[kk] = t_eval;
+            cnt->nthreads = nth;
         }
         free(lb); free(lk);
     }

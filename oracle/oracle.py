@@ -43,7 +43,8 @@ class _Opts(ctypes.Structure):
 
 
 class _Counts(ctypes.Structure):
-    _fields_ = [("c", (ctypes.c_int64 * 4) * 21)]
+    _fields_ = [("c", (ctypes.c_int64 * 4) * 21), ("t_wall", ctypes.c_double * 21),
+                ("t_eval", ctypes.c_double * 21), ("nthreads", ctypes.c_int32)]
 
 
 _lib = None
@@ -93,9 +94,11 @@ def _basis_struct(b, keep):
 
 def fock_build(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, my_rank=0,
                num_procs=1, sample_mod=1, sample_seed=0, nthreads=0, only_kernel=-1,
-               return_counts=False):
+               return_counts=False, return_times=False):
     """Packed F (this rank's partial) for packed D; optional per-kernel counts
-    [screened quartets, primitive quartets, digested integrals, evaluated]."""
+    [screened quartets, primitive quartets, digested integrals, evaluated] and
+    times (wall seconds per kernel, evaluation seconds summed over threads,
+    thread count)."""
     keep = []
     bs = _basis_struct(basis, keep)
     n = int(basis["num_bas"])
@@ -110,8 +113,10 @@ def fock_build(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, my_rank=0,
                                  ctypes.byref(cnt))
     if rc != 0:
         raise RuntimeError("oracle_fock_build failed: %d" % rc)
+    counts = np.array([[cnt.c[k][j] for j in range(4)] for k in range(21)], dtype=np.int64)
+    if return_times:
+        return f, counts, (np.array(cnt.t_wall[:]), np.array(cnt.t_eval[:]), int(cnt.nthreads))
     if return_counts:
-        counts = np.array([[cnt.c[k][j] for j in range(4)] for k in range(21)], dtype=np.int64)
         return f, counts
     return f
 
