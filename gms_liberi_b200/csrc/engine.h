@@ -18,10 +18,11 @@ namespace liberi {
 constexpr int NKERN = 21;
 constexpr int MAXROOT = 5;
 // Rys tables: intervals of width 1 in T on [0, RYS_TMAX), 13 power-basis
-// coefficients per function in x = 2(T - k) - 1.
+// coefficients per function in x = 2(T - k) - 1, stored padded to 14 so each
+// function is 7 aligned double2 loads.
 constexpr int RYS_NINT = 60;
 constexpr int RYS_DEG = 12;
-constexpr int RYS_NCOEF = RYS_DEG + 1;
+constexpr int RYS_NCOEF = 14;
 constexpr double RYS_TMAX = 60.0;
 // table layout: for n = 1..5 roots, RYS_NINT intervals x 2n functions (n roots
 // then n weights) x RYS_NCOEF coefficients; then per n the large-T limit:

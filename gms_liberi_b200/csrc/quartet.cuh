@@ -67,13 +67,19 @@ __device__ __forceinline__ void rys_eval(double T, double thr, bool strict,
     }
     int k = (int)T;
     double x = 2.0 * (T - (double)k) - 1.0;
-    const double *base = tab + rys_table_off(N) + (size_t)k * (2 * N * RYS_NCOEF);
+    const double2 *base = reinterpret_cast<const double2 *>(tab + rys_table_off(N)) + (size_t)k * (N * RYS_NCOEF);
+    // Estrin evaluation of the degree-12 polynomial: dependency depth 5
+    const double x2 = x * x, x4 = x2 * x2, x8 = x4 * x4;
 #pragma unroll
     for (int f = 0; f < 2 * N; f++) {
-        const double *c = base + f * RYS_NCOEF;
-        double v = __ldg(c + RYS_DEG);
-#pragma unroll
-        for (int j = RYS_DEG - 1; j >= 0; j--) v = fma(v, x, __ldg(c + j));
+        const double2 *c = base + f * (RYS_NCOEF / 2);
+        const double2 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2), c67 = __ldg(c + 3);
+        const double2 c89 = __ldg(c + 4), cab = __ldg(c + 5), ccd = __ldg(c + 6);
+        const double a0 = fma(c01.y, x, c01.x), a1 = fma(c23.y, x, c23.x), a2 = fma(c45.y, x, c45.x);
+        const double a3 = fma(c67.y, x, c67.x), a4 = fma(c89.y, x, c89.x), a5 = fma(cab.y, x, cab.x);
+        const double b0 = fma(a1, x2, a0), b1 = fma(a3, x2, a2), b2 = fma(a5, x2, a4);
+        const double d0 = fma(b1, x4, b0), d1 = fma(ccd.x, x4, b2);
+        const double v = fma(d1, x8, d0);
         if (f < N) u[f] = v; else w[f - N] = v;
     }
 }
@@ -141,26 +147,48 @@ __device__ __forceinline__ int cx_rt(int l, int c) { return l == 0 ? 0 : (l == 1
 __device__ __forceinline__ int cy_rt(int l, int c) { return l == 0 ? 0 : (l == 1 ? (c == 1) : (c == 1 ? 2 : ((c == 3 || c == 5) ? 1 : 0))); }
 __device__ __forceinline__ int cz_rt(int l, int c) { return l == 0 ? 0 : (l == 1 ? (c == 2) : (c == 2 ? 2 : ((c == 4 || c == 5) ? 1 : 0))); }
 
-// slice[b][c][d] = I[e][b][c][d] for a runtime e <= LA (register selects)
+// horizontal transfer for one runtime A exponent ea: s[b][c][d] = I[ea][b][c][d]
+// from the VRR block g[e][f] (rows ea..ea+LB are selected first)
 template <int LA, int LB, int LC, int LD, typename R>
-__device__ __forceinline__ void select_slice(const R (&I)[LA + 1][LB + 1][LC + 1][LD + 1], int e,
-                                             R (&s)[LB + 1][LC + 1][LD + 1]) {
+__device__ __forceinline__ void hrr_slice(const R (&g)[LA + LB + 1][LC + LD + 1], int ea, R ab, R cd,
+                                          R (&s)[LB + 1][LC + 1][LD + 1]) {
+    constexpr int LCD = LC + LD;
+    R h[LB + 1][LB + 1][LCD + 1];  // h[t][b][f] = I(ea + t, b) before the ket transfer
 #pragma unroll
-    for (int b = 0; b <= LB; b++)
+    for (int t = 0; t <= LB; t++)
+#pragma unroll
+        for (int f = 0; f <= LCD; f++) {
+            R v = g[t][f];
+#pragma unroll
+            for (int x = 1; x <= LA; x++) v = (ea == x) ? g[x + t][f] : v;
+            h[t][0][f] = v;
+        }
+#pragma unroll
+    for (int b = 1; b <= LB; b++)
+#pragma unroll
+        for (int t = 0; t <= LB - b; t++)
+#pragma unroll
+            for (int f = 0; f <= LCD; f++) h[t][b][f] = h[t + 1][b - 1][f] + ab * h[t][b - 1][f];
+#pragma unroll
+    for (int b = 0; b <= LB; b++) {
+        R k2[LCD + 1][LD + 1];
+#pragma unroll
+        for (int f = 0; f <= LCD; f++) k2[f][0] = h[0][b][f];
+#pragma unroll
+        for (int d = 1; d <= LD; d++)
+#pragma unroll
+            for (int c = 0; c <= LCD - d; c++) k2[c][d] = k2[c + 1][d - 1] + cd * k2[c][d - 1];
 #pragma unroll
         for (int c = 0; c <= LC; c++)
 #pragma unroll
-            for (int d = 0; d <= LD; d++) {
-                R v = I[0][b][c][d];
-#pragma unroll
-                for (int x = 1; x <= LA; x++) v = (e == x) ? I[x][b][c][d] : v;
-                s[b][c][d] = v;
-            }
+            for (int d = 0; d <= LD; d++) s[b][c][d] = k2[c][d];
+    }
 }
 
 // acc[m][ib][ic][id] for A components ia = mu0 + m (m < NMU, ia < NA), all of
-// B, C, D.  mu0 is a runtime value, so one copy of the primitive loop serves
-// every pass.
+// B, C, D.  A single pass (NMU == NA) uses compile-time component indices; a
+// multi-pass class selects the A exponent at run time, so one copy of the
+// primitive loop serves every pass and the root loop is not unrolled.
 template <int LA, int LB, int LC, int LD, typename R, int NMU>
 __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, int q0, int nq,
                                            const double4 &A, const double4 &C, R abx, R aby, R abz,
@@ -170,7 +198,7 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr int LAB = LA + LB, LCD = LC + LD;
     constexpr int NR = (LAB + LCD) / 2 + 1;
-    constexpr bool FULL = (NMU == NA);  // one pass: compile-time components
+    constexpr bool FULL = (NMU == NA);
     int ex[NMU], ey[NMU], ez[NMU];
 #pragma unroll
     for (int m = 0; m < NMU; m++) {
@@ -202,9 +230,14 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
             double u[NR], w[NR];
             rys_eval<NR>(T, thr, strict, tab, u, w);
             const double pref = Px.x * Qx.x * rs;
-#pragma unroll
+#pragma unroll(FULL ? NR : 1)
             for (int r = 0; r < NR; r++) {
-                const double ui = u[r] * ipq;
+                const double ui = u[0] * ipq, wr = w[0];
+#pragma unroll
+                for (int i = 0; i + 1 < NR; i++) {  // rotate the next root to the front
+                    u[i] = u[i + 1];
+                    w[i] = w[i + 1];
+                }
                 const double fq = q * ui, fp = p * ui;
                 const R b00 = R(0.5 * ui);
                 const R b10 = R(hp * (1.0 - fq));
@@ -213,40 +246,41 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                 vrr<LAB, LCD, R>(gx, R((Pp.x - A.x) - fq * pqx), R((Qp.x - C.x) + fp * pqx), b10, b01, b00, R(1));
                 vrr<LAB, LCD, R>(gy, R((Pp.y - A.y) - fq * pqy), R((Qp.y - C.y) + fp * pqy), b10, b01, b00, R(1));
                 vrr<LAB, LCD, R>(gz, R((Pp.z - A.z) - fq * pqz), R((Qp.z - C.z) + fp * pqz), b10, b01, b00,
-                                 R(w[r] * pref));
-                R ix[LA + 1][LB + 1][LC + 1][LD + 1], iy[LA + 1][LB + 1][LC + 1][LD + 1],
-                    iz[LA + 1][LB + 1][LC + 1][LD + 1];
-                hrr<LA, LB, LC, LD, R>(gx, abx, cdx, ix);
-                hrr<LA, LB, LC, LD, R>(gy, aby, cdy, iy);
-                hrr<LA, LB, LC, LD, R>(gz, abz, cdz, iz);
+                                 R(wr * pref));
+                if constexpr (FULL) {
+                    R ix[LA + 1][LB + 1][LC + 1][LD + 1], iy[LA + 1][LB + 1][LC + 1][LD + 1],
+                        iz[LA + 1][LB + 1][LC + 1][LD + 1];
+                    hrr<LA, LB, LC, LD, R>(gx, abx, cdx, ix);
+                    hrr<LA, LB, LC, LD, R>(gy, aby, cdy, iy);
+                    hrr<LA, LB, LC, LD, R>(gz, abz, cdz, iz);
 #pragma unroll
-                for (int m = 0; m < NMU; m++) {
-                    R sx[LB + 1][LC + 1][LD + 1], sy[LB + 1][LC + 1][LD + 1], sz[LB + 1][LC + 1][LD + 1];
-                    if constexpr (FULL) {
+                    for (int m = 0; m < NMU; m++)
 #pragma unroll
-                        for (int b2 = 0; b2 <= LB; b2++)
+                        for (int ib = 0; ib < NB; ib++)
 #pragma unroll
-                            for (int c2 = 0; c2 <= LC; c2++)
+                            for (int ic = 0; ic < NC; ic++)
 #pragma unroll
-                                for (int d2 = 0; d2 <= LD; d2++) {
-                                    sx[b2][c2][d2] = ix[cxp(LA, m)][b2][c2][d2];
-                                    sy[b2][c2][d2] = iy[cyp(LA, m)][b2][c2][d2];
-                                    sz[b2][c2][d2] = iz[czp(LA, m)][b2][c2][d2];
-                                }
-                    } else {
-                        select_slice<LA, LB, LC, LD, R>(ix, ex[m], sx);
-                        select_slice<LA, LB, LC, LD, R>(iy, ey[m], sy);
-                        select_slice<LA, LB, LC, LD, R>(iz, ez[m], sz);
+                                for (int id = 0; id < ND; id++)
+                                    acc[m][ib][ic][id] += ix[cxp(LA, m)][cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)] *
+                                                          iy[cyp(LA, m)][cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)] *
+                                                          iz[czp(LA, m)][czp(LB, ib)][czp(LC, ic)][czp(LD, id)];
+                } else {
+#pragma unroll
+                    for (int m = 0; m < NMU; m++) {
+                        R sx[LB + 1][LC + 1][LD + 1], sy[LB + 1][LC + 1][LD + 1], sz[LB + 1][LC + 1][LD + 1];
+                        hrr_slice<LA, LB, LC, LD, R>(gx, ex[m], abx, cdx, sx);
+                        hrr_slice<LA, LB, LC, LD, R>(gy, ey[m], aby, cdy, sy);
+                        hrr_slice<LA, LB, LC, LD, R>(gz, ez[m], abz, cdz, sz);
+#pragma unroll
+                        for (int ib = 0; ib < NB; ib++)
+#pragma unroll
+                            for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                                for (int id = 0; id < ND; id++)
+                                    acc[m][ib][ic][id] += sx[cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)] *
+                                                          sy[cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)] *
+                                                          sz[czp(LB, ib)][czp(LC, ic)][czp(LD, id)];
                     }
-#pragma unroll
-                    for (int ib = 0; ib < NB; ib++)
-#pragma unroll
-                        for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-                            for (int id = 0; id < ND; id++)
-                                acc[m][ib][ic][id] += sx[cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)] *
-                                                      sy[cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)] *
-                                                      sz[czp(LB, ib)][czp(LC, ic)][czp(LD, id)];
                 }
             }
         }
@@ -289,24 +323,107 @@ __device__ __forceinline__ double dget(const double *__restrict__ Dm, int i, int
     return __ldg(Dm + tri0(i, j));
 }
 
-// register budget per pass: at most ~40 contracted integrals in flight
+// Per-class compile-time shape: A components per pass (bounds the contracted
+// block held in registers) and resident CTAs per SM requested from the
+// register allocator.  The table was tuned offline with ptxas register and
+// spill reports; LIBERI_TUNE_* override one class for that search.
+constexpr int class_key(int la, int lb, int lc, int ld) { return la * 1000 + lb * 100 + lc * 10 + ld; }
+constexpr int tuned_nmu(int key) {
+#ifdef LIBERI_TUNE_KEY
+    if (key == LIBERI_TUNE_KEY) return LIBERI_TUNE_NMU;
+#endif
+    switch (key) {
+        case 1000: return 3;
+        case 1010: return 3;
+        case 1100: return 3;
+        case 1110: return 3;
+        case 1111: return 1;
+        case 1120: return 3;
+        case 2000: return 6;
+        case 2010: return 6;
+        case 2020: return 6;
+        case 2100: return 6;
+        case 2110: return 6;
+        case 2111: return 1;
+        case 2120: return 1;
+        case 2121: return 1;
+        case 2200: return 6;
+        case 2210: return 1;
+        case 2211: return 1;
+        case 2220: return 1;
+        case 2221: return 1;
+        case 2222: return 1;
+        default: return 0;
+    }
+}
+constexpr int tuned_minb(int key) {
+#ifdef LIBERI_TUNE_KEY
+    if (key == LIBERI_TUNE_KEY) return LIBERI_TUNE_MINB;
+#endif
+    switch (key) {
+        case 0: return 6;
+        case 1000: return 5;
+        case 1010: return 4;
+        case 1100: return 4;
+        case 1110: return 3;
+        case 1111: return 3;
+        case 1120: return 2;
+        case 2000: return 4;
+        case 2010: return 3;
+        case 2020: return 2;
+        case 2100: return 3;
+        case 2110: return 2;
+        case 2111: return 3;
+        case 2120: return 3;
+        case 2121: return 2;
+        case 2200: return 2;
+        case 2210: return 2;
+        case 2211: return 2;
+        case 2220: return 2;
+        case 2221: return 2;
+        case 2222: return 2;
+        default: return 3;
+    }
+}
+
 template <int LA, int LB, int LC, int LD>
 struct PassShape {
     static constexpr int PER_MU = ncart(LB) * ncart(LC) * ncart(LD);
     static constexpr int NA = ncart(LA);
-    static constexpr int NMU0 = PER_MU >= 40 ? 1 : (40 / PER_MU);
-    static constexpr int NMU = NMU0 > NA ? NA : NMU0;
+    static constexpr int NMU_DEF = PER_MU >= 40 ? 1 : (40 / PER_MU);
+    static constexpr int NMU_T =
+        tuned_nmu(class_key(LA, LB, LC, LD)) > 0 ? tuned_nmu(class_key(LA, LB, LC, LD)) : NMU_DEF;
+    static constexpr int NMU = NMU_T > NA ? NA : NMU_T;
     static constexpr int NPASS = (NA + NMU - 1) / NMU;
+    static constexpr int MINB = tuned_minb(class_key(LA, LB, LC, LD));
+};
+
+constexpr int CLASS_THREADS = 128;
+
+// Per-quartet partial sums that outlive a pass: K updates of the B rows
+// (bc[ib][ic], bd[ib][id]) and the ket-pair J block (cd[ic][id]).  Single-
+// pass classes keep them in registers; multi-pass classes in per-thread
+// shared-memory slots (stride CLASS_THREADS, bank-conflict free).
+template <int NB, int NC, int ND, bool SM>
+struct KBuf {
+    static constexpr int N = NB * NC + NB * ND + NC * ND;
+    double r[SM ? 1 : N];
+    double *s;
+    __device__ __forceinline__ double &at(int i) {
+        if constexpr (SM) return s[i * CLASS_THREADS];
+        else return r[i];
+    }
+    __device__ __forceinline__ double &bc(int ib, int ic) { return at(ib * NC + ic); }
+    __device__ __forceinline__ double &bd(int ib, int id) { return at(NB * NC + ib * ND + id); }
+    __device__ __forceinline__ double &cd(int ic, int id) { return at(NB * NC + NB * ND + ic * ND + id); }
 };
 
 // Runtime loop over passes of NMU A components; digestion of each pass.
-template <int LA, int LB, int LC, int LD, typename R>
+template <int LA, int LB, int LC, int LD, typename R, typename KB>
 __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, int q0, int nq, const double4 &A,
                                            const double4 &C, R abx, R aby, R abz, R cdx, R cdy, R cdz,
                                            double thr, bool strict, const double *__restrict__ tab,
-                                           const QuartetCtx &qc, const Rows &rows,
-                                           double (&kbc)[ncart(LB)][ncart(LC)], double (&kbd)[ncart(LB)][ncart(LD)],
-                                           double (&jcd)[ncart(LC)][ncart(LD)]) {
+                                           const QuartetCtx &qc, const Rows &rows, KB &kb) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     using PS = PassShape<LA, LB, LC, LD>;
     constexpr int M = PS::NMU;
@@ -353,11 +470,11 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
                         if (la == si) v *= 0.5;
                         if ((mu == la && nu == si) || (mu == si && nu == la)) v *= 0.5;
                         jab[ib] += 4.0 * v * dget(qc.Dm, la, si);
-                        jcd[ic][id] += 4.0 * v * dmn;
+                        kb.cd(ic, id) += 4.0 * v * dmn;
                         kac[ic] += v * dget(qc.Dm, nu, si);
                         kad[id] += v * dget(qc.Dm, nu, la);
-                        kbc[ib][ic] += v * dget(qc.Dm, mu, si);
-                        kbd[ib][id] += v * dget(qc.Dm, mu, la);
+                        kb.bc(ib, ic) += v * dget(qc.Dm, mu, si);
+                        kb.bd(ib, id) += v * dget(qc.Dm, mu, la);
                     }
                 }
             }
@@ -411,10 +528,8 @@ struct ClassArgs {
     RankSplit rs;
 };
 
-constexpr int CLASS_THREADS = 128;
-
 template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(CLASS_THREADS, 3) class_kernel(ClassArgs a) {
+__global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD>::MINB) class_kernel(ClassArgs a) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     extern __shared__ double tile[];
     const int ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
@@ -431,6 +546,7 @@ __global__ void __launch_bounds__(CLASS_THREADS, 3) class_kernel(ClassArgs a) {
         for (int i = threadIdx.x; i < nrow * a.nbf; i += CLASS_THREADS) tile[i] = 0.0;
         __syncthreads();
     }
+    double *slots = tile + (use_tile ? nrow * a.nbf : 0);  // per-thread partial sums (multi-pass)
     Rows rowsA{use_tile ? tile : nullptr, a.F, a.nbf};
     Rows rowsB{use_tile ? tile + NA * a.nbf : nullptr, a.F, a.nbf};
     const R abx = R(A.x - B.x), aby = R(A.y - B.y), abz = R(A.z - B.z);
@@ -455,32 +571,25 @@ __global__ void __launch_bounds__(CLASS_THREADS, 3) class_kernel(ClassArgs a) {
         qc.bfC = a.b.shell_bf0[scd.x]; qc.bfD = a.b.shell_bf0[scd.y];
         qc.iandj = sab.x == sab.y; qc.kandl = scd.x == scd.y; qc.same = P == Qd;
         qc.cut = a.cut; qc.Dm = a.Dm;
-        double kbc[NB][NC], kbd[NB][ND], jcd[NC][ND];
+        constexpr bool SM = PassShape<LA, LB, LC, LD>::NPASS > 1;
+        KBuf<NB, NC, ND, SM> kb;
+        kb.s = slots + threadIdx.x;
 #pragma unroll
-        for (int ib = 0; ib < NB; ib++) {
-#pragma unroll
-            for (int ic = 0; ic < NC; ic++) kbc[ib][ic] = 0.0;
-#pragma unroll
-            for (int id = 0; id < ND; id++) kbd[ib][id] = 0.0;
-        }
-#pragma unroll
-        for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-            for (int id = 0; id < ND; id++) jcd[ic][id] = 0.0;
+        for (int i = 0; i < KBuf<NB, NC, ND, SM>::N; i++) kb.at(i) = 0.0;
         run_passes<LA, LB, LC, LD, R>(a.b, p0, np, a.b.pair_prim0[Qd], a.b.pair_nprim[Qd], A, C, abx, aby, abz,
-                                      cdx, cdy, cdz, a.thr, a.strict, a.tab, qc, rowsA, kbc, kbd, jcd);
+                                      cdx, cdy, cdz, a.thr, a.strict, a.tab, qc, rowsA, kb);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
 #pragma unroll
-            for (int ic = 0; ic < NC; ic++) rowsB.add(ib, bfB + ib, qc.bfC + ic, -kbc[ib][ic]);
+            for (int ic = 0; ic < NC; ic++) rowsB.add(ib, bfB + ib, qc.bfC + ic, -kb.bc(ib, ic));
 #pragma unroll
-            for (int id = 0; id < ND; id++) rowsB.add(ib, bfB + ib, qc.bfD + id, -kbd[ib][id]);
+            for (int id = 0; id < ND; id++) rowsB.add(ib, bfB + ib, qc.bfD + id, -kb.bd(ib, id));
         }
 #pragma unroll
         for (int ic = 0; ic < NC; ic++)
 #pragma unroll
             for (int id = 0; id < ND; id++) {
-                const double v = jcd[ic][id];
+                const double v = kb.cd(ic, id);
                 if (v != 0.0) atomicAdd(a.F + tri0(qc.bfC + ic, qc.bfD + id), v);
             }
     }
@@ -525,19 +634,25 @@ __device__ __forceinline__ double schwarz_diag(const DevBasis &b, int P, const d
 template <int LA, int LB, int LC, int LD>
 cudaError_t launch_t(const ClassArgs &a, int precision, cudaStream_t st) {
     if (a.ntasks <= 0) return cudaSuccess;
-    constexpr int NA = ncart(LA), NB = ncart(LB);
-    const size_t smem = a.tile_rows ? (size_t)(NA + NB) * a.nbf * sizeof(double) : 0;
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    constexpr bool SM = PassShape<LA, LB, LC, LD>::NPASS > 1;
+    const size_t slot_bytes = SM ? (size_t)KBuf<NB, NC, ND, true>::N * CLASS_THREADS * sizeof(double) : 0;
+    // the F-row tile is staged only when it fits beside the slots (227 KB per CTA)
+    const size_t tile_bytes = (size_t)(NA + NB) * a.nbf * sizeof(double);
+    ClassArgs args = a;
+    args.tile_rows = (a.tile_rows && tile_bytes + slot_bytes <= 220 * 1024) ? 1 : 0;
+    const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes;
     cudaError_t e;
     if (precision == 0) {
         e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, double>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        class_kernel<LA, LB, LC, LD, double><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(a);
+        class_kernel<LA, LB, LC, LD, double><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
     } else {
         e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, float>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        class_kernel<LA, LB, LC, LD, float><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(a);
+        class_kernel<LA, LB, LC, LD, float><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
     }
     return cudaGetLastError();
 }
