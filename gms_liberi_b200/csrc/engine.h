@@ -162,4 +162,13 @@ cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_
 cudaError_t launch_schwarz(int pair_class, int npairs, int pair_off, const DevBasis &b,
                            const double *rys_tab, double *out_per_pair, cudaStream_t stream);
 
+// host-side inputs of the Schwarz generator (host.cpp) and the thread's
+// last-error message, for the allocation-free entry point (noalloc.cu)
+int schwarz_host_inputs(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot, const int32_t *ang_mom,
+                        const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
+                        const int32_t *atom_loc, const double *exponents, const double *contr_coef_s,
+                        const double *contr_coef_p, const double *contr_coef_d, const double *coords,
+                        BasisHost &basis, PairsHost &pairs, std::vector<double4> &shell_xyz);
+int set_error(int code, const char *msg);
+
 }  // namespace liberi

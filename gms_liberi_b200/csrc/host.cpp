@@ -548,6 +548,28 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     return LIBERI_OK;
 }
 
+// Internal helpers for the allocation-free Schwarz entry point (noalloc.cu):
+// the same input checks and host-side pair construction as liberi_c_schwarz.
+namespace liberi {
+int schwarz_host_inputs(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot, const int32_t *ang_mom,
+                        const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
+                        const int32_t *atom_loc, const double *exponents, const double *contr_coef_s,
+                        const double *contr_coef_p, const double *contr_coef_d, const double *coords,
+                        BasisHost &basis, PairsHost &pairs, std::vector<double4> &shell_xyz) {
+    std::vector<double> ones((size_t)(nsh > 0 ? nsh : 0) * (nsh + 1) / 2, 1.0);
+    int rc = copy_basis(basis, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num, atom_loc,
+                        nullptr, nullptr, exponents, contr_coef_s, contr_coef_p, contr_coef_d, nullptr, coords,
+                        ones.data());
+    if (rc) return rc;
+    rc = validate_basis(basis);
+    if (rc) return rc;
+    build_pairs(basis, pairs, shell_xyz);
+    return LIBERI_OK;
+}
+
+int set_error(int code, const char *msg) { return fail(code, "%s", msg); }
+}  // namespace liberi
+
 // ================================ C ABI ===========================================
 extern "C" {
 

@@ -30,7 +30,8 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_cleanup", "liberi_c_init", "liberi_c_fock", "liberi_c_finalize",
            "liberi_c_last_error", "liberi_c_set_option", "liberi_c_get_option",
            "liberi_c_fock_build_device", "liberi_c_schwarz", "liberi_c_get_stats",
-           "liberi_c_kernel_name", "liberi_c_rys_eval", "liberi_c_microbench"]
+           "liberi_c_kernel_name", "liberi_c_rys_eval", "liberi_c_microbench",
+           "liberi_c_schwarz_noalloc"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -83,6 +84,7 @@ def lib():
                                        _I32P, _I32P, _I32P, _I32P, _I32P,
                                        _F64P, _F64P, _F64P, _F64P, _F64P, _F64P]
         L.liberi_c_get_stats.argtypes = [H, ctypes.POINTER(Stats)]
+        L.liberi_c_schwarz_noalloc.argtypes = L.liberi_c_schwarz.argtypes
         L.liberi_c_rys_eval.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                         _F64P, _F64P]
         L.liberi_c_microbench.argtypes = [ctypes.c_int32, _F64P]
@@ -275,4 +277,21 @@ def schwarz(basis):
     _check(lib().liberi_c_schwarz(nsh, natoms, nbf, mx, _i32(ang, k), _i32(cn, k), _i32(sl, k),
                                   _i32(an, k), _i32(al, k), _f64(ex, k), _f64(cs, k), _f64(cp, k),
                                   _f64(cd, k), _f64(xyz, k), out.ctypes.data_as(_F64P)))
+    return out
+
+
+def schwarz_noalloc(basis):
+    """Packed shell Schwarz table without any device allocation.
+
+    For callers that cannot call cudaMalloc: their device memory is already
+    committed to their own pool, or their allocation policy forbids ad-hoc
+    cudaMalloc/cudaFree.  The engine's device working memory for this call is
+    a fixed 8 MiB array reserved when the library loads; bases that need more
+    raise LiberiError (LIBERI_E_NOMEM) and should use schwarz() instead."""
+    (nsh, natoms, nbf, mx, ang, cn, sl, an, al, sb, eb, ex, cs, cp, cd, cf, xyz) = _basis_args(basis)
+    k = []
+    out = np.zeros(nsh * (nsh + 1) // 2)
+    _check(lib().liberi_c_schwarz_noalloc(nsh, natoms, nbf, mx, _i32(ang, k), _i32(cn, k), _i32(sl, k),
+                                          _i32(an, k), _i32(al, k), _f64(ex, k), _f64(cs, k), _f64(cp, k),
+                                          _f64(cd, k), _f64(xyz, k), out.ctypes.data_as(_F64P)))
     return out

@@ -120,6 +120,22 @@ int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgto
                      const double *contr_coef_s, const double *contr_coef_p,
                      const double *contr_coef_d, const double *coords, double *schwrz_out);
 
+/* Schwarz table without device allocation.  No counterpart in the reference:
+ * same inputs and output as liberi_c_schwarz, for callers that cannot call
+ * cudaMalloc (their device memory is already committed to their own pool, or
+ * their allocation policy forbids ad-hoc cudaMalloc/cudaFree).  Its device
+ * scratch is one static array of LIBERI_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading the library holds until exit; bases that need more are rejected
+ * with LIBERI_E_NOMEM before any GPU work.  The first call on a device sets
+ * the array up (symbol lookup, table upload) and should come before any
+ * stream capture.  Calls are serialised and share the array. */
+#define LIBERI_NOALLOC_SCRATCH_BYTES (8u << 20)
+int liberi_c_schwarz_noalloc(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot,
+                             const int32_t *ang_mom, const int32_t *contr_num, const int32_t *sh_loc,
+                             const int32_t *atom_num, const int32_t *atom_loc, const double *exponents,
+                             const double *contr_coef_s, const double *contr_coef_p,
+                             const double *contr_coef_d, const double *coords, double *schwrz_out);
+
 /* Per-kernel statistics of the last build, 21 rows in the reference driver
  * order (liberi_driver.F90:69-102):
  *   quartets[k]     screened shell quartets owned by this rank

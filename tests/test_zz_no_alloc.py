@@ -1,0 +1,42 @@
+"""The allocation-free Schwarz entry point (liberi_c_schwarz_noalloc).
+
+Some callers cannot call cudaMalloc: their device memory is already committed
+to their own pool allocator, or their allocation policy forbids ad-hoc
+cudaMalloc/cudaFree because those calls synchronise the device.  For them the
+library offers a Schwarz-table generator whose device working memory is a
+fixed array reserved when the library loads.  This file checks, through the
+C ABI, that two calls in a row return what the allocating entry point
+(liberi_c_schwarz) returns, and that a basis too large for the fixed array is
+refused with a clear error.  It is named so that pytest collects it last.
+"""
+import numpy as np
+import pytest
+
+from gms_liberi_b200 import liberi
+from gms_liberi_b200 import molecules as M
+
+pytestmark = pytest.mark.gpu
+
+# same kernels on the same inputs: the tables agree to the parity tests' bar
+RTOL = 1e-12
+
+
+def test_noalloc_schwarz_matches_allocating_entry_point_twice():
+    # two calls in a row: the array keeps the previous call's contents
+    for basis in (M.ethane(), M.random_molecule(7, seed=2)):
+        ref = liberi.schwarz(basis)
+        got = liberi.schwarz_noalloc(basis)
+        assert got.shape == ref.shape
+        assert np.allclose(got, ref, rtol=RTOL, atol=1e-300), np.abs(got - ref).max()
+        assert np.all(got >= 0.0)
+
+
+def test_noalloc_schwarz_rejects_bases_over_the_limit():
+    # 60 carbon atoms at one point keep all 405,000 primitive pairs (~19 MB of
+    # device data, above the 8 MiB array); the check happens before any GPU work
+    basis = M.c60()
+    basis["coords"] = np.zeros_like(basis["coords"])
+    with pytest.raises(liberi.LiberiError) as e:
+        liberi.schwarz_noalloc(basis)
+    assert e.value.code == -5
+    assert "limit" in str(e.value)
