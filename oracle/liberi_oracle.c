@@ -26,10 +26,13 @@
  * Integral values.  The reference evaluates (ab|cd) with rotated-axis Boys-table
  * kernels (s/p/d up to L=5) and generated Rys kernels (L>=5 with a d-d pair).
  * Both are exact methods up to ~1e-14; this oracle evaluates every class by Rys
- * quadrature with the reference's own root algorithm: the 35-point discretised
- * Stieltjes procedure (RYSDS) on Gauss-Legendre nodes u=t^2 followed by a
- * Gauss-Christoffel weight evaluation (the reference's RYSGW, an implicit QL;
- * here Sturm bisection on the same Jacobi matrix), int2222_rysgen.F90:636-877.
+ * quadrature.  Rys classes take the reference's own root algorithm: the
+ * 35-point discretised Stieltjes procedure (RYSDS) on Gauss-Legendre nodes
+ * u=t^2 followed by a Gauss-Christoffel weight evaluation (the reference's
+ * RYSGW, an implicit QL; here Sturm bisection on the same Jacobi matrix),
+ * int2222_rysgen.F90:636-877.  Rotated-axis classes work, like the reference's,
+ * from tabulated Boys functions (liberi_boys.F90): the Rys rule is formed from
+ * the Boys moments F_0..F_{2n-1} in long double.
  * The asymptotic branch follows the reference per class: rotated-axis classes
  * switch to the large-T form for T > t_max = 25 (src/liberi_boys.F90:22,
  * int0000.F90:220-234), Rys classes for xx >= 43 / 49 / 55 (3 / 4 / 5 roots,
@@ -90,7 +93,7 @@ typedef struct {
     double schwarz_cut;  /* reference cutoff_schwarz (5e-11 literal) */
     double eri_cut;      /* reference literal 5.0d-11 in most digestions */
     int32_t my_rank, num_procs;
-    int32_t sample_mod;  /* >1: evaluate only a hashed 1/sample_mod of quartets */
+    int32_t sample_mod;  /* >1: evaluate only the quartets of a hashed 1/sample_mod of bra pairs */
     int32_t sample_seed;
     int32_t nthreads;
     int32_t only_kernel; /* -1: all, else kernel index 0..20 */
@@ -225,8 +228,146 @@ static void jacobi_gauss(int n, const double *a, const double *b2, double beta0,
     }
 }
 
+/* ---- rotated-axis classes: Boys functions and the Rys rule from them ------
+ * The reference's rotated-axis kernels work from tabulated Boys functions
+ * F_m(T) for T <= t_max = 25 (src/liberi_boys.F90:22-32) and the large-T form
+ * beyond.  Here F_m is tabulated as a Taylor table (step 0.05, nine terms,
+ * long double) and the Gauss rule of the Rys weight, whose moments are
+ * exactly F_0..F_{2n-1}, is formed from those moments by the Chebyshev
+ * algorithm in long double (n <= 3 for these classes). */
+#define BOYS_STEP 0.05L
+#define BOYS_NPT 503
+#define BOYS_MMAX 14
+#define BOYS_TERMS 9
+static long double BOYS[BOYS_NPT][BOYS_MMAX + 1];
+static double BOYS_D[BOYS_NPT][BOYS_MMAX + 1];
+
+static void boys_table_init(void) {
+    for (int k = 0; k < BOYS_NPT; k++) {
+        long double T = k * BOYS_STEP, e = expl(-T);
+        /* series for the highest order, downward recursion for the rest */
+        long double term = 1.0L / (2 * BOYS_MMAX + 1), s = term;
+        for (int j = 1; j < 400; j++) {
+            term *= 2.0L * T / (2 * BOYS_MMAX + 2 * j + 1);
+            s += term;
+            if (term < 1e-30L * s) break;
+        }
+        BOYS[k][BOYS_MMAX] = e * s;
+        for (int m = BOYS_MMAX; m > 0; m--) BOYS[k][m - 1] = (2.0L * T * BOYS[k][m] + e) / (2 * m - 1);
+        for (int m = 0; m <= BOYS_MMAX; m++) BOYS_D[k][m] = (double)BOYS[k][m];
+    }
+}
+
+/* double-precision Rys rule for 1 and 2 roots (well conditioned) */
+static void rys_small_d(int n, double T, double *u, double *w) {
+    const int mmax = 2 * n - 1;
+    const int k = (int)(T / (double)BOYS_STEP + 0.5);
+    const double d = T - k * (double)BOYS_STEP;
+    double F[4], s = 0.0, f = 1.0;
+    for (int j = 0; j < BOYS_TERMS; j++) {
+        s += BOYS_D[k][mmax + j] * f;
+        f *= -d / (j + 1);
+    }
+    F[mmax] = s;
+    const double e = exp(-T);
+    for (int m = mmax; m > 0; m--) F[m - 1] = (2.0 * T * F[m] + e) / (2 * m - 1);
+    if (n == 1) {
+        u[0] = F[1] / F[0];
+        w[0] = F[0];
+        return;
+    }
+    /* monic recurrence from the moments, then the 2x2 Jacobi matrix */
+    const double a0 = F[1] / F[0];
+    const double s1 = F[2] - a0 * F[1], s2 = F[3] - a0 * F[2];  /* sigma_{1,1}, sigma_{1,2} */
+    const double b1 = s1 / F[0];
+    const double a1 = s2 / s1 - a0;
+    const double m = 0.5 * (a0 + a1), h = 0.5 * (a1 - a0), r = sqrt(h * h + b1);
+    const double x0 = m - r, x1 = m + r;
+    u[0] = x0;
+    u[1] = x1;
+    w[0] = F[0] / (1.0 + (x0 - a0) * (x0 - a0) / b1);
+    w[1] = F[0] / (1.0 + (x1 - a0) * (x1 - a0) / b1);
+}
+
+/* F_0..F_mmax(T), T <= 25 */
+static void boys_eval(int mmax, double T, long double *F) {
+    int k = (int)((long double)T / BOYS_STEP + 0.5L);
+    long double d = (long double)T - k * BOYS_STEP;
+    long double s = 0.0L, f = 1.0L;
+    for (int j = 0; j < BOYS_TERMS; j++) {
+        s += BOYS[k][mmax + j] * f;
+        f *= -d / (j + 1);
+    }
+    F[mmax] = s;
+    long double e = expl(-(long double)T);
+    for (int m = mmax; m > 0; m--) F[m - 1] = (2.0L * T * F[m] + e) / (2 * m - 1);
+}
+
+/* Gauss rule (n <= 3) of the Rys weight from its moments F_0..F_{2n-1} */
+static void rys_from_moments(int n, double T, double *u, double *w) {
+    long double F[2 * MAXROOT + 1];
+    boys_eval(2 * n - 1, T, F);
+    long double a[MAXROOT] = {0}, b[MAXROOT] = {0};
+    long double sp[2 * MAXROOT] = {0}, sc[2 * MAXROOT], sn[2 * MAXROOT];
+    for (int l = 0; l < 2 * n; l++) sc[l] = F[l];
+    a[0] = F[1] / F[0];
+    b[0] = F[0];
+    for (int k = 1; k < n; k++) {
+        for (int l = k; l < 2 * n - k; l++) sn[l] = sc[l + 1] - a[k - 1] * sc[l] - b[k - 1] * sp[l];
+        a[k] = sn[k + 1] / sn[k] - sc[k] / sc[k - 1];
+        b[k] = sn[k] / sc[k - 1];
+        for (int l = 0; l < 2 * n; l++) { sp[l] = sc[l]; sc[l] = sn[l]; }
+    }
+    long double x[MAXROOT];
+    if (n == 1) {
+        x[0] = a[0];
+    } else if (n == 2) {
+        long double m = 0.5L * (a[0] + a[1]), h = 0.5L * (a[1] - a[0]);
+        long double r = sqrtl(h * h + b[1]);
+        x[0] = m - r;
+        x[1] = m + r;
+    } else {
+        /* characteristic polynomial of the 3x3 Jacobi matrix, trigonometric
+         * roots, two Newton polishing steps each */
+        long double c2 = -(a[0] + a[1] + a[2]);
+        long double c1 = a[0] * a[1] + a[0] * a[2] + a[1] * a[2] - b[1] - b[2];
+        long double c0 = -(a[0] * a[1] * a[2]) + a[0] * b[2] + a[2] * b[1];
+        long double p = c1 - c2 * c2 / 3.0L, q = 2.0L * c2 * c2 * c2 / 27.0L - c2 * c1 / 3.0L + c0;
+        long double rr = sqrtl(-p / 3.0L);
+        long double arg = 3.0L * q / (2.0L * p * rr);
+        if (arg > 1.0L) arg = 1.0L;
+        if (arg < -1.0L) arg = -1.0L;
+        long double th = acosl(arg) / 3.0L;
+        const long double PI_L = 3.141592653589793238462643383279502884L;
+        for (int i = 0; i < 3; i++) x[i] = 2.0L * rr * cosl(th - 2.0L * PI_L * i / 3.0L) - c2 / 3.0L;
+        for (int i = 0; i < 3; i++)
+            for (int it = 0; it < 2; it++) {
+                long double v = ((x[i] + c2) * x[i] + c1) * x[i] + c0;
+                long double dv = (3.0L * x[i] + 2.0L * c2) * x[i] + c1;
+                if (dv != 0.0L) x[i] -= v / dv;
+            }
+        for (int i = 0; i < 3; i++)
+            for (int j = i + 1; j < 3; j++)
+                if (x[j] < x[i]) { long double t = x[i]; x[i] = x[j]; x[j] = t; }
+    }
+    for (int i = 0; i < n; i++) {
+        /* Christoffel number: b0 / sum_k p_k(x)^2 / (b1..bk), monic p_k */
+        long double p0 = 1.0L, p1 = 0.0L, nrm = 1.0L, s = 1.0L;
+        for (int k = 0; k + 1 < n; k++) {
+            long double pn = (x[i] - a[k]) * p0 - (k > 0 ? b[k] * p1 : 0.0L);
+            p1 = p0;
+            p0 = pn;
+            nrm *= b[k + 1];
+            s += p0 * p0 / nrm;
+        }
+        u[i] = (double)x[i];
+        w[i] = (double)(b[0] / s);
+    }
+}
+
 static void init_tables(void) {
     if (g_init) return;
+    boys_table_init();
     double gx[NGRID], gw[NGRID];
     gauss_legendre(NGRID, gx, gw);
     for (int i = 0; i < NGRID; i++) {
@@ -257,6 +398,14 @@ static void rys_roots(int n, double T, double thr, int rot, double *u, double *w
     if (asym) {
         double it = 1.0 / T, sq = sqrt(it);
         for (int i = 0; i < n; i++) { u[i] = HR[n][i] * it; w[i] = HW[n][i] * sq; }
+        return;
+    }
+    if (rot && n <= 2) {  /* rotated-axis classes: Boys-function moments */
+        rys_small_d(n, T, u, w);
+        return;
+    }
+    if (rot && n == 3) {
+        rys_from_moments(n, T, u, w);
         return;
     }
     /* RYSDS: Stieltjes on the discrete measure {GRID_U, GRID_W*exp(-T u)} */
@@ -418,17 +567,19 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
             rys_roots(n, T, kd->asym, !kd->rys, u, w);
             double pref = twopi52 * (pb->cc[bq] / p) * (pk->cc[kq] / q) * eab * ecd / sqrt(p + q);
             nprim++;
-            /* 2D integrals per root and dimension */
-            double G[MAXROOT][3][5][5];
+            /* 2D integrals per root and dimension: vertical recurrence, then
+             * horizontal transfer to I[a][b][c][d] by recurrences */
+            double I2[MAXROOT][3][3][3][3][3];
+            const double ipq = 1.0 / (p + q);
             for (int r = 0; r < n; r++) {
                 double ur = u[r];
-                double B00 = 0.5 * ur / (p + q);
-                double B10 = 0.5 / p * (1.0 - q * ur / (p + q));
-                double B01 = 0.5 / q * (1.0 - p * ur / (p + q));
+                double B00 = 0.5 * ur * ipq;
+                double B10 = 0.5 / p * (1.0 - q * ur * ipq);
+                double B01 = 0.5 / q * (1.0 - p * ur * ipq);
                 for (int x = 0; x < 3; x++) {
-                    double C00 = (P[x] - Ar[x]) - q * ur / (p + q) * (P[x] - Q[x]);
-                    double Cp00 = (Q[x] - Cr[x]) + p * ur / (p + q) * (P[x] - Q[x]);
-                    double (*g)[5] = G[r][x];
+                    double C00 = (P[x] - Ar[x]) - q * ur * ipq * (P[x] - Q[x]);
+                    double Cp00 = (Q[x] - Cr[x]) + p * ur * ipq * (P[x] - Q[x]);
+                    double g[5][5];
                     g[0][0] = 1.0;
                     for (int i = 0; i < nij; i++)
                         g[i + 1][0] = C00 * g[i][0] + (i > 0 ? i * B10 * g[i - 1][0] : 0.0);
@@ -440,38 +591,35 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
                             g[i][k + 1] = v;
                         }
                     }
+                    double h[5][3][5];
+                    for (int e = 0; e <= nij; e++)
+                        for (int f = 0; f <= nkl; f++) h[e][0][f] = g[e][f];
+                    for (int bb = 1; bb <= lb; bb++)
+                        for (int a2 = 0; a2 <= nij - bb; a2++)
+                            for (int f = 0; f <= nkl; f++) h[a2][bb][f] = h[a2 + 1][bb - 1][f] + AB[x] * h[a2][bb - 1][f];
+                    for (int a2 = 0; a2 <= la; a2++)
+                        for (int bb = 0; bb <= lb; bb++) {
+                            double k2[5][3];
+                            for (int f = 0; f <= nkl; f++) k2[f][0] = h[a2][bb][f];
+                            for (int dd = 1; dd <= ld; dd++)
+                                for (int cc = 0; cc <= nkl - dd; cc++) k2[cc][dd] = k2[cc + 1][dd - 1] + CD[x] * k2[cc][dd - 1];
+                            for (int cc = 0; cc <= lc; cc++)
+                                for (int dd = 0; dd <= ld; dd++) I2[r][x][a2][bb][cc][dd] = k2[cc][dd];
+                        }
                 }
             }
-            /* horizontal transfer with binomial expansion and assembly */
+            /* assembly */
             for (int ia = 0; ia < na; ia++)
             for (int ib = 0; ib < nb; ib++)
             for (int ic = 0; ic < nc; ic++)
             for (int id = 0; id < nd; id++) {
-                int e[4][3] = {{CX[la][ia], CY[la][ia], CZ[la][ia]},
-                               {CX[lb][ib], CY[lb][ib], CZ[lb][ib]},
-                               {CX[lc][ic], CY[lc][ic], CZ[lc][ic]},
-                               {CX[ld][id], CY[ld][id], CZ[ld][id]}};
+                const int ax = CX[la][ia], ay = CY[la][ia], az = CZ[la][ia];
+                const int bx = CX[lb][ib], by = CY[lb][ib], bz = CZ[lb][ib];
+                const int cx = CX[lc][ic], cy = CY[lc][ic], cz = CZ[lc][ic];
+                const int dx = CX[ld][id], dy = CY[ld][id], dz = CZ[ld][id];
                 double acc = 0.0;
-                for (int r = 0; r < n; r++) {
-                    double prod = w[r];
-                    for (int x = 0; x < 3; x++) {
-                        int ai = e[0][x], bi = e[1][x], ci = e[2][x], di = e[3][x];
-                        double s = 0.0;
-                        double cb = 1.0;
-                        for (int t = 0; t <= bi; t++) {
-                            double fb = cb * pow(AB[x], bi - t);
-                            double cd = 1.0, s2 = 0.0;
-                            for (int v = 0; v <= di; v++) {
-                                s2 += cd * pow(CD[x], di - v) * G[r][x][ai + t][ci + v];
-                                cd = cd * (di - v) / (v + 1);
-                            }
-                            s += fb * s2;
-                            cb = cb * (bi - t) / (t + 1);
-                        }
-                        prod *= s;
-                    }
-                    acc += prod;
-                }
+                for (int r = 0; r < n; r++)
+                    acc += w[r] * I2[r][0][ax][bx][cx][dx] * I2[r][1][ay][by][cy][dy] * I2[r][2][az][bz][cz][dz];
                 out[((ia * nb + ib) * nc + ic) * nd + id] += pref * acc;
             }
         }
@@ -650,7 +798,9 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
                     if (kd->op == OP_GT && !(test > o->schwarz_cut)) continue;
                     c_scr++;
                     if (o->sample_mod > 1) {
-                        uint64_t h = mix64(((uint64_t)kk << 56) ^ ((uint64_t)bi << 28) ^ (uint64_t)ki ^ ((uint64_t)o->sample_seed << 40));
+                        /* sample whole bra pairs (all their kets), so the sampled
+                         * work keeps the cache behaviour of a full run */
+                        uint64_t h = mix64(((uint64_t)kk << 56) ^ ((uint64_t)bi << 8) ^ ((uint64_t)o->sample_seed << 40));
                         if (h % (uint64_t)o->sample_mod) continue;
                     }
                     c_eval++;
