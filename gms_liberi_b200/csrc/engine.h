@@ -67,6 +67,19 @@ struct DevBasis {
 
 // One launch of a class: a list of CTA tasks (bra position, first ket
 // position, ket count) over the plan's sorted lists.
+// Batched launches: one task list over several molecules; task.w selects the
+// molecule, whose device data and class lists come from these views.
+struct MolView {
+    DevBasis b;
+    const double *D;
+    double *F;
+    int nbf;
+    int pad;
+};
+struct ClassView {
+    const int *bra_ids, *ket_ids;
+};
+
 struct DevPlan {
     const int *bra_ids, *ket_ids;    // global pair ids, sorted by xint desc
     const int *bra_orig, *ket_orig;  // positions in the reference's compacted lists
@@ -154,6 +167,10 @@ struct LaunchCtx {
 
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
                          int precision, int nbf, int tile_rows);  // precision 0: FP64, 1: FP32
+// one launch of class k over the tasks of several molecules (task.w = molecule)
+cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, int ntasks, int nbf_max,
+                               const MolView *d_mols, const ClassView *d_cviews, bool swapped);
+cudaError_t launch_zero_fock(const MolView *d_mols, int nmol, long long max_ntri, cudaStream_t stream);
 cudaError_t launch_maxabs(const double *x, long long n, unsigned long long *out,
                           cudaStream_t stream);
 cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_x, const double *ket_x,

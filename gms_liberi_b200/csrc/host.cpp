@@ -348,6 +348,11 @@ static void build_plan(const PairsHost &pr, int k, double cut, int chunk, PlanHo
     }
 }
 
+static void make_tasks(const PlanHost &ph, int chunk, int mol, std::vector<int4> &out) {
+    for (const int4 &it : ph.items)
+        for (int k0 = 0; k0 < it.z; k0 += chunk) out.push_back(make_int4(it.x, it.y + k0, std::min(chunk, it.z - k0), mol));
+}
+
 static int upload_plans(liberi_handle h) {
     for (int k = 0; k < NKERN; k++) {
         PlanHost &ph = h->plan[k];
@@ -570,6 +575,75 @@ int schwarz_host_inputs(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mx
 int set_error(int code, const char *msg) { return fail(code, "%s", msg); }
 }  // namespace liberi
 
+
+// ---- batched builds over several molecules ---------------------------------------
+// One launch per class covers every molecule of the batch (the task's w field
+// selects the molecule); one F-zeroing launch precedes them.  The sequence can
+// be captured once into a CUDA graph and replayed every SCF iteration.
+struct liberi_batch_s {
+    std::vector<liberi_handle> hs;
+    int device = 0;
+    int nbf_max = 0;
+    long long ntri_max = 0;
+    MolView *d_mols = nullptr;
+    ClassView *d_cv[NKERN] = {};
+    int4 *d_tasks[NKERN] = {};
+    int ntasks[NKERN] = {};
+    int chunk[NKERN] = {};
+    bool bound = false;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<void *> allocs;
+};
+
+static void batch_free(liberi_batch b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    for (void *p : b->allocs) cudaFree(p);
+    b->allocs.clear();
+    if (b->stream) cudaStreamDestroy(b->stream);
+    b->stream = nullptr;
+}
+
+static int batch_build_tasks(liberi_batch b, int k) {
+    std::vector<int4> tasks;
+    for (size_t m = 0; m < b->hs.size(); m++) make_tasks(b->hs[m]->plan[k], b->chunk[k], (int)m, tasks);
+    if (b->d_tasks[k]) {
+        cudaFree(b->d_tasks[k]);
+        b->allocs.erase(std::remove(b->allocs.begin(), b->allocs.end(), (void *)b->d_tasks[k]), b->allocs.end());
+        b->d_tasks[k] = nullptr;
+    }
+    b->ntasks[k] = (int)tasks.size();
+    if (tasks.empty()) return LIBERI_OK;
+    CUDA_TRY(cudaMalloc((void **)&b->d_tasks[k], tasks.size() * sizeof(int4)));
+    b->allocs.push_back(b->d_tasks[k]);
+    CUDA_TRY(cudaMemcpy(b->d_tasks[k], tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    return LIBERI_OK;
+}
+
+static int batch_enqueue(liberi_batch b, cudaStream_t st, uint32_t mask) {
+    liberi_handle h0 = b->hs[0];
+    CUDA_TRY(launch_zero_fock(b->d_mols, (int)b->hs.size(), b->ntri_max, st));
+    LaunchCtx ctx;
+    ctx.basis = DevBasis{};
+    ctx.rys_tab = h0->d_tab;
+    ctx.D = nullptr;
+    ctx.F = nullptr;
+    ctx.schwarz_cut = h0->schwarz_cut;
+    ctx.eri_cut = h0->eri_cut;
+    ctx.stream = st;
+    ctx.num_sms = h0->num_sms;
+    for (int k = 0; k < NKERN; k++) {
+        if (!((mask >> k) & 1u) || b->ntasks[k] == 0) continue;
+        CUDA_TRY(launch_class_batch(k, ctx, b->d_tasks[k], b->ntasks[k], b->nbf_max, b->d_mols, b->d_cv[k],
+                                    KDESC[k].swap));
+    }
+    return LIBERI_OK;
+}
+
 // ================================ C ABI ===========================================
 extern "C" {
 
@@ -722,6 +796,235 @@ int liberi_c_fock_build(liberi_handle h, const double *density, double *fock, in
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return LIBERI_OK;
+}
+
+int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32_t n) {
+    if (!out || !handles || n <= 0) return fail(LIBERI_E_ARG, "liberi_batch_create: bad arguments");
+    liberi_batch b = new (std::nothrow) liberi_batch_s();
+    if (!b) return fail(LIBERI_E_NOMEM, "liberi_batch_create: out of host memory");
+    for (int i = 0; i < n; i++) {
+        liberi_handle h = handles[i];
+        if (!h || !h->initialized) {
+            delete b;
+            return fail(LIBERI_E_STATE, "liberi_batch_create: handle %d is not set up", i);
+        }
+        if (h->num_procs != 1 || h->device != handles[0]->device || h->precision != 0 ||
+            h->schwarz_cut != handles[0]->schwarz_cut || h->eri_cut != handles[0]->eri_cut) {
+            delete b;
+            return fail(LIBERI_E_ARG, "liberi_batch_create: handle %d differs in device, rank split, precision or cuts", i);
+        }
+        if (h->plan_dirty) {
+            int rc = replan(h);
+            if (rc) {
+                delete b;
+                return rc;
+            }
+        }
+        b->hs.push_back(h);
+        b->nbf_max = std::max(b->nbf_max, h->basis.num_bas);
+    }
+    b->ntri_max = (long long)b->nbf_max * (b->nbf_max + 1) / 2;
+    b->device = handles[0]->device;
+    cudaSetDevice(b->device);
+    int rc = LIBERI_OK;
+    auto die = [&](int code) { batch_free(b); delete b; return code; };
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return die(fail(LIBERI_E_DEVICE, "liberi_batch_create: stream creation failed"));
+    if (cudaMalloc((void **)&b->d_mols, n * sizeof(MolView)) != cudaSuccess)
+        return die(fail(LIBERI_E_NOMEM, "liberi_batch_create: out of device memory"));
+    b->allocs.push_back(b->d_mols);
+    for (int k = 0; k < NKERN; k++) {
+        std::vector<ClassView> cv(n);
+        for (int m = 0; m < n; m++) cv[m] = ClassView{b->hs[m]->plan[k].d_bra, b->hs[m]->plan[k].d_ket};
+        if (cudaMalloc((void **)&b->d_cv[k], n * sizeof(ClassView)) != cudaSuccess)
+            return die(fail(LIBERI_E_NOMEM, "liberi_batch_create: out of device memory"));
+        b->allocs.push_back(b->d_cv[k]);
+        cudaMemcpy(b->d_cv[k], cv.data(), n * sizeof(ClassView), cudaMemcpyHostToDevice);
+        b->chunk[k] = default_chunk(k);
+        rc = batch_build_tasks(b, k);
+        if (rc) return die(rc);
+    }
+    *out = b;
+    return LIBERI_OK;
+}
+
+int liberi_c_batch_bind(liberi_batch b, const double *const *d_density, double *const *d_fock) {
+    if (!b || !d_density || !d_fock) return fail(LIBERI_E_ARG, "liberi_batch_bind: null argument");
+    CUDA_TRY(cudaSetDevice(b->device));
+    std::vector<MolView> mv(b->hs.size());
+    for (size_t m = 0; m < b->hs.size(); m++) {
+        if (!d_density[m] || !d_fock[m]) return fail(LIBERI_E_ARG, "liberi_batch_bind: null buffer %zu", m);
+        mv[m].b = dev_basis(b->hs[m]);
+        mv[m].D = d_density[m];
+        mv[m].F = d_fock[m];
+        mv[m].nbf = b->hs[m]->basis.num_bas;
+        mv[m].pad = 0;
+    }
+    // a captured graph reads the views through d_mols, so rebinding needs no re-capture
+    CUDA_TRY(cudaMemcpy(b->d_mols, mv.data(), mv.size() * sizeof(MolView), cudaMemcpyHostToDevice));
+    b->bound = true;
+    return LIBERI_OK;
+}
+
+int liberi_c_batch_fock_build(liberi_batch b, void *stream) {
+    if (!b) return fail(LIBERI_E_ARG, "liberi_batch_fock_build: null batch");
+    if (!b->bound) return fail(LIBERI_E_STATE, "liberi_batch_fock_build: call liberi_c_batch_bind first");
+    CUDA_TRY(cudaSetDevice(b->device));
+    return batch_enqueue(b, stream ? (cudaStream_t)stream : b->stream, (1u << NKERN) - 1);
+}
+
+int liberi_c_batch_capture(liberi_batch b) {
+    if (!b) return fail(LIBERI_E_ARG, "liberi_batch_capture: null batch");
+    if (!b->bound) return fail(LIBERI_E_STATE, "liberi_batch_capture: call liberi_c_batch_bind first");
+    CUDA_TRY(cudaSetDevice(b->device));
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    // attributes set outside capture (dynamic shared memory of each class)
+    int rc = batch_enqueue(b, b->stream, (1u << NKERN) - 1);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    rc = batch_enqueue(b, b->stream, (1u << NKERN) - 1);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(LIBERI_E_DEVICE, "liberi_batch_capture: %s", cudaGetErrorString(e));
+    b->graph = g;
+    CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    return LIBERI_OK;
+}
+
+int liberi_c_batch_launch(liberi_batch b, void *stream) {
+    if (!b || !b->exec) return fail(LIBERI_E_STATE, "liberi_batch_launch: no captured graph");
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaGraphLaunch(b->exec, stream ? (cudaStream_t)stream : b->stream));
+    return LIBERI_OK;
+}
+
+int liberi_c_batch_synchronize(liberi_batch b) {
+    if (!b) return fail(LIBERI_E_ARG, "liberi_batch_synchronize: null batch");
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return LIBERI_OK;
+}
+
+int liberi_c_batch_destroy(liberi_batch b) {
+    if (!b) return fail(LIBERI_E_ARG, "liberi_batch_destroy: null batch");
+    cudaSetDevice(b->device);
+    batch_free(b);
+    delete b;
+    return LIBERI_OK;
+}
+
+// ---- autotuner: kets per CTA task, per class ------------------------------------
+static const int TUNE_CHUNKS[] = {128, 256, 512, 1024, 2048};
+
+int liberi_c_batch_autotune(liberi_batch b, int32_t reps, int32_t *chunks_out) {
+    if (!b || !b->bound) return fail(LIBERI_E_STATE, "liberi_batch_autotune: batch not bound");
+    if (reps < 1) reps = 1;
+    CUDA_TRY(cudaSetDevice(b->device));
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    for (int k = 0; k < NKERN; k++) {
+        long long work = 0;
+        for (auto h : b->hs) work += h->plan[k].total;
+        if (work == 0) continue;
+        float best = 1e30f;
+        int best_c = b->chunk[k];
+        for (int c : TUNE_CHUNKS) {
+            b->chunk[k] = c;
+            int rc = batch_build_tasks(b, k);
+            if (rc) return rc;
+            rc = batch_enqueue(b, b->stream, 1u << k);  // warm-up
+            if (rc) return rc;
+            CUDA_TRY(cudaEventRecord(e0, b->stream));
+            for (int r = 0; r < reps; r++) {
+                rc = batch_enqueue(b, b->stream, 1u << k);
+                if (rc) return rc;
+            }
+            CUDA_TRY(cudaEventRecord(e1, b->stream));
+            CUDA_TRY(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                best_c = c;
+            }
+        }
+        b->chunk[k] = best_c;
+        int rc = batch_build_tasks(b, k);
+        if (rc) return rc;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (chunks_out)
+        for (int k = 0; k < NKERN; k++) chunks_out[k] = b->chunk[k];
+    if (b->exec) return liberi_c_batch_capture(b);  // re-capture with the tuned tasks
+    return LIBERI_OK;
+}
+
+int liberi_c_autotune(liberi_handle h, int32_t reps, int32_t *chunks_out) {
+    if (!h || !h->initialized) return fail(LIBERI_E_STATE, "liberi_autotune: handle not set up");
+    if (reps < 1) reps = 1;
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    const uint32_t mask0 = h->class_mask;
+    const int prec0 = h->precision;
+    h->precision = 0;
+    int rc = LIBERI_OK;
+    for (int k = 0; k < NKERN && !rc; k++) {
+        if (h->plan_dirty) rc = replan(h);
+        if (rc || h->plan[k].total == 0) continue;
+        float best = 1e30f;
+        int best_c = h->plan[k].chunk;
+        for (int c : TUNE_CHUNKS) {
+            PlanHost &ph = h->plan[k];
+            ph.chunk = c;
+            ph.tasks.clear();
+            make_tasks(ph, c, 0, ph.tasks);
+            if (ph.d_tasks) {
+                cudaFree(ph.d_tasks);
+                h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)ph.d_tasks), h->allocs.end());
+                ph.d_tasks = nullptr;
+            }
+            if (dev_upload(h, &ph.d_tasks, ph.tasks.data(), ph.tasks.size()) != cudaSuccess) {
+                rc = fail(LIBERI_E_NOMEM, "liberi_autotune: out of device memory");
+                break;
+            }
+            h->class_mask = 1u << k;
+            rc = build_on_device(h, h->dev.D, h->dev.F, h->stream);
+            if (rc) break;
+            cudaEventRecord(e0, h->stream);
+            for (int r = 0; r < reps && !rc; r++) rc = build_on_device(h, h->dev.D, h->dev.F, h->stream);
+            cudaEventRecord(e1, h->stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                best_c = c;
+            }
+        }
+        if (rc) break;
+        h->chunk[k] = best_c;
+    }
+    h->class_mask = mask0;
+    h->precision = prec0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    h->plan_dirty = true;  // rebuild plans with the tuned chunks on the next build
+    rc = replan(h);
+    if (chunks_out)
+        for (int k = 0; k < NKERN; k++) chunks_out[k] = h->plan[k].chunk;
+    return rc;
 }
 
 int liberi_c_set_option(liberi_handle h, const char *name, double value) {

@@ -5,6 +5,8 @@
 
 namespace liberi {
 
+static int ncart_h(int l) { return (l + 1) * (l + 2) / 2; }
+
 #define LIBERI_CLASSES(X)                                                                    \
     X(0, 0, 0, 0, 0) X(1, 1, 0, 0, 0) X(2, 1, 1, 0, 0) X(3, 1, 1, 1, 0) X(4, 1, 0, 1, 0)         \
     X(5, 1, 1, 1, 1) X(6, 2, 0, 0, 0) X(7, 2, 1, 0, 0) X(8, 2, 0, 1, 0) X(9, 2, 1, 1, 0)         \
@@ -120,11 +122,62 @@ cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const
     a.ket_orig = plan.ket_orig;
     a.swapped = plan.swapped ? 1 : 0;
     a.rs = rs;
+    a.mols = nullptr;
+    a.cviews = nullptr;
 #define LIBERI_CASE(kk, A, B, C, D) \
     case kk: return launch_t<A, B, C, D>(a, precision, ctx.stream);
     switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
 #undef LIBERI_CASE
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, int ntasks, int nbf_max,
+                               const MolView *d_mols, const ClassView *d_cviews, bool swapped) {
+    const KernelDesc &kd = KDESC[k];
+    ClassArgs a{};
+    a.b = DevBasis{};
+    a.tab = ctx.rys_tab;
+    a.Dm = nullptr;
+    a.F = nullptr;
+    a.cut = kd.digest_schwarz ? ctx.schwarz_cut : ctx.eri_cut;
+    a.thr = kd.asym;
+    a.strict = !kd.rys;
+    a.tasks = tasks;
+    a.ntasks_dev = nullptr;
+    a.ntasks = ntasks;
+    a.nbf = nbf_max;
+    const size_t tile_bytes = (size_t)(ncart_h(kd.la) + ncart_h(kd.lb)) * nbf_max * sizeof(double);
+    a.tile_rows = tile_bytes <= 160 * 1024 ? 1 : 0;
+    a.bra_ids = a.ket_ids = a.bra_orig = a.ket_orig = nullptr;
+    a.swapped = swapped ? 1 : 0;
+    a.rs = RankSplit{0, 1, 0, 0, 0, 0, 0, 0};
+    a.mols = d_mols;
+    a.cviews = d_cviews;
+#define LIBERI_CASE(kk, A, B, C, D) \
+    case kk: return launch_t<A, B, C, D>(a, 0, ctx.stream);
+    switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
+#undef LIBERI_CASE
+    return cudaErrorInvalidValue;
+}
+
+__global__ void zero_fock_kernel(const MolView *mols, int nmol, long long max_ntri) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < (long long)nmol * max_ntri;
+         g += stride) {
+        const int m = (int)(g / max_ntri);
+        const long long i = g - (long long)m * max_ntri;
+        const long long n = mols[m].nbf;
+        if (i < n * (n + 1) / 2) mols[m].F[i] = 0.0;
+    }
+}
+
+cudaError_t launch_zero_fock(const MolView *d_mols, int nmol, long long max_ntri, cudaStream_t st) {
+    if (nmol <= 0) return cudaSuccess;
+    long long blocks = ((long long)nmol * max_ntri + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    zero_fock_kernel<<<(unsigned)blocks, 256, 0, st>>>(d_mols, nmol, max_ntri);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_schwarz(int pc, int npairs, int pair_off, const DevBasis &b, const double *tab, double *out,

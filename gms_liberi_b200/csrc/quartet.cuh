@@ -526,31 +526,64 @@ struct ClassArgs {
     const int *bra_ids, *ket_ids, *bra_orig, *ket_orig;
     int swapped;             // plan bra list is the reference's ket list
     RankSplit rs;
+    const MolView *mols;     // batched launch: per-molecule data (task.w), else null
+    const ClassView *cviews; // batched launch: per-molecule lists of this class
 };
 
-template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD>::MINB) class_kernel(ClassArgs a) {
+// One CTA task: row pair t.x against kets t.y .. t.y+t.z-1 of one molecule.
+// Per-molecule data of a task.  A single-molecule launch reads the kernel
+// parameters at every use (constant-bank operands, no registers held across
+// the quartet loop); a batched launch reads the task's molecule view (task.w).
+template <bool BATCH>
+__device__ __forceinline__ const DevBasis &mol_basis(const ClassArgs &a, int w) {
+    if constexpr (BATCH) return a.mols[w].b; else return a.b;
+}
+template <bool BATCH>
+__device__ __forceinline__ const double *mol_D(const ClassArgs &a, int w) {
+    if constexpr (BATCH) return a.mols[w].D; else return a.Dm;
+}
+template <bool BATCH>
+__device__ __forceinline__ double *mol_F(const ClassArgs &a, int w) {
+    if constexpr (BATCH) return a.mols[w].F; else return a.F;
+}
+template <bool BATCH>
+__device__ __forceinline__ int mol_nbf(const ClassArgs &a, int w) {
+    if constexpr (BATCH) return a.mols[w].nbf; else return a.nbf;
+}
+template <bool BATCH>
+__device__ __forceinline__ const int *mol_bra(const ClassArgs &a, int w) {
+    if constexpr (BATCH) return a.cviews[w].bra_ids; else return a.bra_ids;
+}
+template <bool BATCH>
+__device__ __forceinline__ const int *mol_ket(const ClassArgs &a, int w) {
+    if constexpr (BATCH) return a.cviews[w].ket_ids; else return a.ket_ids;
+}
+
+// One CTA task: row pair t.x against kets t.y .. t.y+t.z-1 of one molecule.
+template <int LA, int LB, int LC, int LD, typename R, bool BATCH>
+__device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     extern __shared__ double tile[];
-    const int ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
-    if ((int)blockIdx.x >= ntasks) return;
-    const int4 t = a.tasks[blockIdx.x];
     const int ibra = t.x, k0 = t.y, cnt = t.z;
-    const int P = __ldg(a.bra_ids + ibra);
-    const int2 sab = a.b.pair_shell[P];
-    const double4 A = a.b.shell_xyz[sab.x], B = a.b.shell_xyz[sab.y];
-    const int bfA = a.b.shell_bf0[sab.x], bfB = a.b.shell_bf0[sab.y];
+    const DevBasis &bas = mol_basis<BATCH>(a, t.w);
+#define LIBERI_D mol_D<BATCH>(a, t.w)
+#define LIBERI_F mol_F<BATCH>(a, t.w)
+#define LIBERI_NBF mol_nbf<BATCH>(a, t.w)
+    const int P = __ldg(mol_bra<BATCH>(a, t.w) + ibra);
+    const int2 sab = bas.pair_shell[P];
+    const double4 A = bas.shell_xyz[sab.x], B = bas.shell_xyz[sab.y];
+    const int bfA = bas.shell_bf0[sab.x], bfB = bas.shell_bf0[sab.y];
     const int nrow = NA + NB;
     const bool use_tile = a.tile_rows != 0;
     if (use_tile) {
-        for (int i = threadIdx.x; i < nrow * a.nbf; i += CLASS_THREADS) tile[i] = 0.0;
+        for (int i = threadIdx.x; i < nrow * LIBERI_NBF; i += CLASS_THREADS) tile[i] = 0.0;
         __syncthreads();
     }
-    double *slots = tile + (use_tile ? nrow * a.nbf : 0);  // per-thread partial sums (multi-pass)
-    Rows rowsA{use_tile ? tile : nullptr, a.F, a.nbf};
-    Rows rowsB{use_tile ? tile + NA * a.nbf : nullptr, a.F, a.nbf};
+    double *slots = tile + (use_tile ? nrow * LIBERI_NBF : 0);  // per-thread partial sums (multi-pass)
+    Rows rowsA{use_tile ? tile : nullptr, LIBERI_F, LIBERI_NBF};
+    Rows rowsB{use_tile ? tile + NA * LIBERI_NBF : nullptr, LIBERI_F, LIBERI_NBF};
     const R abx = R(A.x - B.x), aby = R(A.y - B.y), abz = R(A.z - B.z);
-    const int p0 = a.b.pair_prim0[P], np = a.b.pair_nprim[P];
+    const int p0 = bas.pair_prim0[P], np = bas.pair_nprim[P];
     for (int qi = threadIdx.x; qi < cnt; qi += CLASS_THREADS) {
         const int j = k0 + qi;
         if (a.rs.nsize > 1) {
@@ -562,21 +595,21 @@ __global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD>::MINB
             else it = bo * a.rs.nket_ref + ko + 1;
             if (!rank_owns(a.rs, it)) continue;
         }
-        const int Qd = __ldg(a.ket_ids + j);
-        const int2 scd = a.b.pair_shell[Qd];
-        const double4 C = a.b.shell_xyz[scd.x], D = a.b.shell_xyz[scd.y];
+        const int Qd = __ldg(mol_ket<BATCH>(a, t.w) + j);
+        const int2 scd = bas.pair_shell[Qd];
+        const double4 C = bas.shell_xyz[scd.x], D = bas.shell_xyz[scd.y];
         const R cdx = R(C.x - D.x), cdy = R(C.y - D.y), cdz = R(C.z - D.z);
         QuartetCtx qc;
         qc.bfA = bfA; qc.bfB = bfB;
-        qc.bfC = a.b.shell_bf0[scd.x]; qc.bfD = a.b.shell_bf0[scd.y];
+        qc.bfC = bas.shell_bf0[scd.x]; qc.bfD = bas.shell_bf0[scd.y];
         qc.iandj = sab.x == sab.y; qc.kandl = scd.x == scd.y; qc.same = P == Qd;
-        qc.cut = a.cut; qc.Dm = a.Dm;
+        qc.cut = a.cut; qc.Dm = LIBERI_D;
         constexpr bool SM = PassShape<LA, LB, LC, LD>::NPASS > 1;
         KBuf<NB, NC, ND, SM> kb;
         kb.s = slots + threadIdx.x;
 #pragma unroll
         for (int i = 0; i < KBuf<NB, NC, ND, SM>::N; i++) kb.at(i) = 0.0;
-        run_passes<LA, LB, LC, LD, R>(a.b, p0, np, a.b.pair_prim0[Qd], a.b.pair_nprim[Qd], A, C, abx, aby, abz,
+        run_passes<LA, LB, LC, LD, R>(bas, p0, np, bas.pair_prim0[Qd], bas.pair_nprim[Qd], A, C, abx, aby, abz,
                                       cdx, cdy, cdz, a.thr, a.strict, a.tab, qc, rowsA, kb);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
@@ -590,19 +623,32 @@ __global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD>::MINB
 #pragma unroll
             for (int id = 0; id < ND; id++) {
                 const double v = kb.cd(ic, id);
-                if (v != 0.0) atomicAdd(a.F + tri0(qc.bfC + ic, qc.bfD + id), v);
+                if (v != 0.0) atomicAdd(LIBERI_F + tri0(qc.bfC + ic, qc.bfD + id), v);
             }
     }
     if (use_tile) {
         __syncthreads();
-        for (int i = threadIdx.x; i < nrow * a.nbf; i += CLASS_THREADS) {
+        for (int i = threadIdx.x; i < nrow * LIBERI_NBF; i += CLASS_THREADS) {
             const double v = tile[i];
             if (v == 0.0) continue;
-            const int r = i / a.nbf, col = i - r * a.nbf;
+            const int r = i / LIBERI_NBF, col = i - r * LIBERI_NBF;
             const int bf = r < NA ? bfA + r : bfB + (r - NA);
-            atomicAdd(a.F + tri0(bf, col), v);
+            atomicAdd(LIBERI_F + tri0(bf, col), v);
         }
     }
+#undef LIBERI_D
+#undef LIBERI_F
+#undef LIBERI_NBF
+}
+
+// BATCH: the task's w field selects the molecule (basis, D, F, plan lists);
+// the launch sized the shared-memory tile for the largest molecule.
+template <int LA, int LB, int LC, int LD, typename R, bool BATCH>
+__global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD>::MINB) class_kernel(ClassArgs a) {
+    const int ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
+    if ((int)blockIdx.x >= ntasks) return;
+    const int4 t = a.tasks[blockIdx.x];
+    class_task<LA, LB, LC, LD, R, BATCH>(a, t);
 }
 
 // sqrt(max |(ab|ab)|) over the components of one pair, for the Schwarz table.
@@ -642,17 +688,25 @@ cudaError_t launch_t(const ClassArgs &a, int precision, cudaStream_t st) {
     ClassArgs args = a;
     args.tile_rows = (a.tile_rows && tile_bytes + slot_bytes <= 220 * 1024) ? 1 : 0;
     const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes;
+    // the opt-in limit is raised to the per-CTA maximum once per launch, not
+    // to this launch's size: a captured graph may hold a larger launch
+    const int smem_cap = 227 * 1024;
     cudaError_t e;
-    if (precision == 0) {
-        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, double>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (a.mols) {
+        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, double, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap);
         if (e != cudaSuccess) return e;
-        class_kernel<LA, LB, LC, LD, double><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
+        class_kernel<LA, LB, LC, LD, double, true><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
+    } else if (precision == 0) {
+        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, double, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap);
+        if (e != cudaSuccess) return e;
+        class_kernel<LA, LB, LC, LD, double, false><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
     } else {
-        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, float, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap);
         if (e != cudaSuccess) return e;
-        class_kernel<LA, LB, LC, LD, float><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
+        class_kernel<LA, LB, LC, LD, float, false><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
     }
     return cudaGetLastError();
 }

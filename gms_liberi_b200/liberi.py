@@ -31,7 +31,10 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_last_error", "liberi_c_set_option", "liberi_c_get_option",
            "liberi_c_fock_build_device", "liberi_c_schwarz", "liberi_c_get_stats",
            "liberi_c_kernel_name", "liberi_c_rys_eval", "liberi_c_microbench",
-           "liberi_c_schwarz_noalloc"]
+           "liberi_c_schwarz_noalloc", "liberi_c_batch_create", "liberi_c_batch_bind",
+           "liberi_c_batch_fock_build", "liberi_c_batch_capture", "liberi_c_batch_launch",
+           "liberi_c_batch_synchronize", "liberi_c_batch_autotune", "liberi_c_batch_destroy",
+           "liberi_c_autotune"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -89,6 +92,15 @@ def lib():
                                         _F64P, _F64P]
         L.liberi_c_microbench.argtypes = [ctypes.c_int32, _F64P]
         L.liberi_c_kernel_name.argtypes = [ctypes.c_int32]
+        L.liberi_c_batch_create.argtypes = [ctypes.POINTER(H), ctypes.POINTER(H), ctypes.c_int32]
+        L.liberi_c_batch_bind.argtypes = [H, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]
+        L.liberi_c_batch_fock_build.argtypes = [H, ctypes.c_void_p]
+        L.liberi_c_batch_capture.argtypes = [H]
+        L.liberi_c_batch_launch.argtypes = [H, ctypes.c_void_p]
+        L.liberi_c_batch_synchronize.argtypes = [H]
+        L.liberi_c_batch_autotune.argtypes = [H, ctypes.c_int32, _I32P]
+        L.liberi_c_batch_destroy.argtypes = [H]
+        L.liberi_c_autotune.argtypes = [H, ctypes.c_int32, _I32P]
         L.liberi_c_kernel_name.restype = ctypes.c_char_p
         for name in EXPORTS:
             if name != "liberi_c_kernel_name":
@@ -259,6 +271,52 @@ def fock_build_device(handle, d_density_ptr, d_fock_ptr, stream_ptr=0):
     """liberi_c_fock_build_device on raw device pointers (enqueued, async)."""
     _check(lib().liberi_c_fock_build_device(handle.ptr, ctypes.c_void_p(d_density_ptr),
                                             ctypes.c_void_p(d_fock_ptr), ctypes.c_void_p(stream_ptr)))
+
+
+def autotune(handle, reps=3):
+    """Per-class kets-per-task choice timed on the handle's device buffers."""
+    out = np.zeros(21, dtype=np.int32)
+    _check(lib().liberi_c_autotune(handle.ptr, int(reps), out.ctypes.data_as(_I32P)))
+    return out
+
+
+class Batch:
+    """Several set-up handles built together: one launch per class over all
+    molecules, optionally captured once as a CUDA graph (liberi_c_batch_*)."""
+
+    def __init__(self, handles):
+        self.handles = list(handles)
+        arr = (ctypes.c_void_p * len(self.handles))(*[h.ptr.value for h in self.handles])
+        self._b = ctypes.c_void_p()
+        _check(lib().liberi_c_batch_create(ctypes.byref(self._b), arr, len(self.handles)))
+
+    def bind(self, d_density_ptrs, d_fock_ptrs):
+        n = len(self.handles)
+        dp = (ctypes.c_void_p * n)(*d_density_ptrs)
+        fp = (ctypes.c_void_p * n)(*d_fock_ptrs)
+        _check(lib().liberi_c_batch_bind(self._b, dp, fp))
+
+    def fock_build(self, stream_ptr=0):
+        _check(lib().liberi_c_batch_fock_build(self._b, ctypes.c_void_p(stream_ptr)))
+
+    def capture(self):
+        _check(lib().liberi_c_batch_capture(self._b))
+
+    def launch(self, stream_ptr=0):
+        _check(lib().liberi_c_batch_launch(self._b, ctypes.c_void_p(stream_ptr)))
+
+    def synchronize(self):
+        _check(lib().liberi_c_batch_synchronize(self._b))
+
+    def autotune(self, reps=3):
+        out = np.zeros(21, dtype=np.int32)
+        _check(lib().liberi_c_batch_autotune(self._b, int(reps), out.ctypes.data_as(_I32P)))
+        return out
+
+    def destroy(self):
+        if self._b:
+            _check(lib().liberi_c_batch_destroy(self._b))
+            self._b = ctypes.c_void_p()
 
 
 def rys_eval(n, T, thr=60.0, strict=False):

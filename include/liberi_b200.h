@@ -152,6 +152,34 @@ typedef struct {
 } liberi_stats;
 int liberi_c_get_stats(liberi_handle handle, liberi_stats *stats);
 
+/* Batched Fock builds over several set-up handles (one molecule each): one
+ * launch per quartet class covers every molecule (a persistent multi-molecule
+ * work list), preceded by one launch that zeroes every F.  No counterpart in
+ * the reference.  Handles must share device and cuts, use FP64 and one rank.
+ *   bind:     device density / Fock buffer of every molecule (kept by address);
+ *   fock_build: enqueue one SCF iteration of all molecules on `stream` (NULL:
+ *             the batch's own stream);
+ *   capture / launch: record that iteration once as a CUDA graph and replay it;
+ *   autotune: time each class at 128..2048 kets per CTA task, keep the
+ *             fastest (chunks_out[21] may be NULL), re-capture if captured.
+ * The batch reads each handle's plans as they are at create: changing a
+ * handle's options, setting it up again or cleaning it up afterwards needs a
+ * new batch.  Destroy the batch before its handles. */
+typedef struct liberi_batch_s *liberi_batch;
+int liberi_c_batch_create(liberi_batch *batch, const liberi_handle *handles, int32_t n);
+int liberi_c_batch_bind(liberi_batch batch, const double *const *d_density, double *const *d_fock);
+int liberi_c_batch_fock_build(liberi_batch batch, void *stream);
+int liberi_c_batch_capture(liberi_batch batch);
+int liberi_c_batch_launch(liberi_batch batch, void *stream);
+int liberi_c_batch_synchronize(liberi_batch batch);
+int liberi_c_batch_autotune(liberi_batch batch, int32_t reps, int32_t *chunks_out);
+int liberi_c_batch_destroy(liberi_batch batch);
+
+/* Autotuner for one handle: per class, the fastest of 128..2048 kets per CTA
+ * task on the handle's own device buffers (their contents are overwritten);
+ * the plan is rebuilt with the choice.  No counterpart in the reference. */
+int liberi_c_autotune(liberi_handle handle, int32_t reps, int32_t *chunks_out);
+
 /* Rys roots u_i = t_i^2 and weights w_i (sum w_i = F_0(T)) for n = 1..5 from
  * the engine's piecewise tables, evaluated on the host exactly as the device
  * does; the large-T limit is used for T > thr (strict) or T >= thr. */
