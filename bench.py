@@ -328,9 +328,12 @@ def run_ours(args):
             for _ in range(2):
                 step()
             m_ms = max_over_ranks(timed_loop(max(3, args.steps // 2))[0])
+            st_m = h.stats()
+            f32 = float(st_m["fp32_quartets"].sum()) / max(1.0, float(st_m["quartets"].sum()))
             dF = (F - F_fp64).abs().max().item()
             dE = 0.5 * abs(float(torch.dot(F - F_fp64, _weights(D))))
             sweep.append({"fp32_cut": cut, "ms": round(m_ms, 3), "speedup_vs_fp64": round(ms / m_ms, 3),
+                          "fp32_quartet_share": round(f32, 4),
                           "max_dF_vs_fp64": dF, "dE_vs_fp64": dE})
         h.set_option("precision", 0)
         mixed = {"reference_path": "plain FP64 GPU build (parity-tested against the oracle to 1e-10)",

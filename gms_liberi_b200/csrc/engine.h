@@ -32,6 +32,18 @@ __host__ __device__ constexpr int rys_herm_off(int n) {
     return rys_table_off(MAXROOT + 1) + (n - 1) * 2 * MAXROOT;
 }
 constexpr int RYS_TABLE_SIZE = rys_herm_off(MAXROOT + 1);
+// Single-precision tables for the FP32 tier: intervals of width 1/4 on
+// [0, RYS_TMAX), degree-7 power basis in x = 2(4T - k) - 1 (8 coefficients,
+// two float4 loads per function); then the large-T limit as above, in float.
+constexpr int RYSF_PER_UNIT = 4;
+constexpr int RYSF_NINT = 60 * RYSF_PER_UNIT;
+constexpr int RYSF_DEG = 7;
+constexpr int RYSF_NCOEF = 8;
+__host__ __device__ constexpr int rysf_table_off(int n) { return RYSF_NINT * RYSF_NCOEF * n * (n - 1); }
+__host__ __device__ constexpr int rysf_herm_off(int n) {
+    return rysf_table_off(MAXROOT + 1) + (n - 1) * 2 * MAXROOT;
+}
+constexpr int RYSF_TABLE_SIZE = rysf_herm_off(MAXROOT + 1);
 
 enum PairClass { SS = 0, SP, PP, SD, PD, DD, NPC };
 enum Op { OP_GE = 0, OP_GT = 1, OP_NONE = 2 };
@@ -63,6 +75,8 @@ struct DevBasis {
     const int *pair_nprim;     // number of kept primitive pairs
     const double4 *prim_P;     // Px, Py, Pz, p
     const double2 *prim_X;     // sqrt(2 pi^2.5) c_a c_b exp(-mu R^2) / p, 0.5 / p
+    const float4 *prim_Pf;     // FP32 tier: Px, Py, Pz, p
+    const float4 *prim_Af;     // FP32 tier: P - A (x, y, z; rounded once from FP64), prefactor
 };
 
 // One launch of a class: a list of CTA tasks (bra position, first ket
@@ -146,6 +160,7 @@ struct DeviceBuffers {
     int *pair_prim0 = nullptr, *pair_nprim = nullptr;
     double4 *prim_P = nullptr;
     double2 *prim_X = nullptr;
+    float4 *prim_Pf = nullptr, *prim_Af = nullptr;
     double *D = nullptr, *F = nullptr;
     long long *scratch_total = nullptr;  // device counters (mixed split)
     size_t bytes = 0;
@@ -153,11 +168,13 @@ struct DeviceBuffers {
 
 // Rys root/weight tables (host generated once, uploaded per handle), layout above
 const std::vector<double> &rys_table_host();
+const std::vector<float> &rys_table_f32_host();
 
 // Launchers (kernels.cu) ------------------------------------------------------
 struct LaunchCtx {
     DevBasis basis;
     const double *rys_tab;
+    const float *rys_tabf;
     const double *D;
     double *F;
     double schwarz_cut, eri_cut;

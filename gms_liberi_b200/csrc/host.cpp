@@ -122,6 +122,7 @@ struct liberi_handle_s {
     PlanHost plan[NKERN];
     DeviceBuffers dev;
     double *d_tab = nullptr;
+    float *d_tabf = nullptr;
     unsigned long long *d_maxd = nullptr;
     cudaStream_t stream = nullptr;
     int num_sms = 148;
@@ -156,6 +157,7 @@ static void free_device(liberi_handle h) {
     h->allocs.clear();
     h->dev = DeviceBuffers();
     h->d_tab = nullptr;
+    h->d_tabf = nullptr;
     h->d_maxd = nullptr;
     for (int k = 0; k < NKERN; k++) h->plan[k] = PlanHost();
     if (h->stream) {
@@ -430,8 +432,24 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
     CUDA_TRY(dev_upload(h, &h->dev.pair_nprim, h->pairs.nprim.data(), h->pairs.nprim.size()));
     CUDA_TRY(dev_upload(h, &h->dev.prim_P, h->pairs.P.data(), h->pairs.P.size()));
     CUDA_TRY(dev_upload(h, &h->dev.prim_X, h->pairs.X.data(), h->pairs.X.size()));
+    {  // FP32 tier copies: P - A is formed in FP64 and rounded once
+        const PairsHost &pr = h->pairs;
+        std::vector<float4> pf(pr.P.size()), af(pr.P.size());
+        for (size_t q = 0; q < pr.shell.size(); q++) {
+            const double4 A = shell_xyz[pr.shell[q].x];
+            for (int k = pr.prim0[q]; k < pr.prim0[q] + pr.nprim[q]; k++) {
+                const double4 P = pr.P[k];
+                pf[k] = make_float4((float)P.x, (float)P.y, (float)P.z, (float)P.w);
+                af[k] = make_float4((float)(P.x - A.x), (float)(P.y - A.y), (float)(P.z - A.z), (float)pr.X[k].x);
+            }
+        }
+        CUDA_TRY(dev_upload(h, &h->dev.prim_Pf, pf.data(), pf.size()));
+        CUDA_TRY(dev_upload(h, &h->dev.prim_Af, af.data(), af.size()));
+    }
     const std::vector<double> &tab = rys_table_host();
     CUDA_TRY(dev_upload(h, &h->d_tab, tab.data(), tab.size()));
+    const std::vector<float> &tabf = rys_table_f32_host();
+    CUDA_TRY(dev_upload(h, &h->d_tabf, tabf.data(), tabf.size()));
     const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
     CUDA_TRY(dev_alloc(h, &h->dev.D, ntri));
     CUDA_TRY(dev_alloc(h, &h->dev.F, ntri));
@@ -448,6 +466,8 @@ static DevBasis dev_basis(liberi_handle h) {
     d.pair_nprim = h->dev.pair_nprim;
     d.prim_P = h->dev.prim_P;
     d.prim_X = h->dev.prim_X;
+    d.prim_Pf = h->dev.prim_Pf;
+    d.prim_Af = h->dev.prim_Af;
     return d;
 }
 
@@ -491,6 +511,7 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     LaunchCtx ctx;
     ctx.basis = dev_basis(h);
     ctx.rys_tab = h->d_tab;
+    ctx.rys_tabf = h->d_tabf;
     ctx.D = dD;
     ctx.F = dF;
     ctx.schwarz_cut = h->schwarz_cut;
@@ -630,6 +651,7 @@ static int batch_enqueue(liberi_batch b, cudaStream_t st, uint32_t mask) {
     LaunchCtx ctx;
     ctx.basis = DevBasis{};
     ctx.rys_tab = h0->d_tab;
+    ctx.rys_tabf = h0->d_tabf;
     ctx.D = nullptr;
     ctx.F = nullptr;
     ctx.schwarz_cut = h0->schwarz_cut;
@@ -679,6 +701,34 @@ int liberi_c_rys_eval(int32_t n, double T, double thr, int32_t strict, double *u
         const double b0 = std::fma(a1, x2, a0), b1 = std::fma(a3, x2, a2), b2 = std::fma(a5, x2, a4);
         const double d0 = std::fma(b1, x4, b0), d1 = std::fma(c[12], x4, b2);
         const double v = std::fma(d1, x8, d0);
+        if (f < n) u[f] = v; else w[f - n] = v;
+    }
+    return LIBERI_OK;
+}
+
+int liberi_c_rys_eval_f32(int32_t n, float T, float thr, int32_t strict, float *u, float *w) {
+    if (n < 1 || n > MAXROOT || !u || !w || !(T >= 0.0f)) return fail(LIBERI_E_ARG, "liberi_rys_eval_f32: bad argument");
+    const std::vector<float> &tab = rys_table_f32_host();
+    const bool asym = strict ? (T > thr) : (T >= thr);
+    if (asym || T >= (float)RYS_TMAX) {
+        const float it = 1.0f / T, sq = std::sqrt(it);
+        for (int i = 0; i < n; i++) {
+            u[i] = tab[rysf_herm_off(n) + i] * it;
+            w[i] = tab[rysf_herm_off(n) + MAXROOT + i] * sq;
+        }
+        return LIBERI_OK;
+    }
+    const float t4 = T * (float)RYSF_PER_UNIT;
+    const int k = (int)t4;
+    const float x = 2.0f * (t4 - (float)k) - 1.0f;
+    const float *base = tab.data() + rysf_table_off(n) + (size_t)k * 2 * n * RYSF_NCOEF;
+    const float x2 = x * x, x4 = x2 * x2;
+    for (int f = 0; f < 2 * n; f++) {  // same Estrin scheme as the device
+        const float *c = base + f * RYSF_NCOEF;
+        const float a0 = std::fmaf(c[1], x, c[0]), a1 = std::fmaf(c[3], x, c[2]);
+        const float a2 = std::fmaf(c[5], x, c[4]), a3 = std::fmaf(c[7], x, c[6]);
+        const float b0 = std::fmaf(a1, x2, a0), b1 = std::fmaf(a3, x2, a2);
+        const float v = std::fmaf(b1, x4, b0);
         if (f < n) u[f] = v; else w[f - n] = v;
     }
     return LIBERI_OK;

@@ -106,6 +106,7 @@ cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const
     ClassArgs a;
     a.b = ctx.basis;
     a.tab = ctx.rys_tab;
+    a.tabf = ctx.rys_tabf;
     a.Dm = ctx.D;
     a.F = ctx.F;
     a.cut = kd.digest_schwarz ? ctx.schwarz_cut : ctx.eri_cut;
@@ -137,6 +138,7 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     ClassArgs a{};
     a.b = DevBasis{};
     a.tab = ctx.rys_tab;
+    a.tabf = ctx.rys_tabf;
     a.Dm = nullptr;
     a.F = nullptr;
     a.cut = kd.digest_schwarz ? ctx.schwarz_cut : ctx.eri_cut;

@@ -21,11 +21,14 @@
 //        J update of the row pair (A,B)   -> warp-reduced, then the tile
 //        J update of the ket pair (C,D)   -> FP64 global atomics
 //      and the tile is flushed to F with FP64 atomics when the CTA ends.
-// The FP32 instantiation evaluates step 1 in single precision (roots,
-// weights and pair prefactors stay FP64) for the quartets whose Schwarz bound
-// falls below the mixed-precision cut; step 2 always accumulates in FP64.
+// The FP32 instantiation evaluates step 1 entirely in single precision (pair
+// data rounded once from FP64, Rys roots and weights from single-precision
+// tables, recurrences and contraction) for the quartets whose Schwarz bound
+// times max|D| falls below the mixed-precision cut; step 2 always digests in
+// FP64.
 #pragma once
 #include <cstdio>
+#include <type_traits>
 
 #include "engine.h"
 
@@ -80,6 +83,38 @@ __device__ __forceinline__ void rys_eval(double T, double thr, bool strict,
         const double b0 = fma(a1, x2, a0), b1 = fma(a3, x2, a2), b2 = fma(a5, x2, a4);
         const double d0 = fma(b1, x4, b0), d1 = fma(ccd.x, x4, b2);
         const double v = fma(d1, x8, d0);
+        if (f < N) u[f] = v; else w[f - N] = v;
+    }
+}
+
+// FP32 tier: width-1/4 intervals, degree 7 (Estrin, two float4 loads per
+// function); the large-T limit as in FP64.
+template <int N>
+__device__ __forceinline__ void rys_eval(float T, float thr, bool strict, const float *__restrict__ tab, float *u,
+                                         float *w) {
+    bool asym = strict ? (T > thr) : (T >= thr);
+    if (asym) {
+        const float sq = rsqrtf(T), it = sq * sq;
+        const float *hr = tab + rysf_herm_off(N);
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            u[i] = __ldg(hr + i) * it;
+            w[i] = __ldg(hr + MAXROOT + i) * sq;
+        }
+        return;
+    }
+    const float t4 = T * (float)RYSF_PER_UNIT;
+    const int k = (int)t4;
+    const float x = 2.0f * (t4 - (float)k) - 1.0f;
+    const float4 *base = reinterpret_cast<const float4 *>(tab + rysf_table_off(N)) + (size_t)k * (N * RYSF_NCOEF / 2);
+    const float x2 = x * x, x4 = x2 * x2;
+#pragma unroll
+    for (int f = 0; f < 2 * N; f++) {
+        const float4 c0 = __ldg(base + 2 * f), c1 = __ldg(base + 2 * f + 1);
+        const float a0 = fmaf(c0.y, x, c0.x), a1 = fmaf(c0.w, x, c0.z);
+        const float a2 = fmaf(c1.y, x, c1.x), a3 = fmaf(c1.w, x, c1.z);
+        const float b0 = fmaf(a1, x2, a0), b1 = fmaf(a3, x2, a2);
+        const float v = fmaf(b1, x4, b0);
         if (f < N) u[f] = v; else w[f - N] = v;
     }
 }
@@ -185,6 +220,54 @@ __device__ __forceinline__ void hrr_slice(const R (&g)[LA + LB + 1][LC + LD + 1]
     }
 }
 
+// One root's contribution: horizontal transfer of the three 2D blocks and
+// accumulation of the contracted Cartesian block (all A components of the
+// pass at compile-time indices when the pass covers all of A).
+template <int LA, int LB, int LC, int LD, typename R, int NMU>
+__device__ __forceinline__ void contract_root(const R (&gx)[LA + LB + 1][LC + LD + 1],
+                                              const R (&gy)[LA + LB + 1][LC + LD + 1],
+                                              const R (&gz)[LA + LB + 1][LC + LD + 1], R abx, R aby, R abz,
+                                              R cdx, R cdy, R cdz, const int (&ex)[NMU], const int (&ey)[NMU],
+                                              const int (&ez)[NMU], R (&acc)[NMU][ncart(LB)][ncart(LC)][ncart(LD)]) {
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    constexpr bool FULL = (NMU == NA);
+    if constexpr (FULL) {
+        R ix[LA + 1][LB + 1][LC + 1][LD + 1], iy[LA + 1][LB + 1][LC + 1][LD + 1],
+            iz[LA + 1][LB + 1][LC + 1][LD + 1];
+        hrr<LA, LB, LC, LD, R>(gx, abx, cdx, ix);
+        hrr<LA, LB, LC, LD, R>(gy, aby, cdy, iy);
+        hrr<LA, LB, LC, LD, R>(gz, abz, cdz, iz);
+#pragma unroll
+        for (int m = 0; m < NMU; m++)
+#pragma unroll
+            for (int ib = 0; ib < NB; ib++)
+#pragma unroll
+                for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                    for (int id = 0; id < ND; id++)
+                        acc[m][ib][ic][id] += ix[cxp(LA, m)][cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)] *
+                                              iy[cyp(LA, m)][cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)] *
+                                              iz[czp(LA, m)][czp(LB, ib)][czp(LC, ic)][czp(LD, id)];
+    } else {
+#pragma unroll
+        for (int m = 0; m < NMU; m++) {
+            R sx[LB + 1][LC + 1][LD + 1], sy[LB + 1][LC + 1][LD + 1], sz[LB + 1][LC + 1][LD + 1];
+            hrr_slice<LA, LB, LC, LD, R>(gx, ex[m], abx, cdx, sx);
+            hrr_slice<LA, LB, LC, LD, R>(gy, ey[m], aby, cdy, sy);
+            hrr_slice<LA, LB, LC, LD, R>(gz, ez[m], abz, cdz, sz);
+#pragma unroll
+            for (int ib = 0; ib < NB; ib++)
+#pragma unroll
+                for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                    for (int id = 0; id < ND; id++)
+                        acc[m][ib][ic][id] += sx[cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)] *
+                                              sy[cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)] *
+                                              sz[czp(LB, ib)][czp(LC, ic)][czp(LD, id)];
+        }
+    }
+}
+
 // acc[m][ib][ic][id] for A components ia = mu0 + m (m < NMU, ia < NA), all of
 // B, C, D.  A single pass (NMU == NA) uses compile-time component indices; a
 // multi-pass class selects the A exponent at run time, so one copy of the
@@ -193,8 +276,8 @@ template <int LA, int LB, int LC, int LD, typename R, int NMU>
 __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, int q0, int nq,
                                            const double4 &A, const double4 &C, R abx, R aby, R abz,
                                            R cdx, R cdy, R cdz, double thr, bool strict,
-                                           const double *__restrict__ tab, int mu0,
-                                           R (&acc)[NMU][ncart(LB)][ncart(LC)][ncart(LD)]) {
+                                           const double *__restrict__ tab, const float *__restrict__ tabf,
+                                           int mu0, R (&acc)[NMU][ncart(LB)][ncart(LC)][ncart(LD)]) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr int LAB = LA + LB, LCD = LC + LD;
     constexpr int NR = (LAB + LCD) / 2 + 1;
@@ -215,72 +298,76 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
             for (int ic = 0; ic < NC; ic++)
 #pragma unroll
                 for (int id = 0; id < ND; id++) acc[m][ib][ic][id] = R(0);
-    for (int kq = q0; kq < q0 + nq; kq++) {
-        const double4 Qp = b.prim_P[kq];
-        const double2 Qx = b.prim_X[kq];
-        const double q = Qp.w, hq = Qx.y;
-        for (int kp = p0; kp < p0 + np; kp++) {
-            const double4 Pp = b.prim_P[kp];
-            const double2 Px = b.prim_X[kp];
-            const double p = Pp.w, hp = Px.y;
-            const double rs = rsqrt(p + q);
-            const double ipq = rs * rs;
-            const double pqx = Pp.x - Qp.x, pqy = Pp.y - Qp.y, pqz = Pp.z - Qp.z;
-            const double T = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
-            double u[NR], w[NR];
-            rys_eval<NR>(T, thr, strict, tab, u, w);
-            const double pref = Px.x * Qx.x * rs;
+    if constexpr (std::is_same<R, double>::value) {
+        for (int kq = q0; kq < q0 + nq; kq++) {
+            const double4 Qp = b.prim_P[kq];
+            const double2 Qx = b.prim_X[kq];
+            const double q = Qp.w, hq = Qx.y;
+            for (int kp = p0; kp < p0 + np; kp++) {
+                const double4 Pp = b.prim_P[kp];
+                const double2 Px = b.prim_X[kp];
+                const double p = Pp.w, hp = Px.y;
+                const double rs = rsqrt(p + q);
+                const double ipq = rs * rs;
+                const double pqx = Pp.x - Qp.x, pqy = Pp.y - Qp.y, pqz = Pp.z - Qp.z;
+                const double T = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
+                double u[NR], w[NR];
+                rys_eval<NR>(T, thr, strict, tab, u, w);
+                const double pref = Px.x * Qx.x * rs;
 #pragma unroll(FULL ? NR : 1)
-            for (int r = 0; r < NR; r++) {
-                const double ui = u[0] * ipq, wr = w[0];
+                for (int r = 0; r < NR; r++) {
+                    const double ui = u[0] * ipq, wr = w[0];
 #pragma unroll
-                for (int i = 0; i + 1 < NR; i++) {  // rotate the next root to the front
-                    u[i] = u[i + 1];
-                    w[i] = w[i + 1];
-                }
-                const double fq = q * ui, fp = p * ui;
-                const R b00 = R(0.5 * ui);
-                const R b10 = R(hp * (1.0 - fq));
-                const R b01 = R(hq * (1.0 - fp));
-                R gx[LAB + 1][LCD + 1], gy[LAB + 1][LCD + 1], gz[LAB + 1][LCD + 1];
-                vrr<LAB, LCD, R>(gx, R((Pp.x - A.x) - fq * pqx), R((Qp.x - C.x) + fp * pqx), b10, b01, b00, R(1));
-                vrr<LAB, LCD, R>(gy, R((Pp.y - A.y) - fq * pqy), R((Qp.y - C.y) + fp * pqy), b10, b01, b00, R(1));
-                vrr<LAB, LCD, R>(gz, R((Pp.z - A.z) - fq * pqz), R((Qp.z - C.z) + fp * pqz), b10, b01, b00,
-                                 R(wr * pref));
-                if constexpr (FULL) {
-                    R ix[LA + 1][LB + 1][LC + 1][LD + 1], iy[LA + 1][LB + 1][LC + 1][LD + 1],
-                        iz[LA + 1][LB + 1][LC + 1][LD + 1];
-                    hrr<LA, LB, LC, LD, R>(gx, abx, cdx, ix);
-                    hrr<LA, LB, LC, LD, R>(gy, aby, cdy, iy);
-                    hrr<LA, LB, LC, LD, R>(gz, abz, cdz, iz);
-#pragma unroll
-                    for (int m = 0; m < NMU; m++)
-#pragma unroll
-                        for (int ib = 0; ib < NB; ib++)
-#pragma unroll
-                            for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-                                for (int id = 0; id < ND; id++)
-                                    acc[m][ib][ic][id] += ix[cxp(LA, m)][cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)] *
-                                                          iy[cyp(LA, m)][cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)] *
-                                                          iz[czp(LA, m)][czp(LB, ib)][czp(LC, ic)][czp(LD, id)];
-                } else {
-#pragma unroll
-                    for (int m = 0; m < NMU; m++) {
-                        R sx[LB + 1][LC + 1][LD + 1], sy[LB + 1][LC + 1][LD + 1], sz[LB + 1][LC + 1][LD + 1];
-                        hrr_slice<LA, LB, LC, LD, R>(gx, ex[m], abx, cdx, sx);
-                        hrr_slice<LA, LB, LC, LD, R>(gy, ey[m], aby, cdy, sy);
-                        hrr_slice<LA, LB, LC, LD, R>(gz, ez[m], abz, cdz, sz);
-#pragma unroll
-                        for (int ib = 0; ib < NB; ib++)
-#pragma unroll
-                            for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-                                for (int id = 0; id < ND; id++)
-                                    acc[m][ib][ic][id] += sx[cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)] *
-                                                          sy[cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)] *
-                                                          sz[czp(LB, ib)][czp(LC, ic)][czp(LD, id)];
+                    for (int i = 0; i + 1 < NR; i++) {  // rotate the next root to the front
+                        u[i] = u[i + 1];
+                        w[i] = w[i + 1];
                     }
+                    const double fq = q * ui, fp = p * ui;
+                    const R b00 = R(0.5 * ui);
+                    const R b10 = R(hp * (1.0 - fq));
+                    const R b01 = R(hq * (1.0 - fp));
+                    R gx[LAB + 1][LCD + 1], gy[LAB + 1][LCD + 1], gz[LAB + 1][LCD + 1];
+                    vrr<LAB, LCD, R>(gx, R((Pp.x - A.x) - fq * pqx), R((Qp.x - C.x) + fp * pqx), b10, b01, b00, R(1));
+                    vrr<LAB, LCD, R>(gy, R((Pp.y - A.y) - fq * pqy), R((Qp.y - C.y) + fp * pqy), b10, b01, b00, R(1));
+                    vrr<LAB, LCD, R>(gz, R((Pp.z - A.z) - fq * pqz), R((Qp.z - C.z) + fp * pqz), b10, b01, b00,
+                                     R(wr * pref));
+                    contract_root<LA, LB, LC, LD, R, NMU>(gx, gy, gz, abx, aby, abz, cdx, cdy, cdz, ex, ey, ez, acc);
+                }
+            }
+        }
+    } else {
+        // FP32 tier: pair data, roots and recurrences in single precision
+        const float4 *__restrict__ Pf = b.prim_Pf;
+        const float4 *__restrict__ Af = b.prim_Af;
+        const float thrf = (float)thr;
+        for (int kq = q0; kq < q0 + nq; kq++) {
+            const float4 Qp = __ldg(Pf + kq), Qa = __ldg(Af + kq);
+            const float q = Qp.w, hq = __fdividef(0.5f, q);
+            for (int kp = p0; kp < p0 + np; kp++) {
+                const float4 Pp = __ldg(Pf + kp), Pa = __ldg(Af + kp);
+                const float p = Pp.w, hp = __fdividef(0.5f, p);
+                const float rs = rsqrtf(p + q);
+                const float ipq = rs * rs;
+                const float pqx = Pp.x - Qp.x, pqy = Pp.y - Qp.y, pqz = Pp.z - Qp.z;
+                const float T = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
+                float u[NR], w[NR];
+                rys_eval<NR>(T, thrf, strict, tabf, u, w);
+                const float pref = Pa.w * Qa.w * rs;
+#pragma unroll(FULL ? NR : 1)
+                for (int r = 0; r < NR; r++) {
+                    const float ui = u[0] * ipq, wr = w[0];
+#pragma unroll
+                    for (int i = 0; i + 1 < NR; i++) {
+                        u[i] = u[i + 1];
+                        w[i] = w[i + 1];
+                    }
+                    const float fq = q * ui, fp = p * ui;
+                    const float b00 = 0.5f * ui, b10 = hp * (1.0f - fq), b01 = hq * (1.0f - fp);
+                    R gx[LAB + 1][LCD + 1], gy[LAB + 1][LCD + 1], gz[LAB + 1][LCD + 1];
+                    vrr<LAB, LCD, R>(gx, Pa.x - fq * pqx, Qa.x + fp * pqx, b10, b01, b00, 1.0f);
+                    vrr<LAB, LCD, R>(gy, Pa.y - fq * pqy, Qa.y + fp * pqy, b10, b01, b00, 1.0f);
+                    vrr<LAB, LCD, R>(gz, Pa.z - fq * pqz, Qa.z + fp * pqz, b10, b01, b00, wr * pref);
+                    contract_root<LA, LB, LC, LD, R, NMU>(gx, gy, gz, abx, aby, abz, cdx, cdy, cdz, ex, ey, ez, acc);
                 }
             }
         }
@@ -386,16 +473,38 @@ constexpr int tuned_minb(int key) {
     }
 }
 
-template <int LA, int LB, int LC, int LD>
+// FP32 tier shapes (half the register footprint per value); 0 / default
+// falls back to the FP64 choice.  LIBERI_TUNE_* with LIBERI_TUNE_F32 override
+// one class of this table for the offline search.
+constexpr int tuned_nmu_f32(int key) {
+#ifdef LIBERI_TUNE_KEY
+    if (key == LIBERI_TUNE_KEY) return LIBERI_TUNE_NMU;
+#endif
+    switch (key) {
+        default: return tuned_nmu(key);
+    }
+}
+constexpr int tuned_minb_f32(int key) {
+#ifdef LIBERI_TUNE_KEY
+    if (key == LIBERI_TUNE_KEY) return LIBERI_TUNE_MINB;
+#endif
+    switch (key) {
+        default: return tuned_minb(key);
+    }
+}
+
+template <int LA, int LB, int LC, int LD, typename R>
 struct PassShape {
+    static constexpr bool F32 = std::is_same<R, float>::value;
+    static constexpr int KEY = class_key(LA, LB, LC, LD);
     static constexpr int PER_MU = ncart(LB) * ncart(LC) * ncart(LD);
     static constexpr int NA = ncart(LA);
     static constexpr int NMU_DEF = PER_MU >= 40 ? 1 : (40 / PER_MU);
-    static constexpr int NMU_T =
-        tuned_nmu(class_key(LA, LB, LC, LD)) > 0 ? tuned_nmu(class_key(LA, LB, LC, LD)) : NMU_DEF;
+    static constexpr int NMU_TUNED = F32 ? tuned_nmu_f32(KEY) : tuned_nmu(KEY);
+    static constexpr int NMU_T = NMU_TUNED > 0 ? NMU_TUNED : NMU_DEF;
     static constexpr int NMU = NMU_T > NA ? NA : NMU_T;
     static constexpr int NPASS = (NA + NMU - 1) / NMU;
-    static constexpr int MINB = tuned_minb(class_key(LA, LB, LC, LD));
+    static constexpr int MINB = F32 ? tuned_minb_f32(KEY) : tuned_minb(KEY);
 };
 
 constexpr int CLASS_THREADS = 128;
@@ -423,16 +532,17 @@ template <int LA, int LB, int LC, int LD, typename R, typename KB>
 __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, int q0, int nq, const double4 &A,
                                            const double4 &C, R abx, R aby, R abz, R cdx, R cdy, R cdz,
                                            double thr, bool strict, const double *__restrict__ tab,
-                                           const QuartetCtx &qc, const Rows &rows, KB &kb) {
+                                           const float *__restrict__ tabf, const QuartetCtx &qc,
+                                           const Rows &rows, KB &kb) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    using PS = PassShape<LA, LB, LC, LD>;
+    using PS = PassShape<LA, LB, LC, LD, R>;
     constexpr int M = PS::NMU;
     constexpr bool can_same = (LA == LC) && (LB == LD);
 #pragma unroll 1
     for (int pass = 0; pass < PS::NPASS; pass++) {
         const int mu0 = pass * M;
         R acc[M][NB][NC][ND];
-        eval_block<LA, LB, LC, LD, R, M>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict, tab,
+        eval_block<LA, LB, LC, LD, R, M>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict, tab, tabf,
                                          mu0, acc);
 #pragma unroll
         for (int m = 0; m < M; m++) {
@@ -513,6 +623,7 @@ __device__ __forceinline__ bool rank_owns(const RankSplit &rs, long long it) {
 struct ClassArgs {
     DevBasis b;
     const double *tab;
+    const float *tabf;
     const double *Dm;
     double *F;
     double cut;
@@ -604,13 +715,13 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
         qc.bfC = bas.shell_bf0[scd.x]; qc.bfD = bas.shell_bf0[scd.y];
         qc.iandj = sab.x == sab.y; qc.kandl = scd.x == scd.y; qc.same = P == Qd;
         qc.cut = a.cut; qc.Dm = LIBERI_D;
-        constexpr bool SM = PassShape<LA, LB, LC, LD>::NPASS > 1;
+        constexpr bool SM = PassShape<LA, LB, LC, LD, R>::NPASS > 1;
         KBuf<NB, NC, ND, SM> kb;
         kb.s = slots + threadIdx.x;
 #pragma unroll
         for (int i = 0; i < KBuf<NB, NC, ND, SM>::N; i++) kb.at(i) = 0.0;
         run_passes<LA, LB, LC, LD, R>(bas, p0, np, bas.pair_prim0[Qd], bas.pair_nprim[Qd], A, C, abx, aby, abz,
-                                      cdx, cdy, cdz, a.thr, a.strict, a.tab, qc, rowsA, kb);
+                                      cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
 #pragma unroll
@@ -644,7 +755,7 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
 // BATCH: the task's w field selects the molecule (basis, D, F, plan lists);
 // the launch sized the shared-memory tile for the largest molecule.
 template <int LA, int LB, int LC, int LD, typename R, bool BATCH>
-__global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD>::MINB) class_kernel(ClassArgs a) {
+__global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD, R>::MINB) class_kernel(ClassArgs a) {
     const int ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
     if ((int)blockIdx.x >= ntasks) return;
     const int4 t = a.tasks[blockIdx.x];
@@ -664,7 +775,7 @@ __device__ __forceinline__ double schwarz_diag(const DevBasis &b, int P, const d
     for (int ia = 0; ia < NA; ia++) {
         double acc[1][NB][NA][NB];
         eval_block<LA, LB, LA, LB, double, 1>(b, p0, np, p0, np, A, A, abx, aby, abz, abx, aby, abz, RYS_TMAX,
-                                              false, tab, ia, acc);
+                                              false, tab, nullptr, ia, acc);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
             double v = 0.0;
@@ -677,38 +788,31 @@ __device__ __forceinline__ double schwarz_diag(const DevBasis &b, int P, const d
     return sqrt(m);
 }
 
-template <int LA, int LB, int LC, int LD>
-cudaError_t launch_t(const ClassArgs &a, int precision, cudaStream_t st) {
-    if (a.ntasks <= 0) return cudaSuccess;
+template <int LA, int LB, int LC, int LD, typename R, bool BATCH>
+cudaError_t launch_shape(const ClassArgs &a, cudaStream_t st) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    constexpr bool SM = PassShape<LA, LB, LC, LD>::NPASS > 1;
+    constexpr bool SM = PassShape<LA, LB, LC, LD, R>::NPASS > 1;
     const size_t slot_bytes = SM ? (size_t)KBuf<NB, NC, ND, true>::N * CLASS_THREADS * sizeof(double) : 0;
     // the F-row tile is staged only when it fits beside the slots (227 KB per CTA)
     const size_t tile_bytes = (size_t)(NA + NB) * a.nbf * sizeof(double);
     ClassArgs args = a;
     args.tile_rows = (a.tile_rows && tile_bytes + slot_bytes <= 220 * 1024) ? 1 : 0;
     const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes;
-    // the opt-in limit is raised to the per-CTA maximum once per launch, not
-    // to this launch's size: a captured graph may hold a larger launch
-    const int smem_cap = 227 * 1024;
-    cudaError_t e;
-    if (a.mols) {
-        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, double, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap);
-        if (e != cudaSuccess) return e;
-        class_kernel<LA, LB, LC, LD, double, true><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
-    } else if (precision == 0) {
-        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, double, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap);
-        if (e != cudaSuccess) return e;
-        class_kernel<LA, LB, LC, LD, double, false><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
-    } else {
-        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, float, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap);
-        if (e != cudaSuccess) return e;
-        class_kernel<LA, LB, LC, LD, float, false><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
-    }
+    // the opt-in limit is raised to the per-CTA maximum, not to this launch's
+    // size: a captured graph may hold a larger launch
+    cudaError_t e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, R, BATCH>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    class_kernel<LA, LB, LC, LD, R, BATCH><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
     return cudaGetLastError();
+}
+
+template <int LA, int LB, int LC, int LD>
+cudaError_t launch_t(const ClassArgs &a, int precision, cudaStream_t st) {
+    if (a.ntasks <= 0) return cudaSuccess;
+    if (a.mols) return launch_shape<LA, LB, LC, LD, double, true>(a, st);
+    if (precision == 0) return launch_shape<LA, LB, LC, LD, double, false>(a, st);
+    return launch_shape<LA, LB, LC, LD, float, false>(a, st);
 }
 
 }  // namespace liberi

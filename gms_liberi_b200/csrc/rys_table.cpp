@@ -16,7 +16,9 @@
 //     scheme (15 FMAs, dependency depth 5) from 7 aligned double2 loads.
 // Interpolation error is ~1e-14 relative (checked by the unit tests against
 // the oracle's 35-point procedure).  Above the class threshold the device
-// uses the large-T (Gauss-Hermite) limit, built here as well.
+// uses the large-T (Gauss-Hermite) limit, built here as well.  A second,
+// single-precision set (intervals of width 1/4, degree 7) serves the FP32
+// tier of the mixed-precision build.
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -130,6 +132,70 @@ void exact_rys(const Grid &g, int n, double T, double *u, double *w) {
 
 std::vector<double> g_table;
 std::once_flag g_once;
+std::vector<float> g_table_f;
+std::once_flag g_once_f;
+
+// Chebyshev interpolation of f at the M nodes of [-1, 1], converted to the
+// power basis of x (coefficients 0..M-1).
+std::vector<double> cheb_to_power(const std::vector<double> &f) {
+    const int M = (int)f.size();
+    std::vector<double> c(M, 0.0);
+    for (int j = 0; j < M; j++) {
+        double s = 0.0;
+        for (int m = 0; m < M; m++) s += f[m] * std::cos(PI * j * (m + 0.5) / M);
+        c[j] = 2.0 * s / M;
+    }
+    c[0] *= 0.5;
+    std::vector<double> pw(M, 0.0), tprev(M, 0.0), tcur(M, 0.0);
+    tcur[0] = 1.0;
+    for (int j = 0; j < M; j++) {
+        if (j == 1) {
+            tprev = tcur;
+            std::fill(tcur.begin(), tcur.end(), 0.0);
+            tcur[1] = 1.0;
+        } else if (j > 1) {
+            std::vector<double> tn(M, 0.0);
+            for (int i = 0; i + 1 < M; i++) tn[i + 1] += 2.0 * tcur[i];
+            for (int i = 0; i < M; i++) tn[i] -= tprev[i];
+            tprev = tcur;
+            tcur = tn;
+        }
+        for (int i = 0; i < M; i++) pw[i] += c[j] * tcur[i];
+    }
+    return pw;
+}
+
+// FP32 tier: width-1/4 intervals, degree 7, so that the power-basis
+// coefficients stay small and single-precision evaluation keeps ~1e-7
+// relative accuracy.
+void build_tables_f32() {
+    Grid g;
+    const std::vector<double> &dt = rys_table_host();
+    g_table_f.assign(RYSF_TABLE_SIZE, 0.0f);
+    const int M = RYSF_DEG + 1;
+    std::vector<double> xs(M);
+    for (int m = 0; m < M; m++) xs[m] = std::cos(PI * (m + 0.5) / M);
+    for (int n = 1; n <= MAXROOT; n++) {
+        for (int k = 0; k < RYSF_NINT; k++) {
+            std::vector<std::vector<double>> f(2 * n, std::vector<double>(M));
+            for (int m = 0; m < M; m++) {
+                double T = (k + 0.5 * (xs[m] + 1.0)) / RYSF_PER_UNIT;
+                double u[MAXROOT], w[MAXROOT];
+                exact_rys(g, n, T, u, w);
+                for (int i = 0; i < n; i++) {
+                    f[i][m] = u[i];
+                    f[n + i][m] = w[i];
+                }
+            }
+            for (int fi = 0; fi < 2 * n; fi++) {
+                std::vector<double> pw = cheb_to_power(f[fi]);
+                float *dst = &g_table_f[rysf_table_off(n) + ((size_t)k * 2 * n + fi) * RYSF_NCOEF];
+                for (int i = 0; i < M; i++) dst[i] = (float)pw[i];
+            }
+        }
+        for (int i = 0; i < 2 * MAXROOT; i++) g_table_f[rysf_herm_off(n) + i] = (float)dt[rys_herm_off(n) + i];
+    }
+}
 
 void build_tables() {
     Grid g;
@@ -203,6 +269,11 @@ void build_tables() {
 const std::vector<double> &rys_table_host() {
     std::call_once(g_once, build_tables);
     return g_table;
+}
+
+const std::vector<float> &rys_table_f32_host() {
+    std::call_once(g_once_f, build_tables_f32);
+    return g_table_f;
 }
 
 

@@ -34,7 +34,7 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_schwarz_noalloc", "liberi_c_batch_create", "liberi_c_batch_bind",
            "liberi_c_batch_fock_build", "liberi_c_batch_capture", "liberi_c_batch_launch",
            "liberi_c_batch_synchronize", "liberi_c_batch_autotune", "liberi_c_batch_destroy",
-           "liberi_c_autotune"]
+           "liberi_c_autotune", "liberi_c_rys_eval_f32"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -91,6 +91,8 @@ def lib():
         L.liberi_c_rys_eval.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                         _F64P, _F64P]
         L.liberi_c_microbench.argtypes = [ctypes.c_int32, _F64P]
+        L.liberi_c_rys_eval_f32.argtypes = [ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                            ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         L.liberi_c_kernel_name.argtypes = [ctypes.c_int32]
         L.liberi_c_batch_create.argtypes = [ctypes.POINTER(H), ctypes.POINTER(H), ctypes.c_int32]
         L.liberi_c_batch_bind.argtypes = [H, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]
@@ -325,6 +327,15 @@ def rys_eval(n, T, thr=60.0, strict=False):
     w = np.zeros(n)
     _check(lib().liberi_c_rys_eval(n, T, thr, int(strict), u.ctypes.data_as(_F64P), w.ctypes.data_as(_F64P)))
     return u, w
+
+
+def rys_eval_f32(n, T, thr=60.0, strict=False):
+    """FP32-tier Rys roots/weights (host evaluation in single precision)."""
+    u = np.zeros(n, dtype=np.float32)
+    w = np.zeros(n, dtype=np.float32)
+    FP = ctypes.POINTER(ctypes.c_float)
+    _check(lib().liberi_c_rys_eval_f32(n, T, thr, int(strict), u.ctypes.data_as(FP), w.ctypes.data_as(FP)))
+    return u.astype(np.float64), w.astype(np.float64)
 
 
 def schwarz(basis):

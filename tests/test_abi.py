@@ -93,3 +93,17 @@ def test_engine_rys_tables_match_oracle(n):
         ue, we = liberi.rys_eval(n, T, thr=25.0, strict=True)
         uo, wo = oracle.rys_roots(n, T, thr=25.0, rot=True)
         assert np.allclose(ue, uo, rtol=1e-14) and np.allclose(we, wo, rtol=1e-14)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5])
+def test_engine_fp32_rys_tables(n):
+    # the FP32 tier's tables, evaluated in single precision as on the device:
+    # relative error within a few float ulps of the reference roots/weights
+    from oracle import oracle
+    rng = np.random.default_rng(100 + n)
+    worst = 0.0
+    for T in np.concatenate([[0.0, 1e-6, 0.25, 0.5, 24.999, 42.99, 59.99], rng.uniform(0, 60, 200)]):
+        uf, wf = liberi.rys_eval_f32(n, float(T), thr=60.0)
+        uo, wo = oracle.rys_roots(n, float(np.float32(T)), thr=60.0)
+        worst = max(worst, np.max(np.abs(uf - uo) / np.abs(uo)), np.max(np.abs(wf - wo) / np.abs(wo)))
+    assert worst <= 3e-6, worst
