@@ -374,6 +374,24 @@ static int upload_plans(liberi_handle h) {
     return LIBERI_OK;
 }
 
+// Device bytes that upload_plans allocates for one class plan.
+static size_t plan_device_bytes(const PlanHost &ph) {
+    if (ph.nbra == 0) return 0;
+    const size_t nb = ph.bra_ids.size(), nk = ph.ket_ids.size();
+    const size_t cap = ph.task_cap > 0 ? (size_t)ph.task_cap : 1;
+    return 4 * (nb + nk) * 2 + 8 * (nb + nk) + sizeof(int4) * (ph.items.size() + ph.tasks.size()) +
+           2 * sizeof(int4) * cap + 4 * sizeof(int);
+}
+
+// Device bytes that upload_basis allocates.
+static size_t basis_device_bytes(const BasisHost &b, const PairsHost &pr) {
+    const size_t npair = pr.shell.size(), nprim = pr.P.size();
+    const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
+    return sizeof(double4) * b.nsh + sizeof(int) * b.nsh + (sizeof(int2) + 2 * sizeof(int)) * npair +
+           (sizeof(double4) + sizeof(double2) + 2 * sizeof(float4)) * nprim + sizeof(double) * RYS_TABLE_SIZE +
+           sizeof(float) * RYSF_TABLE_SIZE + 2 * sizeof(double) * (ntri > 0 ? ntri : 1) + sizeof(unsigned long long);
+}
+
 static void compute_stats(liberi_handle h) {
     for (int k = 0; k < NKERN; k++) {
         const PlanHost &ph = h->plan[k];
@@ -475,6 +493,7 @@ static DevBasis dev_basis(liberi_handle h) {
 static int replan(liberi_handle h) {
     for (int k = 0; k < NKERN; k++) {
         PlanHost &ph = h->plan[k];
+        h->dev.bytes -= plan_device_bytes(ph);
         for (void *p : {(void *)ph.d_bra, (void *)ph.d_ket, (void *)ph.d_bra_orig, (void *)ph.d_ket_orig,
                         (void *)ph.d_bra_x, (void *)ph.d_ket_x, (void *)ph.d_items, (void *)ph.d_tasks,
                         (void *)ph.d_tasks64, (void *)ph.d_tasks32, (void *)ph.d_ntasks}) {
@@ -496,6 +515,7 @@ static int replan(liberi_handle h) {
     int rc = upload_plans(h);
     if (rc) return rc;
     compute_stats(h);
+    h->stats.device_bytes = (int64_t)h->dev.bytes;
     h->plan_dirty = false;
     return LIBERI_OK;
 }
@@ -763,6 +783,33 @@ int liberi_c_destroy(liberi_handle h) {
     if (!h) return fail(LIBERI_E_ARG, "liberi_destroy: null handle");
     liberi_c_cleanup(h);
     delete h;
+    return LIBERI_OK;
+}
+
+int liberi_c_setup_bytes(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot, const int32_t *ang_mom,
+                         const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
+                         const int32_t *atom_loc, const double *exponents, const double *contr_coef_s,
+                         const double *contr_coef_p, const double *contr_coef_d, const double *coords,
+                         const double *schwrz_int, double schwarz_cut, int64_t *bytes) {
+    if (!bytes) return fail(LIBERI_E_ARG, "liberi_setup_bytes: null result pointer");
+    BasisHost b;
+    int rc = copy_basis(b, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num, atom_loc, nullptr,
+                        nullptr, exponents, contr_coef_s, contr_coef_p, contr_coef_d, nullptr, coords, schwrz_int);
+    if (rc) return rc;
+    rc = validate_basis(b);
+    if (rc) return rc;
+    PairsHost pr;
+    std::vector<double4> shell_xyz;
+    build_pairs(b, pr, shell_xyz);
+    size_t total = basis_device_bytes(b, pr);
+    for (int k = 0; k < NKERN; k++) {
+        const bool run = (k == 0 && pr.nl[0] > 0) || (k >= 1 && k <= 5 && pr.nl[1] > 0) || (k >= 6 && pr.nl[2] > 0);
+        if (!run) continue;
+        PlanHost ph;
+        build_plan(pr, k, schwarz_cut, 0, ph);
+        total += plan_device_bytes(ph);
+    }
+    *bytes = (int64_t)total;
     return LIBERI_OK;
 }
 

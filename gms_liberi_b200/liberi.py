@@ -34,7 +34,7 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_schwarz_noalloc", "liberi_c_batch_create", "liberi_c_batch_bind",
            "liberi_c_batch_fock_build", "liberi_c_batch_capture", "liberi_c_batch_launch",
            "liberi_c_batch_synchronize", "liberi_c_batch_autotune", "liberi_c_batch_destroy",
-           "liberi_c_autotune", "liberi_c_rys_eval_f32"]
+           "liberi_c_autotune", "liberi_c_rys_eval_f32", "liberi_c_setup_bytes"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -87,6 +87,10 @@ def lib():
                                        _I32P, _I32P, _I32P, _I32P, _I32P,
                                        _F64P, _F64P, _F64P, _F64P, _F64P, _F64P]
         L.liberi_c_get_stats.argtypes = [H, ctypes.POINTER(Stats)]
+        L.liberi_c_setup_bytes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                           _I32P, _I32P, _I32P, _I32P, _I32P,
+                                           _F64P, _F64P, _F64P, _F64P, _F64P, _F64P, ctypes.c_double,
+                                           ctypes.POINTER(ctypes.c_int64)]
         L.liberi_c_schwarz_noalloc.argtypes = L.liberi_c_schwarz.argtypes
         L.liberi_c_rys_eval.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                         _F64P, _F64P]
@@ -336,6 +340,18 @@ def rys_eval_f32(n, T, thr=60.0, strict=False):
     FP = ctypes.POINTER(ctypes.c_float)
     _check(lib().liberi_c_rys_eval_f32(n, T, thr, int(strict), u.ctypes.data_as(FP), w.ctypes.data_as(FP)))
     return u.astype(np.float64), w.astype(np.float64)
+
+
+def setup_bytes(basis, schwarz_cut=5.00000000000000018e-11):
+    """Device bytes liberi_setup would allocate for `basis` (host-only dry run)."""
+    (nsh, natoms, nbf, mx, ang, cn, sl, an, al, sb, eb, ex, cs, cp, cd, cf, xyz) = _basis_args(basis)
+    k = []
+    out = ctypes.c_int64()
+    _check(lib().liberi_c_setup_bytes(nsh, natoms, nbf, mx, _i32(ang, k), _i32(cn, k), _i32(sl, k), _i32(an, k),
+                                      _i32(al, k), _f64(ex, k), _f64(cs, k), _f64(cp, k), _f64(cd, k),
+                                      _f64(xyz, k), _f64(basis["schwrz"], k), float(schwarz_cut),
+                                      ctypes.byref(out)))
+    return int(out.value)
 
 
 def schwarz(basis):

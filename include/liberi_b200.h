@@ -152,6 +152,16 @@ typedef struct {
 } liberi_stats;
 int liberi_c_get_stats(liberi_handle handle, liberi_stats *stats);
 
+/* Device bytes liberi_c_setup would allocate for this basis at this Schwarz
+ * cut (host-only dry run of the pair and plan construction, no device
+ * access): the admission figure of a serving loop.  No counterpart in the
+ * reference. */
+int liberi_c_setup_bytes(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot, const int32_t *ang_mom,
+                         const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
+                         const int32_t *atom_loc, const double *exponents, const double *contr_coef_s,
+                         const double *contr_coef_p, const double *contr_coef_d, const double *coords,
+                         const double *schwrz_int, double schwarz_cut, int64_t *bytes);
+
 /* Batched Fock builds over several set-up handles (one molecule each): one
  * launch per quartet class covers every molecule (a persistent multi-molecule
  * work list), preceded by one launch that zeroes every F.  No counterpart in
