@@ -198,7 +198,7 @@ def traffic_per_launch(kernel):
 
 def run_ours(args):
     import torch
-    from gms_liberi_b200 import flops, liberi
+    from gms_liberi_b200 import flops, liberi, ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -227,10 +227,12 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     launched = int(sum(1 for k in range(21) if st0["quartets"][k] > 0))
 
-    def step():
+    def partial(r, n):
         liberi.fock_build_device(h, D.data_ptr(), F.data_ptr(), stream.cuda_stream)
-        if world > 1:
-            dist.all_reduce(F)
+        return F
+
+    def step():
+        ranks.reduced_fock(partial)  # one NCCL all-reduce of the packed F when N > 1
 
     def barrier():
         if world > 1:
@@ -253,11 +255,7 @@ def run_ours(args):
         return float(np.mean(ms)), cls / max(1, nsteps)
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ranks.max_over_ranks(x, device=dev)
 
     assert stream.cuda_stream != 0
     uuid = None
