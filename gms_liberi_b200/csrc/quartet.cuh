@@ -18,7 +18,8 @@
 //      int0000.F90:241-311 / int2222_rysgen.F90:11176-11338), pre-reduced in
 //      registers per quartet:
 //        K updates into rows A and B of F -> shared-memory tile of the CTA
-//        J update of the row pair (A,B)   -> warp-reduced, then the tile
+//        J update of the row pair (A,B)   -> summed over the warp (shuffles),
+//                                            one tile update per warp
 //        J update of the ket pair (C,D)   -> FP64 global atomics
 //      and the tile is flushed to F with FP64 atomics when the CTA ends.
 // The FP32 instantiation evaluates step 1 entirely in single precision (pair
@@ -527,6 +528,121 @@ struct KBuf {
     __device__ __forceinline__ double &cd(int ic, int id) { return at(NB * NC + NB * ND + ic * ND + id); }
 };
 
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Digestion of one A component (row mu) of a quartet whose four shells give
+// distinct function pairs (no identical shells in the bra or the ket, bra !=
+// ket): every Cartesian component is unique and no 0.5 factor applies
+// (int0000.F90:255-292 reduce to the plain six updates), so the D sub-blocks
+// are loaded once per pass and each integral costs one cut select and six
+// FMAs.  jab returns 4 sum D(la,si) (mu nu|la si) for the warp-level J
+// reduction of the row pair.
+template <int LA, int LB, int LC, int LD, typename R, typename KB>
+__device__ __forceinline__ void digest_row_distinct(const R (&a)[ncart(LB)][ncart(LC)][ncart(LD)], int ia,
+                                                    const QuartetCtx &qc,
+                                                    const double (&dCD)[ncart(LC)][ncart(LD)],
+                                                    const double (&dBD)[ncart(LB)][ncart(LD)],
+                                                    const double (&dBC)[ncart(LB)][ncart(LC)], const Rows &rows,
+                                                    KB &kb, double (&jab)[ncart(LB)]) {
+    constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    const double *__restrict__ Dm = qc.Dm;
+    const int mu = qc.bfA + ia;
+    const double sa = s3pow(cs3_rt(LA, ia));
+    double dAB[NB], dAC[NC], dAD[ND];
+#pragma unroll
+    for (int ib = 0; ib < NB; ib++) dAB[ib] = 4.0 * dget(Dm, mu, qc.bfB + ib);
+#pragma unroll
+    for (int ic = 0; ic < NC; ic++) dAC[ic] = dget(Dm, mu, qc.bfC + ic);
+#pragma unroll
+    for (int id = 0; id < ND; id++) dAD[id] = dget(Dm, mu, qc.bfD + id);
+    double kac[NC], kad[ND];
+#pragma unroll
+    for (int ib = 0; ib < NB; ib++) jab[ib] = 0.0;
+#pragma unroll
+    for (int ic = 0; ic < NC; ic++) kac[ic] = 0.0;
+#pragma unroll
+    for (int id = 0; id < ND; id++) kad[id] = 0.0;
+#pragma unroll
+    for (int ib = 0; ib < NB; ib++)
+#pragma unroll
+        for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+            for (int id = 0; id < ND; id++) {
+                double v = (double)a[ib][ic][id] * (sa * s3pow(cs3(LB, ib) + cs3(LC, ic) + cs3(LD, id)));
+                v = fabs(v) < qc.cut ? 0.0 : v;
+                jab[ib] = fma(v, dCD[ic][id], jab[ib]);
+                kb.cd(ic, id) = fma(v, dAB[ib], kb.cd(ic, id));
+                kac[ic] = fma(v, dBD[ib][id], kac[ic]);
+                kad[id] = fma(v, dBC[ib][ic], kad[id]);
+                kb.bc(ib, ic) = fma(v, dAD[id], kb.bc(ib, ic));
+                kb.bd(ib, id) = fma(v, dAC[ic], kb.bd(ib, id));
+            }
+#pragma unroll
+    for (int ib = 0; ib < NB; ib++) jab[ib] *= 4.0;
+#pragma unroll
+    for (int ic = 0; ic < NC; ic++) rows.add(ia, mu, qc.bfC + ic, -kac[ic]);
+#pragma unroll
+    for (int id = 0; id < ND; id++) rows.add(ia, mu, qc.bfD + id, -kad[id]);
+}
+
+// Digestion of one A component with the reference's unique-component loops
+// and 0.5 factors (identical shells in the bra or the ket, or bra == ket).
+template <int LA, int LB, int LC, int LD, typename R, typename KB>
+__device__ __forceinline__ void digest_row_general(const R (&a)[ncart(LB)][ncart(LC)][ncart(LD)], int ia,
+                                                   const QuartetCtx &qc, const Rows &rows, KB &kb,
+                                                   double (&jab)[ncart(LB)]) {
+    constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    constexpr bool can_same = (LA == LC) && (LB == LD);
+    const int mu = qc.bfA + ia;
+    const int n3a = cs3_rt(LA, ia);
+    double kac[NC], kad[ND];
+#pragma unroll
+    for (int ic = 0; ic < NC; ic++) kac[ic] = 0.0;
+#pragma unroll
+    for (int id = 0; id < ND; id++) kad[id] = 0.0;
+#pragma unroll
+    for (int ib = 0; ib < NB; ib++) {
+        jab[ib] = 0.0;
+        if (LA == LB && qc.iandj && ib > ia) continue;
+        const int nu = qc.bfB + ib;
+        const double dmn = dget(qc.Dm, mu, nu);
+#pragma unroll
+        for (int ic = 0; ic < NC; ic++) {
+            const int la = qc.bfC + ic;
+#pragma unroll
+            for (int id = 0; id < ND; id++) {
+                if (LC == LD && qc.kandl && id > ic) continue;
+                if (can_same && qc.same) {
+                    const int oij = qc.iandj ? ia * (ia + 1) / 2 + ib : ia * NB + ib;
+                    const int okl = qc.kandl ? ic * (ic + 1) / 2 + id : ic * ND + id;
+                    if (okl > oij) continue;
+                }
+                double v = (double)a[ib][ic][id] * s3pow(n3a + cs3(LB, ib) + cs3(LC, ic) + cs3(LD, id));
+                if (fabs(v) < qc.cut) continue;
+                const int si = qc.bfD + id;
+                // 0.5 factors for coinciding function indices (int0000.F90:288-292)
+                if (mu == nu) v *= 0.5;
+                if (la == si) v *= 0.5;
+                if ((mu == la && nu == si) || (mu == si && nu == la)) v *= 0.5;
+                jab[ib] += 4.0 * v * dget(qc.Dm, la, si);
+                kb.cd(ic, id) += 4.0 * v * dmn;
+                kac[ic] += v * dget(qc.Dm, nu, si);
+                kad[id] += v * dget(qc.Dm, nu, la);
+                kb.bc(ib, ic) += v * dget(qc.Dm, mu, si);
+                kb.bd(ib, id) += v * dget(qc.Dm, mu, la);
+            }
+        }
+    }
+#pragma unroll
+    for (int ic = 0; ic < NC; ic++) rows.add(ia, mu, qc.bfC + ic, -kac[ic]);
+#pragma unroll
+    for (int id = 0; id < ND; id++) rows.add(ia, mu, qc.bfD + id, -kad[id]);
+}
+
 // Runtime loop over passes of NMU A components; digestion of each pass.
 template <int LA, int LB, int LC, int LD, typename R, typename KB>
 __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, int q0, int nq, const double4 &A,
@@ -537,63 +653,46 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     using PS = PassShape<LA, LB, LC, LD, R>;
     constexpr int M = PS::NMU;
-    constexpr bool can_same = (LA == LC) && (LB == LD);
 #pragma unroll 1
     for (int pass = 0; pass < PS::NPASS; pass++) {
         const int mu0 = pass * M;
         R acc[M][NB][NC][ND];
         eval_block<LA, LB, LC, LD, R, M>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict, tab, tabf,
                                          mu0, acc);
+        // The J update of the row pair (mu nu) is the same address for every
+        // lane of the warp (one bra per CTA): it is summed over the warp and
+        // added once.  Every lane reaches the reduction (the quartet loop is
+        // warp-uniform; idle lanes carry zero integrals).
+        const bool distinct = !qc.iandj && !qc.kandl && !qc.same;
+        double dCD[NC][ND], dBD[NB][ND], dBC[NB][NC];
+        if (distinct) {
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                for (int id = 0; id < ND; id++) dCD[ic][id] = dget(qc.Dm, qc.bfC + ic, qc.bfD + id);
+#pragma unroll
+            for (int ib = 0; ib < NB; ib++) {
+#pragma unroll
+                for (int id = 0; id < ND; id++) dBD[ib][id] = dget(qc.Dm, qc.bfB + ib, qc.bfD + id);
+#pragma unroll
+                for (int ic = 0; ic < NC; ic++) dBC[ib][ic] = dget(qc.Dm, qc.bfB + ib, qc.bfC + ic);
+            }
+        }
 #pragma unroll
         for (int m = 0; m < M; m++) {
             const int ia = mu0 + m;
             if (ia >= NA) break;
-            const int mu = qc.bfA + ia;
-            const int n3a = cs3_rt(LA, ia);
-            double kac[NC], kad[ND], jab[NB];
+            double jab[NB];
+            if (distinct)
+                digest_row_distinct<LA, LB, LC, LD, R>(acc[m], ia, qc, dCD, dBD, dBC, rows, kb, jab);
+            else
+                digest_row_general<LA, LB, LC, LD, R>(acc[m], ia, qc, rows, kb, jab);
 #pragma unroll
-            for (int ic = 0; ic < NC; ic++) kac[ic] = 0.0;
+            for (int ib = 0; ib < NB; ib++) jab[ib] = warp_sum(jab[ib]);
+            if ((threadIdx.x & 31) == 0) {
 #pragma unroll
-            for (int id = 0; id < ND; id++) kad[id] = 0.0;
-#pragma unroll
-            for (int ib = 0; ib < NB; ib++) {
-                jab[ib] = 0.0;
-                if (LA == LB && qc.iandj && ib > ia) continue;
-                const int nu = qc.bfB + ib;
-                const double dmn = dget(qc.Dm, mu, nu);
-#pragma unroll
-                for (int ic = 0; ic < NC; ic++) {
-                    const int la = qc.bfC + ic;
-#pragma unroll
-                    for (int id = 0; id < ND; id++) {
-                        if (LC == LD && qc.kandl && id > ic) continue;
-                        if (can_same && qc.same) {
-                            const int oij = qc.iandj ? ia * (ia + 1) / 2 + ib : ia * NB + ib;
-                            const int okl = qc.kandl ? ic * (ic + 1) / 2 + id : ic * ND + id;
-                            if (okl > oij) continue;
-                        }
-                        double v = (double)acc[m][ib][ic][id] * s3pow(n3a + cs3(LB, ib) + cs3(LC, ic) + cs3(LD, id));
-                        if (fabs(v) < qc.cut) continue;
-                        const int si = qc.bfD + id;
-                        // 0.5 factors for coinciding function indices (int0000.F90:288-292)
-                        if (mu == nu) v *= 0.5;
-                        if (la == si) v *= 0.5;
-                        if ((mu == la && nu == si) || (mu == si && nu == la)) v *= 0.5;
-                        jab[ib] += 4.0 * v * dget(qc.Dm, la, si);
-                        kb.cd(ic, id) += 4.0 * v * dmn;
-                        kac[ic] += v * dget(qc.Dm, nu, si);
-                        kad[id] += v * dget(qc.Dm, nu, la);
-                        kb.bc(ib, ic) += v * dget(qc.Dm, mu, si);
-                        kb.bd(ib, id) += v * dget(qc.Dm, mu, la);
-                    }
-                }
+                for (int ib = 0; ib < NB; ib++) rows.add(ia, qc.bfA + ia, qc.bfB + ib, jab[ib]);
             }
-#pragma unroll
-            for (int ic = 0; ic < NC; ic++) rows.add(ia, mu, qc.bfC + ic, -kac[ic]);
-#pragma unroll
-            for (int id = 0; id < ND; id++) rows.add(ia, mu, qc.bfD + id, -kad[id]);
-#pragma unroll
-            for (int ib = 0; ib < NB; ib++) rows.add(ia, mu, qc.bfB + ib, jab[ib]);
         }
     }
 }
@@ -695,16 +794,22 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     Rows rowsB{use_tile ? tile + NA * LIBERI_NBF : nullptr, LIBERI_F, LIBERI_NBF};
     const R abx = R(A.x - B.x), aby = R(A.y - B.y), abz = R(A.z - B.z);
     const int p0 = bas.pair_prim0[P], np = bas.pair_nprim[P];
-    for (int qi = threadIdx.x; qi < cnt; qi += CLASS_THREADS) {
-        const int j = k0 + qi;
-        if (a.rs.nsize > 1) {
+    // Warp-uniform loop: every lane of a warp runs the same iterations (the
+    // digestion sums the row pair's J over the warp); a lane past the end of
+    // the task, or holding a quartet of another rank, evaluates no primitives
+    // and digests zeros.
+    for (int qb = threadIdx.x & ~31; qb < cnt; qb += CLASS_THREADS) {
+        const int qi = qb + (threadIdx.x & 31);
+        bool act = qi < cnt;
+        const int j = k0 + (act ? qi : 0);
+        if (act && a.rs.nsize > 1) {
             long long bo = a.bra_orig[ibra], ko = a.ket_orig[j];
             if (a.swapped) { long long tmp = bo; bo = ko; ko = tmp; }
             long long it;
             if (a.rs.tri) it = (bo > ko ? bo : ko) + 1;
             else if (a.rs.ketmajor) it = ko * a.rs.nbra_ref + bo + 1;
             else it = bo * a.rs.nket_ref + ko + 1;
-            if (!rank_owns(a.rs, it)) continue;
+            act = rank_owns(a.rs, it);
         }
         const int Qd = __ldg(mol_ket<BATCH>(a, t.w) + j);
         const int2 scd = bas.pair_shell[Qd];
@@ -720,8 +825,8 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
         kb.s = slots + threadIdx.x;
 #pragma unroll
         for (int i = 0; i < KBuf<NB, NC, ND, SM>::N; i++) kb.at(i) = 0.0;
-        run_passes<LA, LB, LC, LD, R>(bas, p0, np, bas.pair_prim0[Qd], bas.pair_nprim[Qd], A, C, abx, aby, abz,
-                                      cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb);
+        run_passes<LA, LB, LC, LD, R>(bas, p0, np, bas.pair_prim0[Qd], act ? bas.pair_nprim[Qd] : 0, A, C, abx, aby,
+                                      abz, cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
 #pragma unroll
