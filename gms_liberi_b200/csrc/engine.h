@@ -162,6 +162,7 @@ struct DeviceBuffers {
     double2 *prim_X = nullptr;
     float4 *prim_Pf = nullptr, *prim_Af = nullptr;
     double *D = nullptr, *F = nullptr;
+    float *Df = nullptr;  // FP32 tier: single-precision copy of the build's D
     long long *scratch_total = nullptr;  // device counters (mixed split)
     size_t bytes = 0;
 };
@@ -176,6 +177,7 @@ struct LaunchCtx {
     const double *rys_tab;
     const float *rys_tabf;
     const double *D;
+    const float *Df;
     double *F;
     double schwarz_cut, eri_cut;
     cudaStream_t stream;
@@ -188,6 +190,7 @@ cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const
 cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, int ntasks, int nbf_max,
                                const MolView *d_mols, const ClassView *d_cviews, bool swapped);
 cudaError_t launch_zero_fock(const MolView *d_mols, int nmol, long long max_ntri, cudaStream_t stream);
+cudaError_t launch_to_float(const double *src, float *dst, long long n, cudaStream_t st);
 cudaError_t launch_maxabs(const double *x, long long n, unsigned long long *out,
                           cudaStream_t stream);
 cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_x, const double *ket_x,

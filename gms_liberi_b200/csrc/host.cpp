@@ -389,7 +389,8 @@ static size_t basis_device_bytes(const BasisHost &b, const PairsHost &pr) {
     const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
     return sizeof(double4) * b.nsh + sizeof(int) * b.nsh + (sizeof(int2) + 2 * sizeof(int)) * npair +
            (sizeof(double4) + sizeof(double2) + 2 * sizeof(float4)) * nprim + sizeof(double) * RYS_TABLE_SIZE +
-           sizeof(float) * RYSF_TABLE_SIZE + 2 * sizeof(double) * (ntri > 0 ? ntri : 1) + sizeof(unsigned long long);
+           sizeof(float) * RYSF_TABLE_SIZE + (2 * sizeof(double) + sizeof(float)) * (ntri > 0 ? ntri : 1) +
+           sizeof(unsigned long long);
 }
 
 static void compute_stats(liberi_handle h) {
@@ -471,6 +472,7 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
     const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
     CUDA_TRY(dev_alloc(h, &h->dev.D, ntri));
     CUDA_TRY(dev_alloc(h, &h->dev.F, ntri));
+    CUDA_TRY(dev_alloc(h, &h->dev.Df, ntri));
     CUDA_TRY(dev_alloc(h, &h->d_maxd, 1));
     return LIBERI_OK;
 }
@@ -539,7 +541,11 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     ctx.stream = st;
     ctx.num_sms = h->num_sms;
     const bool mixed = h->precision == 1;
-    if (mixed) CUDA_TRY(launch_maxabs(dD, ntri, h->d_maxd, st));
+    ctx.Df = h->dev.Df;
+    if (mixed) {
+        CUDA_TRY(launch_maxabs(dD, ntri, h->d_maxd, st));
+        CUDA_TRY(launch_to_float(dD, h->dev.Df, ntri, st));
+    }
     for (int k = 0; k < NKERN; k++) h->ev_recorded[k] = false;
     for (int k = 0; k < NKERN; k++) {
         PlanHost &ph = h->plan[k];
@@ -672,6 +678,7 @@ static int batch_enqueue(liberi_batch b, cudaStream_t st, uint32_t mask) {
     ctx.basis = DevBasis{};
     ctx.rys_tab = h0->d_tab;
     ctx.rys_tabf = h0->d_tabf;
+    ctx.Df = nullptr;
     ctx.D = nullptr;
     ctx.F = nullptr;
     ctx.schwarz_cut = h0->schwarz_cut;

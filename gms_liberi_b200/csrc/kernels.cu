@@ -108,6 +108,7 @@ cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const
     a.tab = ctx.rys_tab;
     a.tabf = ctx.rys_tabf;
     a.Dm = ctx.D;
+    a.Dmf = ctx.Df;
     a.F = ctx.F;
     a.cut = kd.digest_schwarz ? ctx.schwarz_cut : ctx.eri_cut;
     a.thr = kd.asym;
@@ -140,6 +141,7 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     a.tab = ctx.rys_tab;
     a.tabf = ctx.rys_tabf;
     a.Dm = nullptr;
+    a.Dmf = nullptr;
     a.F = nullptr;
     a.cut = kd.digest_schwarz ? ctx.schwarz_cut : ctx.eri_cut;
     a.thr = kd.asym;
@@ -160,6 +162,20 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
 #undef LIBERI_CASE
     return cudaErrorInvalidValue;
+}
+
+__global__ void to_float_kernel(const double *__restrict__ src, float *__restrict__ dst, long long n) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = (float)src[i];
+}
+
+cudaError_t launch_to_float(const double *src, float *dst, long long n, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int threads = 256;
+    const long long want = (n + threads - 1) / threads;
+    const int blocks = (int)(want < 148LL * 8 ? want : 148LL * 8);
+    to_float_kernel<<<blocks, threads, 0, st>>>(src, dst, n);
+    return cudaGetLastError();
 }
 
 __global__ void zero_fock_kernel(const MolView *mols, int nmol, long long max_ntri) {

@@ -389,25 +389,30 @@ __device__ __forceinline__ int tri0(int i, int j) {
 
 // target of a K or J update: the CTA's shared tile (rows of A and B of F) or,
 // when the tile does not fit, the packed matrix itself
+// (T: the digestion type, double for the FP64 tier and float for the FP32
+// tier, whose tile is single precision; F itself is always FP64.)
+template <typename T>
 struct Rows {
-    double *tile;  // rows x nbf, or null
+    T *tile;  // rows x nbf, or null
     double *F;
     int nbf;
-    __device__ __forceinline__ void add(int r, int bf_row, int col, double v) const {
-        if (v == 0.0) return;
+    __device__ __forceinline__ void add(int r, int bf_row, int col, T v) const {
+        if (v == T(0)) return;
         if (tile) atomicAdd(tile + r * nbf + col, v);
-        else atomicAdd(F + tri0(bf_row, col), v);
+        else atomicAdd(F + tri0(bf_row, col), (double)v);
     }
 };
 
+template <typename T>
 struct QuartetCtx {
     int bfA, bfB, bfC, bfD;
     bool iandj, kandl, same;
-    double cut;
-    const double *__restrict__ Dm;
+    T cut;
+    const T *__restrict__ Dm;
 };
 
-__device__ __forceinline__ double dget(const double *__restrict__ Dm, int i, int j) {
+template <typename T>
+__device__ __forceinline__ T dget(const T *__restrict__ Dm, int i, int j) {
     return __ldg(Dm + tri0(i, j));
 }
 
@@ -514,21 +519,22 @@ constexpr int CLASS_THREADS = 128;
 // (bc[ib][ic], bd[ib][id]) and the ket-pair J block (cd[ic][id]).  Single-
 // pass classes keep them in registers; multi-pass classes in per-thread
 // shared-memory slots (stride CLASS_THREADS, bank-conflict free).
-template <int NB, int NC, int ND, bool SM>
+template <int NB, int NC, int ND, bool SM, typename T>
 struct KBuf {
     static constexpr int N = NB * NC + NB * ND + NC * ND;
-    double r[SM ? 1 : N];
-    double *s;
-    __device__ __forceinline__ double &at(int i) {
+    T r[SM ? 1 : N];
+    T *s;
+    __device__ __forceinline__ T &at(int i) {
         if constexpr (SM) return s[i * CLASS_THREADS];
         else return r[i];
     }
-    __device__ __forceinline__ double &bc(int ib, int ic) { return at(ib * NC + ic); }
-    __device__ __forceinline__ double &bd(int ib, int id) { return at(NB * NC + ib * ND + id); }
-    __device__ __forceinline__ double &cd(int ic, int id) { return at(NB * NC + NB * ND + ic * ND + id); }
+    __device__ __forceinline__ T &bc(int ib, int ic) { return at(ib * NC + ic); }
+    __device__ __forceinline__ T &bd(int ib, int id) { return at(NB * NC + ib * ND + id); }
+    __device__ __forceinline__ T &cd(int ic, int id) { return at(NB * NC + NB * ND + ic * ND + id); }
 };
 
-__device__ __forceinline__ double warp_sum(double v) {
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
@@ -543,37 +549,37 @@ __device__ __forceinline__ double warp_sum(double v) {
 // reduction of the row pair.
 template <int LA, int LB, int LC, int LD, typename R, typename KB>
 __device__ __forceinline__ void digest_row_distinct(const R (&a)[ncart(LB)][ncart(LC)][ncart(LD)], int ia,
-                                                    const QuartetCtx &qc,
-                                                    const double (&dCD)[ncart(LC)][ncart(LD)],
-                                                    const double (&dBD)[ncart(LB)][ncart(LD)],
-                                                    const double (&dBC)[ncart(LB)][ncart(LC)], const Rows &rows,
-                                                    KB &kb, double (&jab)[ncart(LB)]) {
+                                                    const QuartetCtx<R> &qc,
+                                                    const R (&dCD)[ncart(LC)][ncart(LD)],
+                                                    const R (&dBD)[ncart(LB)][ncart(LD)],
+                                                    const R (&dBC)[ncart(LB)][ncart(LC)], const Rows<R> &rows,
+                                                    KB &kb, R (&jab)[ncart(LB)]) {
     constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    const double *__restrict__ Dm = qc.Dm;
+    const R *__restrict__ Dm = qc.Dm;
     const int mu = qc.bfA + ia;
-    const double sa = s3pow(cs3_rt(LA, ia));
-    double dAB[NB], dAC[NC], dAD[ND];
+    const R sa = R(s3pow(cs3_rt(LA, ia)));
+    R dAB[NB], dAC[NC], dAD[ND];
 #pragma unroll
-    for (int ib = 0; ib < NB; ib++) dAB[ib] = 4.0 * dget(Dm, mu, qc.bfB + ib);
+    for (int ib = 0; ib < NB; ib++) dAB[ib] = R(4) * dget(Dm, mu, qc.bfB + ib);
 #pragma unroll
     for (int ic = 0; ic < NC; ic++) dAC[ic] = dget(Dm, mu, qc.bfC + ic);
 #pragma unroll
     for (int id = 0; id < ND; id++) dAD[id] = dget(Dm, mu, qc.bfD + id);
-    double kac[NC], kad[ND];
+    R kac[NC], kad[ND];
 #pragma unroll
-    for (int ib = 0; ib < NB; ib++) jab[ib] = 0.0;
+    for (int ib = 0; ib < NB; ib++) jab[ib] = R(0);
 #pragma unroll
-    for (int ic = 0; ic < NC; ic++) kac[ic] = 0.0;
+    for (int ic = 0; ic < NC; ic++) kac[ic] = R(0);
 #pragma unroll
-    for (int id = 0; id < ND; id++) kad[id] = 0.0;
+    for (int id = 0; id < ND; id++) kad[id] = R(0);
 #pragma unroll
     for (int ib = 0; ib < NB; ib++)
 #pragma unroll
         for (int ic = 0; ic < NC; ic++)
 #pragma unroll
             for (int id = 0; id < ND; id++) {
-                double v = (double)a[ib][ic][id] * (sa * s3pow(cs3(LB, ib) + cs3(LC, ic) + cs3(LD, id)));
-                v = fabs(v) < qc.cut ? 0.0 : v;
+                R v = a[ib][ic][id] * (sa * R(s3pow(cs3(LB, ib) + cs3(LC, ic) + cs3(LD, id))));
+                v = fabs(v) < qc.cut ? R(0) : v;
                 jab[ib] = fma(v, dCD[ic][id], jab[ib]);
                 kb.cd(ic, id) = fma(v, dAB[ib], kb.cd(ic, id));
                 kac[ic] = fma(v, dBD[ib][id], kac[ic]);
@@ -582,7 +588,7 @@ __device__ __forceinline__ void digest_row_distinct(const R (&a)[ncart(LB)][ncar
                 kb.bd(ib, id) = fma(v, dAC[ic], kb.bd(ib, id));
             }
 #pragma unroll
-    for (int ib = 0; ib < NB; ib++) jab[ib] *= 4.0;
+    for (int ib = 0; ib < NB; ib++) jab[ib] *= R(4);
 #pragma unroll
     for (int ic = 0; ic < NC; ic++) rows.add(ia, mu, qc.bfC + ic, -kac[ic]);
 #pragma unroll
@@ -593,23 +599,23 @@ __device__ __forceinline__ void digest_row_distinct(const R (&a)[ncart(LB)][ncar
 // and 0.5 factors (identical shells in the bra or the ket, or bra == ket).
 template <int LA, int LB, int LC, int LD, typename R, typename KB>
 __device__ __forceinline__ void digest_row_general(const R (&a)[ncart(LB)][ncart(LC)][ncart(LD)], int ia,
-                                                   const QuartetCtx &qc, const Rows &rows, KB &kb,
-                                                   double (&jab)[ncart(LB)]) {
+                                                   const QuartetCtx<R> &qc, const Rows<R> &rows, KB &kb,
+                                                   R (&jab)[ncart(LB)]) {
     constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr bool can_same = (LA == LC) && (LB == LD);
     const int mu = qc.bfA + ia;
     const int n3a = cs3_rt(LA, ia);
-    double kac[NC], kad[ND];
+    R kac[NC], kad[ND];
 #pragma unroll
-    for (int ic = 0; ic < NC; ic++) kac[ic] = 0.0;
+    for (int ic = 0; ic < NC; ic++) kac[ic] = R(0);
 #pragma unroll
-    for (int id = 0; id < ND; id++) kad[id] = 0.0;
+    for (int id = 0; id < ND; id++) kad[id] = R(0);
 #pragma unroll
     for (int ib = 0; ib < NB; ib++) {
-        jab[ib] = 0.0;
+        jab[ib] = R(0);
         if (LA == LB && qc.iandj && ib > ia) continue;
         const int nu = qc.bfB + ib;
-        const double dmn = dget(qc.Dm, mu, nu);
+        const R dmn = dget(qc.Dm, mu, nu);
 #pragma unroll
         for (int ic = 0; ic < NC; ic++) {
             const int la = qc.bfC + ic;
@@ -621,15 +627,15 @@ __device__ __forceinline__ void digest_row_general(const R (&a)[ncart(LB)][ncart
                     const int okl = qc.kandl ? ic * (ic + 1) / 2 + id : ic * ND + id;
                     if (okl > oij) continue;
                 }
-                double v = (double)a[ib][ic][id] * s3pow(n3a + cs3(LB, ib) + cs3(LC, ic) + cs3(LD, id));
+                R v = a[ib][ic][id] * R(s3pow(n3a + cs3(LB, ib) + cs3(LC, ic) + cs3(LD, id)));
                 if (fabs(v) < qc.cut) continue;
                 const int si = qc.bfD + id;
                 // 0.5 factors for coinciding function indices (int0000.F90:288-292)
-                if (mu == nu) v *= 0.5;
-                if (la == si) v *= 0.5;
-                if ((mu == la && nu == si) || (mu == si && nu == la)) v *= 0.5;
-                jab[ib] += 4.0 * v * dget(qc.Dm, la, si);
-                kb.cd(ic, id) += 4.0 * v * dmn;
+                if (mu == nu) v *= R(0.5);
+                if (la == si) v *= R(0.5);
+                if ((mu == la && nu == si) || (mu == si && nu == la)) v *= R(0.5);
+                jab[ib] += R(4) * v * dget(qc.Dm, la, si);
+                kb.cd(ic, id) += R(4) * v * dmn;
                 kac[ic] += v * dget(qc.Dm, nu, si);
                 kad[id] += v * dget(qc.Dm, nu, la);
                 kb.bc(ib, ic) += v * dget(qc.Dm, mu, si);
@@ -648,8 +654,8 @@ template <int LA, int LB, int LC, int LD, typename R, typename KB>
 __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, int q0, int nq, const double4 &A,
                                            const double4 &C, R abx, R aby, R abz, R cdx, R cdy, R cdz,
                                            double thr, bool strict, const double *__restrict__ tab,
-                                           const float *__restrict__ tabf, const QuartetCtx &qc,
-                                           const Rows &rows, KB &kb) {
+                                           const float *__restrict__ tabf, const QuartetCtx<R> &qc,
+                                           const Rows<R> &rows, KB &kb) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     using PS = PassShape<LA, LB, LC, LD, R>;
     constexpr int M = PS::NMU;
@@ -664,7 +670,7 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
         // added once.  Every lane reaches the reduction (the quartet loop is
         // warp-uniform; idle lanes carry zero integrals).
         const bool distinct = !qc.iandj && !qc.kandl && !qc.same;
-        double dCD[NC][ND], dBD[NB][ND], dBC[NB][NC];
+        R dCD[NC][ND], dBD[NB][ND], dBC[NB][NC];
         if (distinct) {
 #pragma unroll
             for (int ic = 0; ic < NC; ic++)
@@ -682,7 +688,7 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
         for (int m = 0; m < M; m++) {
             const int ia = mu0 + m;
             if (ia >= NA) break;
-            double jab[NB];
+            R jab[NB];
             if (distinct)
                 digest_row_distinct<LA, LB, LC, LD, R>(acc[m], ia, qc, dCD, dBD, dBC, rows, kb, jab);
             else
@@ -724,6 +730,7 @@ struct ClassArgs {
     const double *tab;
     const float *tabf;
     const double *Dm;
+    const float *Dmf;        // FP32 tier: single-precision copy of D (this build's)
     double *F;
     double cut;
     double thr;
@@ -740,7 +747,6 @@ struct ClassArgs {
     const ClassView *cviews; // batched launch: per-molecule lists of this class
 };
 
-// One CTA task: row pair t.x against kets t.y .. t.y+t.z-1 of one molecule.
 // Per-molecule data of a task.  A single-molecule launch reads the kernel
 // parameters at every use (constant-bank operands, no registers held across
 // the quartet loop); a batched launch reads the task's molecule view (task.w).
@@ -748,9 +754,11 @@ template <bool BATCH>
 __device__ __forceinline__ const DevBasis &mol_basis(const ClassArgs &a, int w) {
     if constexpr (BATCH) return a.mols[w].b; else return a.b;
 }
-template <bool BATCH>
-__device__ __forceinline__ const double *mol_D(const ClassArgs &a, int w) {
-    if constexpr (BATCH) return a.mols[w].D; else return a.Dm;
+template <bool BATCH, typename T>
+__device__ __forceinline__ const T *mol_D(const ClassArgs &a, int w) {
+    if constexpr (std::is_same<T, float>::value) return a.Dmf;  // FP32 tier (single-molecule launches)
+    else if constexpr (BATCH) return a.mols[w].D;
+    else return a.Dm;
 }
 template <bool BATCH>
 __device__ __forceinline__ double *mol_F(const ClassArgs &a, int w) {
@@ -773,10 +781,11 @@ __device__ __forceinline__ const int *mol_ket(const ClassArgs &a, int w) {
 template <int LA, int LB, int LC, int LD, typename R, bool BATCH>
 __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    extern __shared__ double tile[];
+    extern __shared__ __align__(16) unsigned char class_smem[];
+    R *tile = reinterpret_cast<R *>(class_smem);  // the digestion type: FP32 tile for the FP32 tier
     const int ibra = t.x, k0 = t.y, cnt = t.z;
     const DevBasis &bas = mol_basis<BATCH>(a, t.w);
-#define LIBERI_D mol_D<BATCH>(a, t.w)
+#define LIBERI_D mol_D<BATCH, R>(a, t.w)
 #define LIBERI_F mol_F<BATCH>(a, t.w)
 #define LIBERI_NBF mol_nbf<BATCH>(a, t.w)
     const int P = __ldg(mol_bra<BATCH>(a, t.w) + ibra);
@@ -786,12 +795,12 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     const int nrow = NA + NB;
     const bool use_tile = a.tile_rows != 0;
     if (use_tile) {
-        for (int i = threadIdx.x; i < nrow * LIBERI_NBF; i += CLASS_THREADS) tile[i] = 0.0;
+        for (int i = threadIdx.x; i < nrow * LIBERI_NBF; i += CLASS_THREADS) tile[i] = R(0);
         __syncthreads();
     }
-    double *slots = tile + (use_tile ? nrow * LIBERI_NBF : 0);  // per-thread partial sums (multi-pass)
-    Rows rowsA{use_tile ? tile : nullptr, LIBERI_F, LIBERI_NBF};
-    Rows rowsB{use_tile ? tile + NA * LIBERI_NBF : nullptr, LIBERI_F, LIBERI_NBF};
+    R *slots = tile + (use_tile ? nrow * LIBERI_NBF : 0);  // per-thread partial sums (multi-pass)
+    Rows<R> rowsA{use_tile ? tile : nullptr, LIBERI_F, LIBERI_NBF};
+    Rows<R> rowsB{use_tile ? tile + NA * LIBERI_NBF : nullptr, LIBERI_F, LIBERI_NBF};
     const R abx = R(A.x - B.x), aby = R(A.y - B.y), abz = R(A.z - B.z);
     const int p0 = bas.pair_prim0[P], np = bas.pair_nprim[P];
     // Warp-uniform loop: every lane of a warp runs the same iterations (the
@@ -815,16 +824,16 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
         const int2 scd = bas.pair_shell[Qd];
         const double4 C = bas.shell_xyz[scd.x], D = bas.shell_xyz[scd.y];
         const R cdx = R(C.x - D.x), cdy = R(C.y - D.y), cdz = R(C.z - D.z);
-        QuartetCtx qc;
+        QuartetCtx<R> qc;
         qc.bfA = bfA; qc.bfB = bfB;
         qc.bfC = bas.shell_bf0[scd.x]; qc.bfD = bas.shell_bf0[scd.y];
         qc.iandj = sab.x == sab.y; qc.kandl = scd.x == scd.y; qc.same = P == Qd;
-        qc.cut = a.cut; qc.Dm = LIBERI_D;
+        qc.cut = R(a.cut); qc.Dm = LIBERI_D;
         constexpr bool SM = PassShape<LA, LB, LC, LD, R>::NPASS > 1;
-        KBuf<NB, NC, ND, SM> kb;
+        KBuf<NB, NC, ND, SM, R> kb;
         kb.s = slots + threadIdx.x;
 #pragma unroll
-        for (int i = 0; i < KBuf<NB, NC, ND, SM>::N; i++) kb.at(i) = 0.0;
+        for (int i = 0; i < KBuf<NB, NC, ND, SM, R>::N; i++) kb.at(i) = R(0);
         run_passes<LA, LB, LC, LD, R>(bas, p0, np, bas.pair_prim0[Qd], act ? bas.pair_nprim[Qd] : 0, A, C, abx, aby,
                                       abz, cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb);
 #pragma unroll
@@ -838,18 +847,18 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
         for (int ic = 0; ic < NC; ic++)
 #pragma unroll
             for (int id = 0; id < ND; id++) {
-                const double v = kb.cd(ic, id);
-                if (v != 0.0) atomicAdd(LIBERI_F + tri0(qc.bfC + ic, qc.bfD + id), v);
+                const R v = kb.cd(ic, id);
+                if (v != R(0)) atomicAdd(LIBERI_F + tri0(qc.bfC + ic, qc.bfD + id), (double)v);
             }
     }
     if (use_tile) {
         __syncthreads();
         for (int i = threadIdx.x; i < nrow * LIBERI_NBF; i += CLASS_THREADS) {
-            const double v = tile[i];
-            if (v == 0.0) continue;
+            const R v = tile[i];
+            if (v == R(0)) continue;
             const int r = i / LIBERI_NBF, col = i - r * LIBERI_NBF;
             const int bf = r < NA ? bfA + r : bfB + (r - NA);
-            atomicAdd(LIBERI_F + tri0(bf, col), v);
+            atomicAdd(LIBERI_F + tri0(bf, col), (double)v);
         }
     }
 #undef LIBERI_D
@@ -897,9 +906,9 @@ template <int LA, int LB, int LC, int LD, typename R, bool BATCH>
 cudaError_t launch_shape(const ClassArgs &a, cudaStream_t st) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr bool SM = PassShape<LA, LB, LC, LD, R>::NPASS > 1;
-    const size_t slot_bytes = SM ? (size_t)KBuf<NB, NC, ND, true>::N * CLASS_THREADS * sizeof(double) : 0;
+    const size_t slot_bytes = SM ? (size_t)KBuf<NB, NC, ND, true, R>::N * CLASS_THREADS * sizeof(R) : 0;
     // the F-row tile is staged only when it fits beside the slots (227 KB per CTA)
-    const size_t tile_bytes = (size_t)(NA + NB) * a.nbf * sizeof(double);
+    const size_t tile_bytes = (size_t)(NA + NB) * a.nbf * sizeof(R);
     ClassArgs args = a;
     args.tile_rows = (a.tile_rows && tile_bytes + slot_bytes <= 220 * 1024) ? 1 : 0;
     const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes;
