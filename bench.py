@@ -488,7 +488,8 @@ def run_serve(local, rate, nsessions):
         b = M.random_molecule(int(n), seed=500 + i)
         b["schwrz"] = liberi.schwarz(b)
         pool.append(b)
-    sessions = poisson_sessions(pool, rate, nsessions, niter=15, seed=5)
+    dens = [M.density(b["num_bas"], M.nocc_of(b), seed=900 + k) for k, b in enumerate(pool)]
+    sessions = poisson_sessions(pool, rate, nsessions, niter=15, seed=5, densities=dens)
     free0, total = torch.cuda.mem_get_info(local)
     peak = [0]
     stop = threading.Event()

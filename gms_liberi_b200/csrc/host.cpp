@@ -130,30 +130,42 @@ struct liberi_handle_s {
     std::vector<void *> allocs;
 };
 
+// Handle memory is stream-ordered on the handle's stream (cudaMallocAsync /
+// cudaFreeAsync), so setting up or releasing one handle never synchronises
+// the device and stalls builds of other handles in flight.  Allocation sites
+// synchronise the handle's stream before the memory is used on other
+// streams; releases require the caller's builds on its own streams to have
+// completed (liberi_c_fock_build_device).  The host source of an upload may
+// be released on return (pageable copies are staged before the call returns).
 template <typename T>
 static cudaError_t dev_upload(liberi_handle h, T **dst, const T *src, size_t n) {
     *dst = nullptr;
     if (n == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T));
+    cudaError_t e = cudaMallocAsync((void **)dst, n * sizeof(T), h->stream);
     if (e != cudaSuccess) return e;
     h->allocs.push_back(*dst);
     h->dev.bytes += n * sizeof(T);
-    return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+    return cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, h->stream);
 }
 
 template <typename T>
 static cudaError_t dev_alloc(liberi_handle h, T **dst, size_t n) {
     *dst = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T));
+    cudaError_t e = cudaMallocAsync((void **)dst, n * sizeof(T), h->stream);
     if (e != cudaSuccess) return e;
     h->allocs.push_back(*dst);
     h->dev.bytes += n * sizeof(T);
     return cudaSuccess;
 }
 
+static void dev_release(liberi_handle h, void *p) {
+    cudaFreeAsync(p, h->stream);
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), p), h->allocs.end());
+}
+
 static void free_device(liberi_handle h) {
-    for (void *p : h->allocs) cudaFree(p);
+    for (void *p : h->allocs) cudaFreeAsync(p, h->stream);
     h->allocs.clear();
     h->dev = DeviceBuffers();
     h->d_tab = nullptr;
@@ -493,16 +505,18 @@ static DevBasis dev_basis(liberi_handle h) {
 
 // ---- build ------------------------------------------------------------------------
 static int replan(liberi_handle h) {
+    bool had_plans = false;
+    for (int k = 0; k < NKERN; k++) had_plans = had_plans || h->plan[k].d_bra != nullptr;
+    // builds of the old plans may still run on any stream (re-plans follow an
+    // option change, rarely): wait for the device before releasing them
+    if (had_plans) CUDA_TRY(cudaDeviceSynchronize());
     for (int k = 0; k < NKERN; k++) {
         PlanHost &ph = h->plan[k];
         h->dev.bytes -= plan_device_bytes(ph);
         for (void *p : {(void *)ph.d_bra, (void *)ph.d_ket, (void *)ph.d_bra_orig, (void *)ph.d_ket_orig,
                         (void *)ph.d_bra_x, (void *)ph.d_ket_x, (void *)ph.d_items, (void *)ph.d_tasks,
-                        (void *)ph.d_tasks64, (void *)ph.d_tasks32, (void *)ph.d_ntasks}) {
-            if (!p) continue;
-            cudaFree(p);
-            h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), p), h->allocs.end());
-        }
+                        (void *)ph.d_tasks64, (void *)ph.d_tasks32, (void *)ph.d_ntasks})
+            if (p) dev_release(h, p);
     }
     const BasisHost &b = h->basis;
     for (int k = 0; k < NKERN; k++) {
@@ -516,6 +530,7 @@ static int replan(liberi_handle h) {
     (void)b;
     int rc = upload_plans(h);
     if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));  // plans visible to builds on other streams
     compute_stats(h);
     h->stats.device_bytes = (int64_t)h->dev.bytes;
     h->plan_dirty = false;
@@ -1093,9 +1108,8 @@ int liberi_c_autotune(liberi_handle h, int32_t reps, int32_t *chunks_out) {
             ph.chunk = c;
             ph.tasks.clear();
             make_tasks(ph, c, 0, ph.tasks);
-            if (ph.d_tasks) {
-                cudaFree(ph.d_tasks);
-                h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)ph.d_tasks), h->allocs.end());
+            if (ph.d_tasks) {  // used only by this tuner's builds on the handle's stream
+                dev_release(h, ph.d_tasks);
                 ph.d_tasks = nullptr;
             }
             if (dev_upload(h, &ph.d_tasks, ph.tasks.data(), ph.tasks.size()) != cudaSuccess) {

@@ -37,6 +37,7 @@ class Session:
     niter: int
     seed: int
     arrival: float
+    D0: object = None           # initial packed density (host), supplied with the request
     nbytes: int = 0
     state: object = None
     it: int = 0                 # builds completed
@@ -238,7 +239,7 @@ class LiberiEngine(Engine):
         h.set_option("fp32_cut", self.fp32_cut)
         liberi.setup_from_basis(h, b)
         stream = torch.cuda.Stream(device=self.dev)
-        D0 = M.density(b["num_bas"], M.nocc_of(b), seed=s.seed)
+        D0 = s.D0 if s.D0 is not None else M.density(b["num_bas"], M.nocc_of(b), seed=s.seed)
         with torch.cuda.stream(stream):
             D = torch.from_numpy(D0).to(self.dev, non_blocking=False)
             F = torch.zeros_like(D)
@@ -281,7 +282,8 @@ class LiberiEngine(Engine):
         from . import molecules as M
         torch = self.torch
         b = s.basis
-        D = torch.from_numpy(M.density(b["num_bas"], M.nocc_of(b), seed=s.seed)).to(self.dev)
+        D0 = s.D0 if s.D0 is not None else M.density(b["num_bas"], M.nocc_of(b), seed=s.seed)
+        D = torch.from_numpy(D0).to(self.dev)
         gen = torch.Generator(device=self.dev)
         out = [D.cpu().numpy().copy()]
         for it in range(1, s.niter):
@@ -291,14 +293,17 @@ class LiberiEngine(Engine):
         return out
 
 
-def poisson_sessions(pool, rate_builds, nsessions, niter=15, seed=0):
+def poisson_sessions(pool, rate_builds, nsessions, niter=15, seed=0, densities=None):
     """Sessions drawn from `pool` (list of bases) arriving as a Poisson
-    process whose build rate is `rate_builds` (sessions at rate/niter)."""
+    process whose build rate is `rate_builds` (sessions at rate/niter).
+    `densities[k]`, when given, is the initial density sent with every
+    session of pool molecule k (client-side data, made before serving)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for i in range(nsessions):
         t += rng.exponential(niter / rate_builds)
-        b = dict(pool[int(rng.integers(0, len(pool)))])
-        out.append(Session(sid=i, basis=b, niter=niter, seed=1000 + i, arrival=t))
+        k = int(rng.integers(0, len(pool)))
+        out.append(Session(sid=i, basis=dict(pool[k]), niter=niter, seed=1000 + i, arrival=t,
+                           D0=None if densities is None else densities[k]))
     return out
