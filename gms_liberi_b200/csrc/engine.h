@@ -17,12 +17,13 @@ namespace liberi {
 
 constexpr int NKERN = 21;
 constexpr int MAXROOT = 5;
-// Rys tables: intervals of width 1 in T on [0, RYS_TMAX), 13 power-basis
-// coefficients per function in x = 2(T - k) - 1, stored padded to 14 so each
-// function is 7 aligned double2 loads.
-constexpr int RYS_NINT = 60;
-constexpr int RYS_DEG = 12;
-constexpr int RYS_NCOEF = 14;
+// Rys tables: intervals of width 1/4 in T on [0, RYS_TMAX), degree-7 power
+// basis in x = 2(4T - k) - 1 (8 coefficients: four aligned double2 loads per
+// function; interpolation error below 6e-15 relative for 1..5 roots).
+constexpr int RYS_PER_UNIT = 4;
+constexpr int RYS_NINT = 60 * RYS_PER_UNIT;
+constexpr int RYS_DEG = 7;
+constexpr int RYS_NCOEF = 8;
 constexpr double RYS_TMAX = 60.0;
 // table layout: for n = 1..5 roots, RYS_NINT intervals x 2n functions (n roots
 // then n weights) x RYS_NCOEF coefficients; then per n the large-T limit:

@@ -731,18 +731,17 @@ int liberi_c_rys_eval(int32_t n, double T, double thr, int32_t strict, double *u
         }
         return LIBERI_OK;
     }
-    const int k = (int)T;
-    const double x = 2.0 * (T - (double)k) - 1.0;
+    const double t4 = T * (double)RYS_PER_UNIT;
+    const int k = (int)t4;
+    const double x = 2.0 * (t4 - (double)k) - 1.0;
     const double *base = tab.data() + rys_table_off(n) + (size_t)k * 2 * n * RYS_NCOEF;
-    const double x2 = x * x, x4 = x2 * x2, x8 = x4 * x4;
-    for (int f = 0; f < 2 * n; f++) {
-        // same Estrin scheme as the device
+    const double x2 = x * x, x4 = x2 * x2;
+    for (int f = 0; f < 2 * n; f++) {  // same Estrin scheme as the device
         const double *c = base + f * RYS_NCOEF;
-        const double a0 = std::fma(c[1], x, c[0]), a1 = std::fma(c[3], x, c[2]), a2 = std::fma(c[5], x, c[4]);
-        const double a3 = std::fma(c[7], x, c[6]), a4 = std::fma(c[9], x, c[8]), a5 = std::fma(c[11], x, c[10]);
-        const double b0 = std::fma(a1, x2, a0), b1 = std::fma(a3, x2, a2), b2 = std::fma(a5, x2, a4);
-        const double d0 = std::fma(b1, x4, b0), d1 = std::fma(c[12], x4, b2);
-        const double v = std::fma(d1, x8, d0);
+        const double a0 = std::fma(c[1], x, c[0]), a1 = std::fma(c[3], x, c[2]);
+        const double a2 = std::fma(c[5], x, c[4]), a3 = std::fma(c[7], x, c[6]);
+        const double b0 = std::fma(a1, x2, a0), b1 = std::fma(a3, x2, a2);
+        const double v = std::fma(b1, x4, b0);
         if (f < n) u[f] = v; else w[f - n] = v;
     }
     return LIBERI_OK;

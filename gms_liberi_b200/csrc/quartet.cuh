@@ -69,21 +69,20 @@ __device__ __forceinline__ void rys_eval(double T, double thr, bool strict,
         }
         return;
     }
-    int k = (int)T;
-    double x = 2.0 * (T - (double)k) - 1.0;
+    const double t4 = T * (double)RYS_PER_UNIT;
+    const int k = (int)t4;
+    const double x = 2.0 * (t4 - (double)k) - 1.0;
     const double2 *base = reinterpret_cast<const double2 *>(tab + rys_table_off(N)) + (size_t)k * (N * RYS_NCOEF);
-    // Estrin evaluation of the degree-12 polynomial: dependency depth 5
-    const double x2 = x * x, x4 = x2 * x2, x8 = x4 * x4;
+    // Estrin evaluation of the degree-7 polynomial: dependency depth 3
+    const double x2 = x * x, x4 = x2 * x2;
 #pragma unroll
     for (int f = 0; f < 2 * N; f++) {
         const double2 *c = base + f * (RYS_NCOEF / 2);
         const double2 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2), c67 = __ldg(c + 3);
-        const double2 c89 = __ldg(c + 4), cab = __ldg(c + 5), ccd = __ldg(c + 6);
-        const double a0 = fma(c01.y, x, c01.x), a1 = fma(c23.y, x, c23.x), a2 = fma(c45.y, x, c45.x);
-        const double a3 = fma(c67.y, x, c67.x), a4 = fma(c89.y, x, c89.x), a5 = fma(cab.y, x, cab.x);
-        const double b0 = fma(a1, x2, a0), b1 = fma(a3, x2, a2), b2 = fma(a5, x2, a4);
-        const double d0 = fma(b1, x4, b0), d1 = fma(ccd.x, x4, b2);
-        const double v = fma(d1, x8, d0);
+        const double a0 = fma(c01.y, x, c01.x), a1 = fma(c23.y, x, c23.x);
+        const double a2 = fma(c45.y, x, c45.x), a3 = fma(c67.y, x, c67.x);
+        const double b0 = fma(a1, x2, a0), b1 = fma(a3, x2, a2);
+        const double v = fma(b1, x4, b0);
         if (f < N) u[f] = v; else w[f - N] = v;
     }
 }

@@ -6,16 +6,16 @@
 // in the rotated-axis kernels (src/liberi_boys.F90).  On the GPU that per-
 // quartet work is replaced by tables built here once per process:
 //   * exact roots u_i(T) = t_i^2 and weights w_i(T) of the Rys weight
-//     exp(-T t^2) on [0,1] are computed at Chebyshev nodes of every unit
-//     interval [k, k+1), k = 0..59, from the recurrence coefficients of a
+//     exp(-T t^2) on [0,1] are computed at Chebyshev nodes of every interval
+//     [k/4, (k+1)/4), k = 0..239, from the recurrence coefficients of a
 //     64-point Gauss-Legendre discretisation (Stieltjes procedure) and Sturm
 //     bisection of the Jacobi matrix, weights by Christoffel numbers;
-//   * each root and weight is interpolated by a degree-12 Chebyshev
-//     polynomial per interval and stored in power form of x = 2(T-k)-1
-//     (padded to 14 coefficients), which the device evaluates with Estrin's
-//     scheme (15 FMAs, dependency depth 5) from 7 aligned double2 loads.
-// Interpolation error is ~1e-14 relative (checked by the unit tests against
-// the oracle's 35-point procedure).  Above the class threshold the device
+//   * each root and weight is interpolated by a degree-7 Chebyshev
+//     polynomial per interval and stored in power form of x = 2(4T-k)-1
+//     (8 coefficients), which the device evaluates with Estrin's scheme
+//     (7 FMAs, dependency depth 3) from 4 aligned double2 loads.
+// Interpolation error is below 6e-15 relative (checked by the unit tests
+// against the oracle's 35-point procedure).  Above the class threshold the device
 // uses the large-T (Gauss-Hermite) limit, built here as well.  A second,
 // single-precision set (intervals of width 1/4, degree 7) serves the FP32
 // tier of the mixed-precision build.
@@ -207,7 +207,7 @@ void build_tables() {
         for (int k = 0; k < RYS_NINT; k++) {
             std::vector<std::vector<double>> f(2 * n, std::vector<double>(M));
             for (int m = 0; m < M; m++) {
-                double T = k + 0.5 * (xs[m] + 1.0);
+                double T = (k + 0.5 * (xs[m] + 1.0)) / RYS_PER_UNIT;
                 double u[MAXROOT], w[MAXROOT];
                 exact_rys(g, n, T, u, w);
                 for (int i = 0; i < n; i++) {

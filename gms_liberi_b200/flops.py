@@ -7,7 +7,7 @@ plan (liberi_c_get_stats) and the per-unit costs below count the arithmetic
 the algorithm needs (add, mul and FMA as 2, one op each for sqrt and
 division), mirroring the loop structure of csrc/quartet.cuh:
   per primitive quartet: pair geometry and T, Rys roots and weights
-  (2n polynomials of degree 12), per root the recurrence coefficients, the
+  (2n polynomials of degree 7), per root the recurrence coefficients, the
   2D vertical recurrence, the horizontal transfer on both sides and the
   assembly of the Cartesian block (two multiplies and one add per integral);
   per shell quartet: DIRFCK digestion, 6 multiply-adds per integral plus the
@@ -24,7 +24,7 @@ def class_costs(la, lb, lc, ld):
     n = (lab + lcd) // 2 + 1
     nc = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
     setup = 20
-    roots = 2 * n * 24 + 3
+    roots = 2 * n * 14 + 7
     per_root = 20
     vrr = 0
     for i in range(lab):
