@@ -486,6 +486,25 @@ constexpr int tuned_nmu_f32(int key) {
     if (key == LIBERI_TUNE_KEY) return LIBERI_TUNE_NMU;
 #endif
     switch (key) {
+        case 0: return 1;
+        case 1000: return 3;
+        case 1010: return 3;
+        case 1100: return 3;
+        case 1110: return 3;
+        case 1111: return 1;
+        case 1120: return 3;
+        case 2000: return 6;
+        case 2010: return 6;
+        case 2020: return 6;
+        case 2100: return 6;
+        case 2110: return 6;
+        case 2111: return 1;
+        case 2120: return 2;
+        case 2121: return 1;
+        case 2200: return 6;
+        case 2210: return 2;
+        case 2211: return 1;
+        case 2220: return 2;
         default: return tuned_nmu(key);
     }
 }
@@ -494,6 +513,25 @@ constexpr int tuned_minb_f32(int key) {
     if (key == LIBERI_TUNE_KEY) return LIBERI_TUNE_MINB;
 #endif
     switch (key) {
+        case 0: return 8;
+        case 1000: return 8;
+        case 1010: return 5;
+        case 1100: return 4;
+        case 1110: return 4;
+        case 1111: return 3;
+        case 1120: return 3;
+        case 2000: return 5;
+        case 2010: return 4;
+        case 2020: return 4;
+        case 2100: return 5;
+        case 2110: return 3;
+        case 2111: return 3;
+        case 2120: return 3;
+        case 2121: return 2;
+        case 2200: return 3;
+        case 2210: return 3;
+        case 2211: return 2;
+        case 2220: return 2;
         default: return tuned_minb(key);
     }
 }
