@@ -830,7 +830,11 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     const double4 A = bas.shell_xyz[sab.x], B = bas.shell_xyz[sab.y];
     const int bfA = bas.shell_bf0[sab.x], bfB = bas.shell_bf0[sab.y];
     const int nrow = NA + NB;
-    const bool use_tile = a.tile_rows != 0;
+    // the F-row tile pays for its zeroing and flush (2 (NA+NB) nbf shared
+    // accesses) only when the task's kets touch a fair part of each row;
+    // short tasks (the FP64 head of a mixed-precision item, item tails) add
+    // their K updates to F directly
+    const bool use_tile = a.tile_rows != 0 && 4 * cnt * (NC + ND) >= LIBERI_NBF;
     if (use_tile) {
         for (int i = threadIdx.x; i < nrow * LIBERI_NBF; i += CLASS_THREADS) tile[i] = R(0);
         __syncthreads();
