@@ -950,8 +950,13 @@ cudaError_t launch_shape(const ClassArgs &a, cudaStream_t st) {
     const size_t slot_bytes = SM ? (size_t)KBuf<NB, NC, ND, true, R>::N * CLASS_THREADS * sizeof(R) : 0;
     // the F-row tile is staged only when it fits beside the slots (227 KB per CTA)
     const size_t tile_bytes = (size_t)(NA + NB) * a.nbf * sizeof(R);
+    // The F-row tile is staged only when it fits beside the slots at the
+    // resident-CTA count the register budget allows: a tile that cut
+    // occupancy below it (and shrank L1, where spills live) costs more than
+    // the global atomics it saves.
+    constexpr int MINB = PassShape<LA, LB, LC, LD, R>::MINB;
     ClassArgs args = a;
-    args.tile_rows = (a.tile_rows && tile_bytes + slot_bytes <= 220 * 1024) ? 1 : 0;
+    args.tile_rows = (a.tile_rows && (tile_bytes + slot_bytes) * MINB <= 227 * 1024) ? 1 : 0;
     const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes;
     // the opt-in limit is raised to the per-CTA maximum, not to this launch's
     // size: a captured graph may hold a larger launch
