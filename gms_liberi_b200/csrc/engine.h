@@ -33,13 +33,14 @@ __host__ __device__ constexpr int rys_herm_off(int n) {
     return rys_table_off(MAXROOT + 1) + (n - 1) * 2 * MAXROOT;
 }
 constexpr int RYS_TABLE_SIZE = rys_herm_off(MAXROOT + 1);
-// Single-precision tables for the FP32 tier: intervals of width 1/4 on
-// [0, RYS_TMAX), degree-7 power basis in x = 2(4T - k) - 1 (8 coefficients,
-// two float4 loads per function); then the large-T limit as above, in float.
-constexpr int RYSF_PER_UNIT = 4;
+// Single-precision tables for the FP32 tier: intervals of width 1/8 on
+// [0, RYS_TMAX), degree-3 power basis in x = 2(8T - k) - 1 (4 coefficients:
+// one float4 load per function; interpolation error below 5e-8 relative);
+// then the large-T limit as above, in float.
+constexpr int RYSF_PER_UNIT = 8;
 constexpr int RYSF_NINT = 60 * RYSF_PER_UNIT;
-constexpr int RYSF_DEG = 7;
-constexpr int RYSF_NCOEF = 8;
+constexpr int RYSF_DEG = 3;
+constexpr int RYSF_NCOEF = 4;
 __host__ __device__ constexpr int rysf_table_off(int n) { return RYSF_NINT * RYSF_NCOEF * n * (n - 1); }
 __host__ __device__ constexpr int rysf_herm_off(int n) {
     return rysf_table_off(MAXROOT + 1) + (n - 1) * 2 * MAXROOT;

@@ -759,17 +759,14 @@ int liberi_c_rys_eval_f32(int32_t n, float T, float thr, int32_t strict, float *
         }
         return LIBERI_OK;
     }
-    const float t4 = T * (float)RYSF_PER_UNIT;
-    const int k = (int)t4;
-    const float x = 2.0f * (t4 - (float)k) - 1.0f;
+    const float t8 = T * (float)RYSF_PER_UNIT;
+    const int k = (int)t8;
+    const float x = 2.0f * (t8 - (float)k) - 1.0f;
     const float *base = tab.data() + rysf_table_off(n) + (size_t)k * 2 * n * RYSF_NCOEF;
-    const float x2 = x * x, x4 = x2 * x2;
-    for (int f = 0; f < 2 * n; f++) {  // same Estrin scheme as the device
+    const float x2 = x * x;
+    for (int f = 0; f < 2 * n; f++) {  // same evaluation as the device
         const float *c = base + f * RYSF_NCOEF;
-        const float a0 = std::fmaf(c[1], x, c[0]), a1 = std::fmaf(c[3], x, c[2]);
-        const float a2 = std::fmaf(c[5], x, c[4]), a3 = std::fmaf(c[7], x, c[6]);
-        const float b0 = std::fmaf(a1, x2, a0), b1 = std::fmaf(a3, x2, a2);
-        const float v = std::fmaf(b1, x4, b0);
+        const float v = std::fmaf(std::fmaf(c[3], x, c[2]), x2, std::fmaf(c[1], x, c[0]));
         if (f < n) u[f] = v; else w[f - n] = v;
     }
     return LIBERI_OK;

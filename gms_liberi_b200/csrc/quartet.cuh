@@ -87,8 +87,8 @@ __device__ __forceinline__ void rys_eval(double T, double thr, bool strict,
     }
 }
 
-// FP32 tier: width-1/4 intervals, degree 7 (Estrin, two float4 loads per
-// function); the large-T limit as in FP64.
+// FP32 tier: width-1/8 intervals, degree 3 (one float4 load per function);
+// the large-T limit as in FP64.
 template <int N>
 __device__ __forceinline__ void rys_eval(float T, float thr, bool strict, const float *__restrict__ tab, float *u,
                                          float *w) {
@@ -103,18 +103,15 @@ __device__ __forceinline__ void rys_eval(float T, float thr, bool strict, const 
         }
         return;
     }
-    const float t4 = T * (float)RYSF_PER_UNIT;
-    const int k = (int)t4;
-    const float x = 2.0f * (t4 - (float)k) - 1.0f;
-    const float4 *base = reinterpret_cast<const float4 *>(tab + rysf_table_off(N)) + (size_t)k * (N * RYSF_NCOEF / 2);
-    const float x2 = x * x, x4 = x2 * x2;
+    const float t8 = T * (float)RYSF_PER_UNIT;
+    const int k = (int)t8;
+    const float x = 2.0f * (t8 - (float)k) - 1.0f;
+    const float4 *base = reinterpret_cast<const float4 *>(tab + rysf_table_off(N)) + (size_t)k * (2 * N);
+    const float x2 = x * x;
 #pragma unroll
     for (int f = 0; f < 2 * N; f++) {
-        const float4 c0 = __ldg(base + 2 * f), c1 = __ldg(base + 2 * f + 1);
-        const float a0 = fmaf(c0.y, x, c0.x), a1 = fmaf(c0.w, x, c0.z);
-        const float a2 = fmaf(c1.y, x, c1.x), a3 = fmaf(c1.w, x, c1.z);
-        const float b0 = fmaf(a1, x2, a0), b1 = fmaf(a3, x2, a2);
-        const float v = fmaf(b1, x4, b0);
+        const float4 c0 = __ldg(base + f);
+        const float v = fmaf(fmaf(c0.w, x, c0.z), x2, fmaf(c0.y, x, c0.x));
         if (f < N) u[f] = v; else w[f - N] = v;
     }
 }

@@ -17,7 +17,7 @@
 // Interpolation error is below 6e-15 relative (checked by the unit tests
 // against the oracle's 35-point procedure).  Above the class threshold the device
 // uses the large-T (Gauss-Hermite) limit, built here as well.  A second,
-// single-precision set (intervals of width 1/4, degree 7) serves the FP32
+// single-precision set (intervals of width 1/8, degree 3) serves the FP32
 // tier of the mixed-precision build.
 #include <cmath>
 #include <mutex>
@@ -165,9 +165,9 @@ std::vector<double> cheb_to_power(const std::vector<double> &f) {
     return pw;
 }
 
-// FP32 tier: width-1/4 intervals, degree 7, so that the power-basis
-// coefficients stay small and single-precision evaluation keeps ~1e-7
-// relative accuracy.
+// FP32 tier: width-1/8 intervals, degree 3: one float4 per function, the
+// power-basis coefficients small, single-precision evaluation within a few
+// float ulps of the exact roots and weights.
 void build_tables_f32() {
     Grid g;
     const std::vector<double> &dt = rys_table_host();

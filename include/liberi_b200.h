@@ -194,7 +194,7 @@ int liberi_c_autotune(liberi_handle handle, int32_t reps, int32_t *chunks_out);
  * the engine's piecewise tables, evaluated on the host exactly as the device
  * does; the large-T limit is used for T > thr (strict) or T >= thr. */
 int liberi_c_rys_eval(int32_t n, double T, double thr, int32_t strict, double *u, double *w);
-/* The FP32 tier's tables (intervals of width 1/4, degree 7), evaluated in
+/* The FP32 tier's tables (intervals of width 1/8, degree 3), evaluated in
  * single precision exactly as the device does.  No counterpart in the
  * reference. */
 int liberi_c_rys_eval_f32(int32_t n, float T, float thr, int32_t strict, float *u, float *w);
