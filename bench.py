@@ -324,9 +324,9 @@ def run_ours(args):
     if not args.no_mixed:
         h.set_option("precision", 1)
         sweep = []
-        # the configured sweep is 1e-5..1e-8; 1e-4 and 1e-3 are added to
+        # the configured sweep is 1e-5..1e-8; 1e-2..1e-4 are added to
         # locate the loosest cut that still meets |dE| <= 1e-6 Eh
-        for cut in (1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8):
+        for cut in (1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8):
             h.set_option("fp32_cut", cut)
             for _ in range(2):
                 step()
