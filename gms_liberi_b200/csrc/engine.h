@@ -16,6 +16,7 @@
 namespace liberi {
 
 constexpr int NKERN = 21;
+constexpr int NVARIANT = 3;  // kernel shape variants per class and precision
 constexpr int MAXROOT = 5;
 // Rys tables: intervals of width 1/4 in T on [0, RYS_TMAX), degree-7 power
 // basis in x = 2(4T - k) - 1 (8 coefficients: four aligned double2 loads per
@@ -187,7 +188,7 @@ struct LaunchCtx {
 };
 
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
-                         int precision, int nbf, int tile_rows);  // precision 0: FP64, 1: FP32
+                         int precision, int nbf, int tile_rows, int variant = 0);  // precision 0: FP64, 1: FP32
 // one launch of class k over the tasks of several molecules (task.w = molecule)
 cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, int ntasks, int nbf_max,
                                const MolView *d_mols, const ClassView *d_cviews, bool swapped);

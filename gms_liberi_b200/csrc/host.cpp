@@ -110,6 +110,7 @@ struct liberi_handle_s {
     int device = 0;
     uint32_t class_mask = (1u << NKERN) - 1;
     int chunk[NKERN] = {};  // kets per CTA task per class (0 = default)
+    int variant[2][NKERN] = {};  // kernel shape variant per class, FP64 / FP32 tier
     bool timing = false;
     cudaEvent_t ev[NKERN + 1][2] = {};
     bool ev_recorded[NKERN] = {};
@@ -595,17 +596,17 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
             dp.tasks = ph.d_tasks;
             dp.ntasks_dev = nullptr;
             dp.ntasks = (int)ph.tasks.size();
-            CUDA_TRY(launch_class(k, ctx, dp, rs, 0, nbf, tile_rows));
+            CUDA_TRY(launch_class(k, ctx, dp, rs, 0, nbf, tile_rows, h->variant[0][k]));
         } else {
             CUDA_TRY(launch_split_tasks((int)ph.items.size(), ph.d_items, ph.d_bra_x, ph.d_ket_x, h->d_maxd,
                                         h->fp32_cut, ph.chunk, ph.d_tasks64, ph.d_tasks32, ph.d_ntasks, st));
             dp.ntasks = ph.task_cap;
             dp.tasks = ph.d_tasks64;
             dp.ntasks_dev = ph.d_ntasks;
-            CUDA_TRY(launch_class(k, ctx, dp, rs, 0, nbf, tile_rows));
+            CUDA_TRY(launch_class(k, ctx, dp, rs, 0, nbf, tile_rows, h->variant[0][k]));
             dp.tasks = ph.d_tasks32;
             dp.ntasks_dev = ph.d_ntasks + 1;
-            CUDA_TRY(launch_class(k, ctx, dp, rs, 1, nbf, tile_rows));
+            CUDA_TRY(launch_class(k, ctx, dp, rs, 1, nbf, tile_rows, h->variant[1][k]));
         }
         if (h->timing) {
             CUDA_TRY(cudaEventRecord(h->ev[k][1], st));
@@ -1092,45 +1093,77 @@ int liberi_c_autotune(liberi_handle h, int32_t reps, int32_t *chunks_out) {
     CUDA_TRY(cudaEventCreate(&e1));
     const uint32_t mask0 = h->class_mask;
     const int prec0 = h->precision;
-    h->precision = 0;
+    const double cut0 = h->fp32_cut;
     int rc = LIBERI_OK;
+    // time one configuration of class k: reps builds of that class alone
+    auto time_class = [&](int k, float *ms) -> int {
+        h->class_mask = 1u << k;
+        int r = build_on_device(h, h->dev.D, h->dev.F, h->stream);  // warm-up
+        if (r) return r;
+        cudaEventRecord(e0, h->stream);
+        for (int i = 0; i < reps && !r; i++) r = build_on_device(h, h->dev.D, h->dev.F, h->stream);
+        cudaEventRecord(e1, h->stream);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(ms, e0, e1);
+        return r;
+    };
     for (int k = 0; k < NKERN && !rc; k++) {
         if (h->plan_dirty) rc = replan(h);
         if (rc || h->plan[k].total == 0) continue;
+        // FP64: shape variant x kets per task
+        h->precision = 0;
         float best = 1e30f;
-        int best_c = h->plan[k].chunk;
-        for (int c : TUNE_CHUNKS) {
-            PlanHost &ph = h->plan[k];
-            ph.chunk = c;
-            ph.tasks.clear();
-            make_tasks(ph, c, 0, ph.tasks);
-            if (ph.d_tasks) {  // used only by this tuner's builds on the handle's stream
-                dev_release(h, ph.d_tasks);
-                ph.d_tasks = nullptr;
-            }
-            if (dev_upload(h, &ph.d_tasks, ph.tasks.data(), ph.tasks.size()) != cudaSuccess) {
-                rc = fail(LIBERI_E_NOMEM, "liberi_autotune: out of device memory");
-                break;
-            }
-            h->class_mask = 1u << k;
-            rc = build_on_device(h, h->dev.D, h->dev.F, h->stream);
-            if (rc) break;
-            cudaEventRecord(e0, h->stream);
-            for (int r = 0; r < reps && !rc; r++) rc = build_on_device(h, h->dev.D, h->dev.F, h->stream);
-            cudaEventRecord(e1, h->stream);
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best) {
-                best = ms;
-                best_c = c;
+        int best_c = h->plan[k].chunk, best_v = h->variant[0][k];
+        for (int v = 0; v < NVARIANT && !rc; v++) {
+            h->variant[0][k] = v;
+            for (int c : TUNE_CHUNKS) {
+                PlanHost &ph = h->plan[k];
+                ph.chunk = c;
+                ph.tasks.clear();
+                make_tasks(ph, c, 0, ph.tasks);
+                if (ph.d_tasks) {  // used only by this tuner's builds on the handle's stream
+                    dev_release(h, ph.d_tasks);
+                    ph.d_tasks = nullptr;
+                }
+                if (dev_upload(h, &ph.d_tasks, ph.tasks.data(), ph.tasks.size()) != cudaSuccess) {
+                    rc = fail(LIBERI_E_NOMEM, "liberi_autotune: out of device memory");
+                    break;
+                }
+                float ms = 0.f;
+                rc = time_class(k, &ms);
+                if (rc) break;
+                if (ms < best) {
+                    best = ms;
+                    best_c = c;
+                    best_v = v;
+                }
             }
         }
         if (rc) break;
         h->chunk[k] = best_c;
+        h->variant[0][k] = best_v;
+        // FP32 tier shape (handles in mixed precision): all quartets in FP32
+        if (prec0 == 1) {
+            h->precision = 1;
+            h->fp32_cut = 1e300;
+            float best32 = 1e30f;
+            int best_v32 = h->variant[1][k];
+            for (int v = 0; v < NVARIANT && !rc; v++) {
+                h->variant[1][k] = v;
+                float ms = 0.f;
+                rc = time_class(k, &ms);
+                if (!rc && ms < best32) {
+                    best32 = ms;
+                    best_v32 = v;
+                }
+            }
+            h->variant[1][k] = best_v32;
+            h->fp32_cut = cut0;
+        }
     }
     h->class_mask = mask0;
     h->precision = prec0;
+    h->fp32_cut = cut0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
@@ -1139,6 +1172,20 @@ int liberi_c_autotune(liberi_handle h, int32_t reps, int32_t *chunks_out) {
     if (chunks_out)
         for (int k = 0; k < NKERN; k++) chunks_out[k] = h->plan[k].chunk;
     return rc;
+}
+
+int liberi_c_set_class_variant(liberi_handle h, int32_t k, int32_t precision, int32_t variant) {
+    if (!h || k < 0 || k >= NKERN || precision < 0 || precision > 1 || variant < 0 || variant >= NVARIANT)
+        return fail(LIBERI_E_ARG, "liberi_set_class_variant: bad argument");
+    h->variant[precision][k] = variant;
+    return LIBERI_OK;
+}
+
+int liberi_c_get_class_variant(liberi_handle h, int32_t k, int32_t precision, int32_t *variant) {
+    if (!h || !variant || k < 0 || k >= NKERN || precision < 0 || precision > 1)
+        return fail(LIBERI_E_ARG, "liberi_get_class_variant: bad argument");
+    *variant = h->variant[precision][k];
+    return LIBERI_OK;
 }
 
 int liberi_c_set_option(liberi_handle h, const char *name, double value) {

@@ -2,8 +2,8 @@
 #include "quartet.cuh"
 
 namespace liberi {
-template cudaError_t launch_t<1, 1, 1, 1>(const ClassArgs &, int, cudaStream_t);
-template cudaError_t launch_t<2, 0, 0, 0>(const ClassArgs &, int, cudaStream_t);
-template cudaError_t launch_t<2, 1, 0, 0>(const ClassArgs &, int, cudaStream_t);
-template cudaError_t launch_t<2, 0, 1, 0>(const ClassArgs &, int, cudaStream_t);
+template cudaError_t launch_t<1, 1, 1, 1>(const ClassArgs &, int, int, cudaStream_t);
+template cudaError_t launch_t<2, 0, 0, 0>(const ClassArgs &, int, int, cudaStream_t);
+template cudaError_t launch_t<2, 1, 0, 0>(const ClassArgs &, int, int, cudaStream_t);
+template cudaError_t launch_t<2, 0, 1, 0>(const ClassArgs &, int, int, cudaStream_t);
 }  // namespace liberi

@@ -2,5 +2,5 @@
 #include "quartet.cuh"
 
 namespace liberi {
-template cudaError_t launch_t<2, 2, 2, 2>(const ClassArgs &, int, cudaStream_t);
+template cudaError_t launch_t<2, 2, 2, 2>(const ClassArgs &, int, int, cudaStream_t);
 }  // namespace liberi

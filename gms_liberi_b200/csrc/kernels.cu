@@ -15,7 +15,7 @@ static int ncart_h(int l) { return (l + 1) * (l + 2) / 2; }
     X(20, 2, 2, 2, 2)
 
 #define LIBERI_EXTERN(k, a, b, c, d) \
-    extern template cudaError_t launch_t<a, b, c, d>(const ClassArgs &, int, cudaStream_t);
+    extern template cudaError_t launch_t<a, b, c, d>(const ClassArgs &, int, int, cudaStream_t);
 LIBERI_CLASSES(LIBERI_EXTERN)
 
 // Schwarz table: sqrt(max |(ab|ab)|) per pair of one class
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(1024) split_tasks_kernel(int nitems, const int
 
 // ---- launchers -------------------------------------------------------------------
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs, int precision,
-                         int nbf, int tile_rows) {
+                         int nbf, int tile_rows, int variant) {
     const KernelDesc &kd = KDESC[k];
     ClassArgs a;
     a.b = ctx.basis;
@@ -127,7 +127,7 @@ cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const
     a.mols = nullptr;
     a.cviews = nullptr;
 #define LIBERI_CASE(kk, A, B, C, D) \
-    case kk: return launch_t<A, B, C, D>(a, precision, ctx.stream);
+    case kk: return launch_t<A, B, C, D>(a, precision, variant, ctx.stream);
     switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
 #undef LIBERI_CASE
     return cudaErrorInvalidValue;
@@ -158,7 +158,7 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     a.mols = d_mols;
     a.cviews = d_cviews;
 #define LIBERI_CASE(kk, A, B, C, D) \
-    case kk: return launch_t<A, B, C, D>(a, 0, ctx.stream);
+    case kk: return launch_t<A, B, C, D>(a, 0, 0, ctx.stream);
     switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
 #undef LIBERI_CASE
     return cudaErrorInvalidValue;

@@ -533,18 +533,34 @@ constexpr int tuned_minb_f32(int key) {
     }
 }
 
-template <int LA, int LB, int LC, int LD, typename R>
+// Alternative shapes per class and precision (variants 1..NVARIANT-1), chosen
+// at run time by the autotuner; 0 in a table means "same as variant 0".
+constexpr int alt_nmu(int key, bool f32, int v) {
+    (void)key; (void)f32; (void)v;
+    return 0;
+}
+constexpr int alt_minb(int key, bool f32, int v) {
+    (void)key; (void)f32; (void)v;
+    return 0;
+}
+
+template <int LA, int LB, int LC, int LD, typename R, int V = 0>
 struct PassShape {
     static constexpr bool F32 = std::is_same<R, float>::value;
     static constexpr int KEY = class_key(LA, LB, LC, LD);
     static constexpr int PER_MU = ncart(LB) * ncart(LC) * ncart(LD);
     static constexpr int NA = ncart(LA);
     static constexpr int NMU_DEF = PER_MU >= 40 ? 1 : (40 / PER_MU);
-    static constexpr int NMU_TUNED = F32 ? tuned_nmu_f32(KEY) : tuned_nmu(KEY);
+    static constexpr int NMU_V0 = F32 ? tuned_nmu_f32(KEY) : tuned_nmu(KEY);
+    static constexpr int NMU_TUNED = (V > 0 && alt_nmu(KEY, F32, V) > 0) ? alt_nmu(KEY, F32, V) : NMU_V0;
     static constexpr int NMU_T = NMU_TUNED > 0 ? NMU_TUNED : NMU_DEF;
     static constexpr int NMU = NMU_T > NA ? NA : NMU_T;
     static constexpr int NPASS = (NA + NMU - 1) / NMU;
-    static constexpr int MINB = F32 ? tuned_minb_f32(KEY) : tuned_minb(KEY);
+    static constexpr int MINB_V0 = F32 ? tuned_minb_f32(KEY) : tuned_minb(KEY);
+    static constexpr int MINB = (V > 0 && alt_minb(KEY, F32, V) > 0) ? alt_minb(KEY, F32, V) : MINB_V0;
+    // a variant is compiled only when it differs from variant 0
+    static constexpr bool DISTINCT = V == 0 || NMU != PassShape<LA, LB, LC, LD, R, 0>::NMU ||
+                                     MINB != PassShape<LA, LB, LC, LD, R, 0>::MINB;
 };
 
 constexpr int CLASS_THREADS = 128;
@@ -684,14 +700,14 @@ __device__ __forceinline__ void digest_row_general(const R (&a)[ncart(LB)][ncart
 }
 
 // Runtime loop over passes of NMU A components; digestion of each pass.
-template <int LA, int LB, int LC, int LD, typename R, typename KB>
+template <int LA, int LB, int LC, int LD, typename R, int V, typename KB>
 __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, int q0, int nq, const double4 &A,
                                            const double4 &C, R abx, R aby, R abz, R cdx, R cdy, R cdz,
                                            double thr, bool strict, const double *__restrict__ tab,
                                            const float *__restrict__ tabf, const QuartetCtx<R> &qc,
                                            const Rows<R> &rows, KB &kb) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    using PS = PassShape<LA, LB, LC, LD, R>;
+    using PS = PassShape<LA, LB, LC, LD, R, V>;
     constexpr int M = PS::NMU;
 #pragma unroll 1
     for (int pass = 0; pass < PS::NPASS; pass++) {
@@ -812,7 +828,7 @@ __device__ __forceinline__ const int *mol_ket(const ClassArgs &a, int w) {
 }
 
 // One CTA task: row pair t.x against kets t.y .. t.y+t.z-1 of one molecule.
-template <int LA, int LB, int LC, int LD, typename R, bool BATCH>
+template <int LA, int LB, int LC, int LD, typename R, bool BATCH, int V>
 __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     extern __shared__ __align__(16) unsigned char class_smem[];
@@ -867,12 +883,12 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
         qc.bfC = bas.shell_bf0[scd.x]; qc.bfD = bas.shell_bf0[scd.y];
         qc.iandj = sab.x == sab.y; qc.kandl = scd.x == scd.y; qc.same = P == Qd;
         qc.cut = R(a.cut); qc.Dm = LIBERI_D;
-        constexpr bool SM = PassShape<LA, LB, LC, LD, R>::NPASS > 1;
+        constexpr bool SM = PassShape<LA, LB, LC, LD, R, V>::NPASS > 1;
         KBuf<NB, NC, ND, SM, R> kb;
         kb.s = slots + threadIdx.x;
 #pragma unroll
         for (int i = 0; i < KBuf<NB, NC, ND, SM, R>::N; i++) kb.at(i) = R(0);
-        run_passes<LA, LB, LC, LD, R>(bas, p0, np, bas.pair_prim0[Qd], act ? bas.pair_nprim[Qd] : 0, A, C, abx, aby,
+        run_passes<LA, LB, LC, LD, R, V>(bas, p0, np, bas.pair_prim0[Qd], act ? bas.pair_nprim[Qd] : 0, A, C, abx, aby,
                                       abz, cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
@@ -906,12 +922,12 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
 
 // BATCH: the task's w field selects the molecule (basis, D, F, plan lists);
 // the launch sized the shared-memory tile for the largest molecule.
-template <int LA, int LB, int LC, int LD, typename R, bool BATCH>
-__global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD, R>::MINB) class_kernel(ClassArgs a) {
+template <int LA, int LB, int LC, int LD, typename R, bool BATCH, int V>
+__global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD, R, V>::MINB) class_kernel(ClassArgs a) {
     const int ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
     if ((int)blockIdx.x >= ntasks) return;
     const int4 t = a.tasks[blockIdx.x];
-    class_task<LA, LB, LC, LD, R, BATCH>(a, t);
+    class_task<LA, LB, LC, LD, R, BATCH, V>(a, t);
 }
 
 // sqrt(max |(ab|ab)|) over the components of one pair, for the Schwarz table.
@@ -940,10 +956,10 @@ __device__ __forceinline__ double schwarz_diag(const DevBasis &b, int P, const d
     return sqrt(m);
 }
 
-template <int LA, int LB, int LC, int LD, typename R, bool BATCH>
+template <int LA, int LB, int LC, int LD, typename R, bool BATCH, int V>
 cudaError_t launch_shape(const ClassArgs &a, cudaStream_t st) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    constexpr bool SM = PassShape<LA, LB, LC, LD, R>::NPASS > 1;
+    constexpr bool SM = PassShape<LA, LB, LC, LD, R, V>::NPASS > 1;
     const size_t slot_bytes = SM ? (size_t)KBuf<NB, NC, ND, true, R>::N * CLASS_THREADS * sizeof(R) : 0;
     // the F-row tile is staged only when it fits beside the slots (227 KB per CTA)
     const size_t tile_bytes = (size_t)(NA + NB) * a.nbf * sizeof(R);
@@ -951,25 +967,38 @@ cudaError_t launch_shape(const ClassArgs &a, cudaStream_t st) {
     // resident-CTA count the register budget allows: a tile that cut
     // occupancy below it (and shrank L1, where spills live) costs more than
     // the global atomics it saves.
-    constexpr int MINB = PassShape<LA, LB, LC, LD, R>::MINB;
+    constexpr int MINB = PassShape<LA, LB, LC, LD, R, V>::MINB;
     ClassArgs args = a;
     args.tile_rows = (a.tile_rows && (tile_bytes + slot_bytes) * MINB <= 227 * 1024) ? 1 : 0;
     const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes;
     // the opt-in limit is raised to the per-CTA maximum, not to this launch's
     // size: a captured graph may hold a larger launch
-    cudaError_t e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, R, BATCH>,
+    cudaError_t e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, R, BATCH, V>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     if (e != cudaSuccess) return e;
-    class_kernel<LA, LB, LC, LD, R, BATCH><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
+    class_kernel<LA, LB, LC, LD, R, BATCH, V><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
     return cudaGetLastError();
 }
 
+template <int LA, int LB, int LC, int LD, typename R>
+cudaError_t launch_variant(const ClassArgs &a, int variant, cudaStream_t st) {
+    if (variant == 1 && PassShape<LA, LB, LC, LD, R, 1>::DISTINCT) {
+        if constexpr (PassShape<LA, LB, LC, LD, R, 1>::DISTINCT) return launch_shape<LA, LB, LC, LD, R, false, 1>(a, st);
+    }
+    if (variant == 2 && PassShape<LA, LB, LC, LD, R, 2>::DISTINCT) {
+        if constexpr (PassShape<LA, LB, LC, LD, R, 2>::DISTINCT) return launch_shape<LA, LB, LC, LD, R, false, 2>(a, st);
+    }
+    return launch_shape<LA, LB, LC, LD, R, false, 0>(a, st);
+}
+
+// precision 0: FP64, 1: FP32; variant: shape variant (0..NVARIANT-1; a
+// variant identical to 0 runs 0); batched launches run FP64 variant 0.
 template <int LA, int LB, int LC, int LD>
-cudaError_t launch_t(const ClassArgs &a, int precision, cudaStream_t st) {
+cudaError_t launch_t(const ClassArgs &a, int precision, int variant, cudaStream_t st) {
     if (a.ntasks <= 0) return cudaSuccess;
-    if (a.mols) return launch_shape<LA, LB, LC, LD, double, true>(a, st);
-    if (precision == 0) return launch_shape<LA, LB, LC, LD, double, false>(a, st);
-    return launch_shape<LA, LB, LC, LD, float, false>(a, st);
+    if (a.mols) return launch_shape<LA, LB, LC, LD, double, true, 0>(a, st);
+    if (precision == 0) return launch_variant<LA, LB, LC, LD, double>(a, variant, st);
+    return launch_variant<LA, LB, LC, LD, float>(a, variant, st);
 }
 
 }  // namespace liberi

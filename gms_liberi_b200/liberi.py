@@ -34,7 +34,8 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_schwarz_noalloc", "liberi_c_batch_create", "liberi_c_batch_bind",
            "liberi_c_batch_fock_build", "liberi_c_batch_capture", "liberi_c_batch_launch",
            "liberi_c_batch_synchronize", "liberi_c_batch_autotune", "liberi_c_batch_destroy",
-           "liberi_c_autotune", "liberi_c_rys_eval_f32", "liberi_c_setup_bytes"]
+           "liberi_c_autotune", "liberi_c_rys_eval_f32", "liberi_c_setup_bytes",
+           "liberi_c_set_class_variant", "liberi_c_get_class_variant"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -107,6 +108,8 @@ def lib():
         L.liberi_c_batch_autotune.argtypes = [H, ctypes.c_int32, _I32P]
         L.liberi_c_batch_destroy.argtypes = [H]
         L.liberi_c_autotune.argtypes = [H, ctypes.c_int32, _I32P]
+        L.liberi_c_set_class_variant.argtypes = [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+        L.liberi_c_get_class_variant.argtypes = [H, ctypes.c_int32, ctypes.c_int32, _I32P]
         L.liberi_c_kernel_name.restype = ctypes.c_char_p
         for name in EXPORTS:
             if name != "liberi_c_kernel_name":
@@ -148,6 +151,15 @@ class LiberiHandle:
 
     def set_option(self, name, value):
         _check(lib().liberi_c_set_option(self._h, name.encode(), float(value)))
+
+    def set_class_variant(self, k, precision, variant):
+        """Kernel shape variant of class k (0..20) for precision 0/1."""
+        _check(lib().liberi_c_set_class_variant(self._h, int(k), int(precision), int(variant)))
+
+    def get_class_variant(self, k, precision):
+        v = ctypes.c_int32()
+        _check(lib().liberi_c_get_class_variant(self._h, int(k), int(precision), ctypes.byref(v)))
+        return v.value
 
     def get_option(self, name):
         v = ctypes.c_double()

@@ -185,10 +185,18 @@ int liberi_c_batch_synchronize(liberi_batch batch);
 int liberi_c_batch_autotune(liberi_batch batch, int32_t reps, int32_t *chunks_out);
 int liberi_c_batch_destroy(liberi_batch batch);
 
-/* Autotuner for one handle: per class, the fastest of 128..2048 kets per CTA
- * task on the handle's own device buffers (their contents are overwritten);
- * the plan is rebuilt with the choice.  No counterpart in the reference. */
+/* Autotuner for one handle: per class, the fastest kernel shape variant
+ * (A components per pass and resident CTAs per SM, 0..2) and number of kets
+ * per CTA task (128..2048) on the handle's own device buffers (their
+ * contents are overwritten), and for a mixed-precision handle the fastest
+ * FP32-tier shape; the plan is rebuilt with the choice.  No counterpart in
+ * the reference. */
 int liberi_c_autotune(liberi_handle handle, int32_t reps, int32_t *chunks_out);
+/* Kernel shape variant of class k (driver order 0..20) for precision 0
+ * (FP64) or 1 (FP32 tier); variant 0 is the default, a variant that is not
+ * distinct for a class runs variant 0.  No counterpart in the reference. */
+int liberi_c_set_class_variant(liberi_handle handle, int32_t k, int32_t precision, int32_t variant);
+int liberi_c_get_class_variant(liberi_handle handle, int32_t k, int32_t precision, int32_t *variant);
 
 /* Rys roots u_i = t_i^2 and weights w_i (sum w_i = F_0(T)) for n = 1..5 from
  * the engine's piecewise tables, evaluated on the host exactly as the device

@@ -107,3 +107,16 @@ def test_engine_fp32_rys_tables(n):
         uo, wo = oracle.rys_roots(n, float(np.float32(T)), thr=60.0)
         worst = max(worst, np.max(np.abs(uf - uo) / np.abs(uo)), np.max(np.abs(wf - wo) / np.abs(wo)))
     assert worst <= 3e-6, worst
+
+
+def test_class_variant_arguments():
+    # shape variants are per class (0..20), per precision (0 FP64, 1 FP32), 0..2
+    h = liberi.liberi_create()
+    assert h.get_class_variant(5, 0) == 0 and h.get_class_variant(5, 1) == 0
+    h.set_class_variant(5, 1, 2)
+    assert h.get_class_variant(5, 1) == 2 and h.get_class_variant(5, 0) == 0
+    for bad in ((21, 0, 0), (-1, 0, 0), (0, 2, 0), (0, 0, 3), (0, 0, -1)):
+        with pytest.raises(liberi.LiberiError) as e:
+            h.set_class_variant(*bad)
+        assert e.value.code == -1
+    liberi.liberi_destroy(h)
