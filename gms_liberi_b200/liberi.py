@@ -35,7 +35,8 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_batch_fock_build", "liberi_c_batch_capture", "liberi_c_batch_launch",
            "liberi_c_batch_synchronize", "liberi_c_batch_autotune", "liberi_c_batch_destroy",
            "liberi_c_autotune", "liberi_c_rys_eval_f32", "liberi_c_setup_bytes",
-           "liberi_c_set_class_variant", "liberi_c_get_class_variant"]
+           "liberi_c_set_class_variant", "liberi_c_get_class_variant", "liberi_c_mdi_create",
+           "liberi_c_mdi_payload", "liberi_c_mdi_execute", "liberi_c_mdi_destroy"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -108,6 +109,10 @@ def lib():
         L.liberi_c_batch_autotune.argtypes = [H, ctypes.c_int32, _I32P]
         L.liberi_c_batch_destroy.argtypes = [H]
         L.liberi_c_autotune.argtypes = [H, ctypes.c_int32, _I32P]
+        L.liberi_c_mdi_create.argtypes = [ctypes.POINTER(H), ctypes.c_int32, ctypes.c_int32]
+        L.liberi_c_mdi_payload.argtypes = [H, ctypes.c_char_p, _I32P, ctypes.POINTER(ctypes.c_int64)]
+        L.liberi_c_mdi_execute.argtypes = [H, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64, _I32P]
+        L.liberi_c_mdi_destroy.argtypes = [H]
         L.liberi_c_set_class_variant.argtypes = [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
         L.liberi_c_get_class_variant.argtypes = [H, ctypes.c_int32, ctypes.c_int32, _I32P]
         L.liberi_c_kernel_name.restype = ctypes.c_char_p
@@ -335,6 +340,54 @@ class Batch:
         if self._b:
             _check(lib().liberi_c_batch_destroy(self._b))
             self._b = ctypes.c_void_p()
+
+
+class MDIEngine:
+    """The MDI plugin's command set (liberi_c_mdi_*): `send(cmd, data)` for
+    '>' commands, `recv(cmd)` for '<' commands, `command(cmd)` for the rest;
+    returns or raises like the C ABI.  A driver emulation for tests and for
+    Python front ends of the plugin."""
+
+    TYPES = {1: np.int32, 2: np.float64, 3: np.uint8}
+
+    def __init__(self, rank=0, nprocs=1):
+        self._s = ctypes.c_void_p()
+        _check(lib().liberi_c_mdi_create(ctypes.byref(self._s), int(rank), int(nprocs)))
+        self.terminated = False
+
+    def payload(self, cmd):
+        t = ctypes.c_int32()
+        n = ctypes.c_int64()
+        _check(lib().liberi_c_mdi_payload(self._s, cmd.encode(), ctypes.byref(t), ctypes.byref(n)))
+        return t.value, n.value
+
+    def _run(self, cmd, buf, count):
+        term = ctypes.c_int32()
+        ptr = None if buf is None else buf.ctypes.data_as(ctypes.c_void_p)
+        _check(lib().liberi_c_mdi_execute(self._s, cmd.encode(), ptr, int(count), ctypes.byref(term)))
+        self.terminated = bool(term.value)
+
+    def send(self, cmd, data):
+        t, n = self.payload(cmd)
+        if t == 3:
+            buf = np.frombuffer(data.ljust(n)[:n].encode(), dtype=np.uint8).copy()
+        else:
+            buf = np.ascontiguousarray(np.atleast_1d(data), dtype=self.TYPES[t])
+        self._run(cmd, buf, buf.size)
+
+    def recv(self, cmd):
+        t, n = self.payload(cmd)
+        buf = np.zeros(n, dtype=self.TYPES[t])
+        self._run(cmd, buf, n)
+        return buf
+
+    def command(self, cmd):
+        self._run(cmd, None, 0)
+
+    def destroy(self):
+        if self._s:
+            _check(lib().liberi_c_mdi_destroy(self._s))
+            self._s = ctypes.c_void_p()
 
 
 def rys_eval(n, T, thr=60.0, strict=False):

@@ -219,6 +219,30 @@ int liberi_c_microbench(int32_t kind, double *result);
 /* Name of kernel class k (0..20), e.g. "int2222"; NULL if out of range. */
 const char *liberi_c_kernel_name(int32_t k);
 
+/* ---- MDI plugin command set (liberi_mdi_api.F90:194-428), transport-free ----
+ * The reference's plugin answers MDI commands from GAMESS: '>' commands
+ * deliver data (accumulated in a persistent state), '>SCHWZ_INT' runs
+ * liberi_setup, '>AO_DENS' delivers D, '<FOCK' returns F.  This object is that
+ * state machine; an MDI plugin shim (MDI_Plugin_init_ERI / open / close,
+ * linked against the MDI library) receives each command, asks
+ * liberi_c_mdi_payload for the element type and count it carries, moves the
+ * payload with MDI_Recv / MDI_Send and calls liberi_c_mdi_execute.  '<FOCK'
+ * writes this rank's partial F; the shim sums the ranks' partials (MPI_Reduce
+ * in the reference, an NCCL reduction on GPUs) before sending.  'EXIT' sets
+ * *terminate and keeps the state for the next launch; 'EXIT_CONVERGED' also
+ * releases the handle.  Open-shell commands ('<FOCK_B') return
+ * LIBERI_E_UNSUPPORTED; commands the reference registers without handling
+ * ('<COORDS', '>FOCK', '>FOCK_B') and unknown ones return LIBERI_E_ARG.
+ * '>RANK_ID' / '>NUM_PROCS' (registered, not handled by the reference) set the
+ * rank split used at setup; liberi_c_mdi_create takes the same from the
+ * shim's communicator. */
+typedef struct liberi_mdi_s *liberi_mdi;
+enum { LIBERI_MDI_NONE = 0, LIBERI_MDI_INT = 1, LIBERI_MDI_DOUBLE = 2, LIBERI_MDI_CHAR = 3 };
+int liberi_c_mdi_create(liberi_mdi *state, int32_t my_rank, int32_t num_procs);
+int liberi_c_mdi_payload(liberi_mdi state, const char *command, int32_t *type, int64_t *count);
+int liberi_c_mdi_execute(liberi_mdi state, const char *command, void *buffer, int64_t count, int32_t *terminate);
+int liberi_c_mdi_destroy(liberi_mdi state);
+
 #ifdef __cplusplus
 }
 #endif
