@@ -451,22 +451,22 @@ constexpr int tuned_minb(int key) {
 #endif
     switch (key) {
         case 0: return 6;
-        case 1000: return 5;
+        case 1000: return 6;
         case 1010: return 4;
         case 1100: return 4;
         case 1110: return 3;
         case 1111: return 3;
         case 1120: return 2;
-        case 2000: return 4;
-        case 2010: return 3;
+        case 2000: return 6;
+        case 2010: return 5;
         case 2020: return 2;
-        case 2100: return 3;
+        case 2100: return 4;
         case 2110: return 2;
         case 2111: return 3;
         case 2120: return 3;
         case 2121: return 2;
         case 2200: return 2;
-        case 2210: return 2;
+        case 2210: return 3;
         case 2211: return 2;
         case 2220: return 2;
         case 2221: return 2;
@@ -488,14 +488,14 @@ constexpr int tuned_nmu_f32(int key) {
         case 1010: return 3;
         case 1100: return 3;
         case 1110: return 3;
-        case 1111: return 1;
+        case 1111: return 3;
         case 1120: return 3;
         case 2000: return 6;
         case 2010: return 6;
         case 2020: return 6;
         case 2100: return 6;
         case 2110: return 6;
-        case 2111: return 1;
+        case 2111: return 3;
         case 2120: return 2;
         case 2121: return 1;
         case 2200: return 6;
@@ -512,17 +512,17 @@ constexpr int tuned_minb_f32(int key) {
     switch (key) {
         case 0: return 8;
         case 1000: return 8;
-        case 1010: return 5;
-        case 1100: return 4;
-        case 1110: return 4;
-        case 1111: return 3;
+        case 1010: return 8;
+        case 1100: return 6;
+        case 1110: return 5;
+        case 1111: return 2;
         case 1120: return 3;
-        case 2000: return 5;
-        case 2010: return 4;
+        case 2000: return 6;
+        case 2010: return 6;
         case 2020: return 4;
         case 2100: return 5;
         case 2110: return 3;
-        case 2111: return 3;
+        case 2111: return 2;
         case 2120: return 3;
         case 2121: return 2;
         case 2200: return 3;
@@ -535,13 +535,48 @@ constexpr int tuned_minb_f32(int key) {
 
 // Alternative shapes per class and precision (variants 1..NVARIANT-1), chosen
 // at run time by the autotuner; 0 in a table means "same as variant 0".
+// Alternative shapes (variants 1, 2) per class and precision from the
+// ptxas register/spill search: higher resident-CTA counts at the price of
+// some spills (measured: occupancy pays more than spills cost, extra passes
+// never pay); variant 0 is the default above, chosen by measurement.
+// Key: class key * 10 + variant; 0 = same as variant 0.
 constexpr int alt_nmu(int key, bool f32, int v) {
-    (void)key; (void)f32; (void)v;
-    return 0;
+    if (f32) {
+        switch (key * 10 + v) {
+            case 11001: return 3;
+            case 20101: return 6;
+            case 21101: return 6;
+            default: return 0;
+        }
+    }
+    switch (key * 10 + v) {
+        case 10001: return 3;
+        case 20001: return 6;
+        case 20101: return 6;
+        case 21001: return 6;
+        case 21002: return 6;
+        case 21101: return 6;
+        default: return 0;
+    }
 }
 constexpr int alt_minb(int key, bool f32, int v) {
-    (void)key; (void)f32; (void)v;
-    return 0;
+    if (f32) {
+        switch (key * 10 + v) {
+            case 11001: return 8;
+            case 20101: return 8;
+            case 21101: return 4;
+            default: return 0;
+        }
+    }
+    switch (key * 10 + v) {
+        case 10001: return 8;
+        case 20001: return 8;
+        case 20101: return 6;
+        case 21001: return 5;
+        case 21002: return 6;
+        case 21101: return 3;
+        default: return 0;
+    }
 }
 
 template <int LA, int LB, int LC, int LD, typename R, int V = 0>
