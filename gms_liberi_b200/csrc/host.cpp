@@ -109,6 +109,10 @@ struct liberi_handle_s {
     int precision = 0;
     int device = 0;
     uint32_t class_mask = (1u << NKERN) - 1;
+    // classes allowed to stage F rows in shared memory: none by default (the
+    // tile's shared memory costs more L1, where tables and spills live, than
+    // its atomics save; measured on C60 and the batched molecules)
+    uint32_t tile_mask = 0;
     int chunk[NKERN] = {};  // kets per CTA task per class (0 = default)
     int variant[2][NKERN] = {};  // kernel shape variant per class, FP64 / FP32 tier
     bool timing = false;
@@ -591,7 +595,7 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
         dp.swapped = kd.swap;
         const int nbf = b.num_bas;
         const size_t tile_bytes = (size_t)(ncart_l(kd.la) + ncart_l(kd.lb)) * nbf * sizeof(double);
-        const int tile_rows = tile_bytes <= TILE_MAX_BYTES ? 1 : 0;
+        const int tile_rows = (tile_bytes <= TILE_MAX_BYTES && ((h->tile_mask >> k) & 1u)) ? 1 : 0;
         if (!mixed) {
             dp.tasks = ph.d_tasks;
             dp.ntasks_dev = nullptr;
@@ -1210,6 +1214,9 @@ int liberi_c_set_option(liberi_handle h, const char *name, double value) {
     } else if (n == "class_mask") {
         if (!(value >= 0 && value < (double)(1u << NKERN))) return fail(LIBERI_E_ARG, "class_mask out of range");
         h->class_mask = (uint32_t)value;
+    } else if (n == "tile_mask") {
+        if (!(value >= 0 && value < (double)(1u << NKERN))) return fail(LIBERI_E_ARG, "tile_mask out of range");
+        h->tile_mask = (uint32_t)value;
     } else if (n == "timing") {
         h->timing = value != 0;
     } else {
@@ -1227,6 +1234,7 @@ int liberi_c_get_option(liberi_handle h, const char *name, double *value) {
     else if (n == "precision") *value = h->precision;
     else if (n == "device") *value = h->device;
     else if (n == "class_mask") *value = h->class_mask;
+    else if (n == "tile_mask") *value = h->tile_mask;
     else if (n == "timing") *value = h->timing ? 1 : 0;
     else return fail(LIBERI_E_ARG, "unknown option '%s'", name);
     return LIBERI_OK;

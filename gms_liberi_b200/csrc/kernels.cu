@@ -5,7 +5,6 @@
 
 namespace liberi {
 
-static int ncart_h(int l) { return (l + 1) * (l + 2) / 2; }
 
 #define LIBERI_CLASSES(X)                                                                    \
     X(0, 0, 0, 0, 0) X(1, 1, 0, 0, 0) X(2, 1, 1, 0, 0) X(3, 1, 1, 1, 0) X(4, 1, 0, 1, 0)         \
@@ -150,8 +149,9 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     a.ntasks_dev = nullptr;
     a.ntasks = ntasks;
     a.nbf = nbf_max;
-    const size_t tile_bytes = (size_t)(ncart_h(kd.la) + ncart_h(kd.lb)) * nbf_max * sizeof(double);
-    a.tile_rows = tile_bytes <= 160 * 1024 ? 1 : 0;
+    // F rows are updated with FP64 atomics in L2 (no shared-memory tile), as
+    // for single-molecule builds by default
+    a.tile_rows = 0;
     a.bra_ids = a.ket_ids = a.bra_orig = a.ket_orig = nullptr;
     a.swapped = swapped ? 1 : 0;
     a.rs = RankSplit{0, 1, 0, 0, 0, 0, 0, 0};

@@ -99,6 +99,9 @@ int liberi_c_last_error(char *buf, int32_t len);
  *   "precision"    (0 = all FP64, 1 = mixed FP32/FP64)
  *   "device"       (CUDA device ordinal used by the next setup, default 0)
  *   "class_mask"   (bit k set = run class k of the driver order; default all 21)
+ *   "tile_mask"    (bit k set = class k may stage rows of F in a shared-memory
+ *                   tile, where it fits; default none: F is updated with FP64
+ *                   atomics in L2, faster on B200 for every class measured)
  *   "timing"       (1 = record per-class device times for liberi_c_get_stats)
  * Options set before liberi_c_setup apply to it; cut options may also be
  * changed between builds (the quartet plan is rebuilt on the next build). */
