@@ -274,7 +274,8 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                                            const double4 &A, const double4 &C, R abx, R aby, R abz,
                                            R cdx, R cdy, R cdz, double thr, bool strict,
                                            const double *__restrict__ tab, const float *__restrict__ tabf,
-                                           int mu0, R (&acc)[NMU][ncart(LB)][ncart(LC)][ncart(LD)]) {
+                                           int mu0, R (&acc)[NMU][ncart(LB)][ncart(LC)][ncart(LD)],
+                                           R *cache_u, R *cache_w, int cache) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr int LAB = LA + LB, LCD = LC + LD;
     constexpr int NR = (LAB + LCD) / 2 + 1;
@@ -295,6 +296,7 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
             for (int ic = 0; ic < NC; ic++)
 #pragma unroll
                 for (int id = 0; id < ND; id++) acc[m][ib][ic][id] = R(0);
+    int slot = 0;  // primitive quartet index within the shell quartet (root cache)
     if constexpr (std::is_same<R, double>::value) {
         for (int kq = q0; kq < q0 + nq; kq++) {
             const double4 Qp = b.prim_P[kq];
@@ -304,16 +306,34 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                 const double4 Pp = b.prim_P[kp];
                 const double2 Px = b.prim_X[kp];
                 const double p = Pp.w, hp = Px.y;
-                const double rs = rsqrt(p + q);
-                const double ipq = rs * rs;
                 const double pqx = Pp.x - Qp.x, pqy = Pp.y - Qp.y, pqz = Pp.z - Qp.z;
-                const double T = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
-                double u[NR], w[NR];
-                rys_eval<NR>(T, thr, strict, tab, u, w);
-                const double pref = Px.x * Qx.x * rs;
+                double u[NR], w[NR];  // u_i / (p+q) and w_i times the pair prefactors
+                if (cache == 2) {
+#pragma unroll
+                    for (int i = 0; i < NR; i++) {
+                        u[i] = cache_u[slot * NR + i];
+                        w[i] = cache_w[slot * NR + i];
+                    }
+                } else {
+                    const double rs = rsqrt(p + q);
+                    const double ipq = rs * rs;
+                    const double T = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
+                    rys_eval<NR>(T, thr, strict, tab, u, w);
+                    const double pref = Px.x * Qx.x * rs;
+#pragma unroll
+                    for (int i = 0; i < NR; i++) {
+                        u[i] *= ipq;
+                        w[i] *= pref;
+                        if (cache == 1) {
+                            cache_u[slot * NR + i] = u[i];
+                            cache_w[slot * NR + i] = w[i];
+                        }
+                    }
+                }
+                slot++;
 #pragma unroll(FULL ? NR : 1)
                 for (int r = 0; r < NR; r++) {
-                    const double ui = u[0] * ipq, wr = w[0];
+                    const double ui = u[0], wr = w[0];
 #pragma unroll
                     for (int i = 0; i + 1 < NR; i++) {  // rotate the next root to the front
                         u[i] = u[i + 1];
@@ -327,7 +347,7 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                     vrr<LAB, LCD, R>(gx, R((Pp.x - A.x) - fq * pqx), R((Qp.x - C.x) + fp * pqx), b10, b01, b00, R(1));
                     vrr<LAB, LCD, R>(gy, R((Pp.y - A.y) - fq * pqy), R((Qp.y - C.y) + fp * pqy), b10, b01, b00, R(1));
                     vrr<LAB, LCD, R>(gz, R((Pp.z - A.z) - fq * pqz), R((Qp.z - C.z) + fp * pqz), b10, b01, b00,
-                                     R(wr * pref));
+                                     R(wr));
                     contract_root<LA, LB, LC, LD, R, NMU>(gx, gy, gz, abx, aby, abz, cdx, cdy, cdz, ex, ey, ez, acc);
                 }
             }
@@ -343,16 +363,34 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
             for (int kp = p0; kp < p0 + np; kp++) {
                 const float4 Pp = __ldg(Pf + kp), Pa = __ldg(Af + kp);
                 const float p = Pp.w, hp = __fdividef(0.5f, p);
-                const float rs = rsqrtf(p + q);
-                const float ipq = rs * rs;
                 const float pqx = Pp.x - Qp.x, pqy = Pp.y - Qp.y, pqz = Pp.z - Qp.z;
-                const float T = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
                 float u[NR], w[NR];
-                rys_eval<NR>(T, thrf, strict, tabf, u, w);
-                const float pref = Pa.w * Qa.w * rs;
+                if (cache == 2) {
+#pragma unroll
+                    for (int i = 0; i < NR; i++) {
+                        u[i] = cache_u[slot * NR + i];
+                        w[i] = cache_w[slot * NR + i];
+                    }
+                } else {
+                    const float rs = rsqrtf(p + q);
+                    const float ipq = rs * rs;
+                    const float T = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
+                    rys_eval<NR>(T, thrf, strict, tabf, u, w);
+                    const float pref = Pa.w * Qa.w * rs;
+#pragma unroll
+                    for (int i = 0; i < NR; i++) {
+                        u[i] *= ipq;
+                        w[i] *= pref;
+                        if (cache == 1) {
+                            cache_u[slot * NR + i] = u[i];
+                            cache_w[slot * NR + i] = w[i];
+                        }
+                    }
+                }
+                slot++;
 #pragma unroll(FULL ? NR : 1)
                 for (int r = 0; r < NR; r++) {
-                    const float ui = u[0] * ipq, wr = w[0];
+                    const float ui = u[0], wr = w[0];
 #pragma unroll
                     for (int i = 0; i + 1 < NR; i++) {
                         u[i] = u[i + 1];
@@ -363,7 +401,7 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                     R gx[LAB + 1][LCD + 1], gy[LAB + 1][LCD + 1], gz[LAB + 1][LCD + 1];
                     vrr<LAB, LCD, R>(gx, Pa.x - fq * pqx, Qa.x + fp * pqx, b10, b01, b00, 1.0f);
                     vrr<LAB, LCD, R>(gy, Pa.y - fq * pqy, Qa.y + fp * pqy, b10, b01, b00, 1.0f);
-                    vrr<LAB, LCD, R>(gz, Pa.z - fq * pqz, Qa.z + fp * pqz, b10, b01, b00, wr * pref);
+                    vrr<LAB, LCD, R>(gz, Pa.z - fq * pqz, Qa.z + fp * pqz, b10, b01, b00, wr);
                     contract_root<LA, LB, LC, LD, R, NMU>(gx, gy, gz, abx, aby, abz, cdx, cdy, cdz, ex, ey, ez, acc);
                 }
             }
@@ -453,7 +491,7 @@ constexpr int tuned_minb(int key) {
         case 0: return 6;
         case 1000: return 6;
         case 1010: return 4;
-        case 1100: return 4;
+        case 1100: return 5;
         case 1110: return 3;
         case 1111: return 3;
         case 1120: return 2;
@@ -515,7 +553,7 @@ constexpr int tuned_minb_f32(int key) {
         case 1010: return 8;
         case 1100: return 6;
         case 1110: return 5;
-        case 1111: return 2;
+        case 1111: return 3;
         case 1120: return 3;
         case 2000: return 6;
         case 2010: return 6;
@@ -544,17 +582,24 @@ constexpr int alt_nmu(int key, bool f32, int v) {
     if (f32) {
         switch (key * 10 + v) {
             case 11001: return 3;
-            case 20101: return 6;
+            case 11101: return 3;
+            case 11102: return 3;
+            case 11111: return 3;
+            case 11112: return 1;
             case 21101: return 6;
+            case 21111: return 3;
+            case 21112: return 1;
+            case 21211: return 1;
             default: return 0;
         }
     }
     switch (key * 10 + v) {
         case 10001: return 3;
-        case 20001: return 6;
-        case 20101: return 6;
-        case 21001: return 6;
-        case 21002: return 6;
+        case 10101: return 3;
+        case 10102: return 3;
+        case 11001: return 3;
+        case 11002: return 3;
+        case 11101: return 3;
         case 21101: return 6;
         default: return 0;
     }
@@ -563,17 +608,24 @@ constexpr int alt_minb(int key, bool f32, int v) {
     if (f32) {
         switch (key * 10 + v) {
             case 11001: return 8;
-            case 20101: return 8;
+            case 11101: return 6;
+            case 11102: return 8;
+            case 11111: return 3;
+            case 11112: return 4;
             case 21101: return 4;
+            case 21111: return 3;
+            case 21112: return 4;
+            case 21211: return 3;
             default: return 0;
         }
     }
     switch (key * 10 + v) {
         case 10001: return 8;
-        case 20001: return 8;
-        case 20101: return 6;
-        case 21001: return 5;
-        case 21002: return 6;
+        case 10101: return 5;
+        case 10102: return 6;
+        case 11001: return 5;
+        case 11002: return 6;
+        case 11101: return 4;
         case 21101: return 3;
         default: return 0;
     }
@@ -599,6 +651,10 @@ struct PassShape {
 };
 
 constexpr int CLASS_THREADS = 128;
+constexpr int ROOT_CACHE_PQ = 32;  // primitive quartets per shell quartet whose roots are kept across passes
+// classes whose passes reuse the roots (measured per class on C60: the FP64
+// multi-pass classes except (pd|pd); FP32 gains nothing)
+constexpr bool root_cache_on(int key, bool f32) { return !f32 && key != 2121; }
 
 // Per-quartet partial sums that outlive a pass: K updates of the B rows
 // (bc[ib][ic], bd[ib][id]) and the ket-pair J block (cd[ic][id]).  Single-
@@ -744,12 +800,22 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     using PS = PassShape<LA, LB, LC, LD, R, V>;
     constexpr int M = PS::NMU;
+    // Multi-pass classes evaluate the Rys roots and weights of each primitive
+    // quartet once: pass 0 keeps them (scaled) in a per-thread local array,
+    // later passes read them back (coalesced across the warp) instead of
+    // gathering table coefficients again; quartets with more primitive
+    // quartets than the array holds recompute them.
+    constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+    constexpr bool CACHE = PS::NPASS > 1 && root_cache_on(PS::KEY, PS::F32);
+    constexpr int CAP = CACHE ? ROOT_CACHE_PQ : 1;
+    R cache_u[CAP * NR], cache_w[CAP * NR];
+    const bool cache_ok = CACHE && np * nq <= CAP;
 #pragma unroll 1
     for (int pass = 0; pass < PS::NPASS; pass++) {
         const int mu0 = pass * M;
         R acc[M][NB][NC][ND];
         eval_block<LA, LB, LC, LD, R, M>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict, tab, tabf,
-                                         mu0, acc);
+                                         mu0, acc, cache_u, cache_w, cache_ok ? (pass == 0 ? 1 : 2) : 0);
         // The J update of the row pair (mu nu) is the same address for every
         // lane of the warp (one bra per CTA): it is summed over the warp and
         // added once.  Every lane reaches the reduction (the quartet loop is
@@ -978,7 +1044,7 @@ __device__ __forceinline__ double schwarz_diag(const DevBasis &b, int P, const d
     for (int ia = 0; ia < NA; ia++) {
         double acc[1][NB][NA][NB];
         eval_block<LA, LB, LA, LB, double, 1>(b, p0, np, p0, np, A, A, abx, aby, abz, abx, aby, abz, RYS_TMAX,
-                                              false, tab, nullptr, ia, acc);
+                                              false, tab, nullptr, ia, acc, nullptr, nullptr, 0);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
             double v = 0.0;
