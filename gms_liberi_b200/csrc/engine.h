@@ -90,11 +90,13 @@ struct MolView {
     DevBasis b;
     const double *D;
     double *F;
+    float *Df;  // FP32 tier of a mixed-precision batch: this iteration's D in float
     int nbf;
     int pad;
 };
 struct ClassView {
     const int *bra_ids, *ket_ids;
+    const double *bra_x, *ket_x;  // Schwarz values of the lists (mixed-precision split)
 };
 
 struct DevPlan {
@@ -188,11 +190,20 @@ struct LaunchCtx {
 };
 
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
-                         int precision, int nbf, int tile_rows, int variant = 0);  // precision 0: FP64, 1: FP32
+                         int precision, int nbf, int tile_rows, int variant);  // precision 0: FP64, 1: FP32
 // one launch of class k over the tasks of several molecules (task.w = molecule)
 cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, int ntasks, int nbf_max,
-                               const MolView *d_mols, const ClassView *d_cviews, bool swapped);
+                               const MolView *d_mols, const ClassView *d_cviews, bool swapped, int precision,
+                               const int *ntasks_dev);
 cudaError_t launch_zero_fock(const MolView *d_mols, int nmol, long long max_ntri, cudaStream_t stream);
+// mixed-precision batch: per molecule max|D| (as ordered bits) and the float copy of D
+cudaError_t launch_batch_prep(const MolView *d_mols, int nmol, long long max_ntri, unsigned long long *maxd,
+                              cudaStream_t stream);
+// mixed-precision batch: FP64/FP32 task lists of one class over every molecule's items
+// (item.w = molecule), as split_tasks_kernel does for one molecule
+cudaError_t launch_split_batch(int nitems, const int4 *items, const ClassView *d_cviews,
+                               const unsigned long long *maxd, double fp32_cut, int chunk, int4 *tasks64,
+                               int4 *tasks32, int *counts, cudaStream_t stream);
 cudaError_t launch_to_float(const double *src, float *dst, long long n, cudaStream_t st);
 cudaError_t launch_maxabs(const double *x, long long n, unsigned long long *out,
                           cudaStream_t stream);

@@ -64,6 +64,7 @@ static const double CUX = 50.0;                    // src/liberi_parameters.F90:
 static const double SQRT_TWOPI52 = 5.9149671727956128778;  // sqrt(2 pi^(5/2))
 static const size_t TILE_MAX_BYTES = 160 * 1024;            // shared-memory F rows per CTA
 static const int CLASS_CTA_THREADS = 128;
+static const int TUNE_CHUNKS[] = {128, 256, 512, 1024, 2048};  // kets per CTA task the autotuner tries
 
 static int ncart_l(int l) { return (l + 1) * (l + 2) / 2; }
 
@@ -657,6 +658,17 @@ struct liberi_batch_s {
     int4 *d_tasks[NKERN] = {};
     int ntasks[NKERN] = {};
     int chunk[NKERN] = {};
+    // mixed precision: every molecule's items per class (w = molecule), per-build task lists
+    int precision = 0;
+    double fp32_cut = 0.0;
+    int4 *d_items[NKERN] = {};
+    int nitems[NKERN] = {};
+    int cap[NKERN] = {};
+    int4 *d_t64[NKERN] = {}, *d_t32[NKERN] = {};
+    int *d_counts[NKERN] = {};
+    unsigned long long *d_maxd = nullptr;
+    float *d_Df = nullptr;
+    std::vector<size_t> df_off;
     bool bound = false;
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -705,10 +717,21 @@ static int batch_enqueue(liberi_batch b, cudaStream_t st, uint32_t mask) {
     ctx.eri_cut = h0->eri_cut;
     ctx.stream = st;
     ctx.num_sms = h0->num_sms;
+    const bool mixed = b->precision == 1;
+    if (mixed) CUDA_TRY(launch_batch_prep(b->d_mols, (int)b->hs.size(), b->ntri_max, b->d_maxd, st));
     for (int k = 0; k < NKERN; k++) {
         if (!((mask >> k) & 1u) || b->ntasks[k] == 0) continue;
-        CUDA_TRY(launch_class_batch(k, ctx, b->d_tasks[k], b->ntasks[k], b->nbf_max, b->d_mols, b->d_cv[k],
-                                    KDESC[k].swap));
+        if (!mixed) {
+            CUDA_TRY(launch_class_batch(k, ctx, b->d_tasks[k], b->ntasks[k], b->nbf_max, b->d_mols, b->d_cv[k],
+                                        KDESC[k].swap, 0, nullptr));
+            continue;
+        }
+        CUDA_TRY(launch_split_batch(b->nitems[k], b->d_items[k], b->d_cv[k], b->d_maxd, b->fp32_cut, b->chunk[k],
+                                    b->d_t64[k], b->d_t32[k], b->d_counts[k], st));
+        CUDA_TRY(launch_class_batch(k, ctx, b->d_t64[k], b->cap[k], b->nbf_max, b->d_mols, b->d_cv[k],
+                                    KDESC[k].swap, 0, b->d_counts[k]));
+        CUDA_TRY(launch_class_batch(k, ctx, b->d_t32[k], b->cap[k], b->nbf_max, b->d_mols, b->d_cv[k],
+                                    KDESC[k].swap, 1, b->d_counts[k] + 1));
     }
     return LIBERI_OK;
 }
@@ -928,8 +951,9 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
             delete b;
             return fail(LIBERI_E_STATE, "liberi_batch_create: handle %d is not set up", i);
         }
-        if (h->num_procs != 1 || h->device != handles[0]->device || h->precision != 0 ||
-            h->schwarz_cut != handles[0]->schwarz_cut || h->eri_cut != handles[0]->eri_cut) {
+        if (h->num_procs != 1 || h->device != handles[0]->device || h->precision != handles[0]->precision ||
+            h->schwarz_cut != handles[0]->schwarz_cut || h->eri_cut != handles[0]->eri_cut ||
+            (h->precision == 1 && h->fp32_cut != handles[0]->fp32_cut)) {
             delete b;
             return fail(LIBERI_E_ARG, "liberi_batch_create: handle %d differs in device, rank split, precision or cuts", i);
         }
@@ -955,7 +979,9 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
     b->allocs.push_back(b->d_mols);
     for (int k = 0; k < NKERN; k++) {
         std::vector<ClassView> cv(n);
-        for (int m = 0; m < n; m++) cv[m] = ClassView{b->hs[m]->plan[k].d_bra, b->hs[m]->plan[k].d_ket};
+        for (int m = 0; m < n; m++)
+            cv[m] = ClassView{b->hs[m]->plan[k].d_bra, b->hs[m]->plan[k].d_ket, b->hs[m]->plan[k].d_bra_x,
+                              b->hs[m]->plan[k].d_ket_x};
         if (cudaMalloc((void **)&b->d_cv[k], n * sizeof(ClassView)) != cudaSuccess)
             return die(fail(LIBERI_E_NOMEM, "liberi_batch_create: out of device memory"));
         b->allocs.push_back(b->d_cv[k]);
@@ -963,6 +989,44 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
         b->chunk[k] = default_chunk(k);
         rc = batch_build_tasks(b, k);
         if (rc) return die(rc);
+    }
+    b->precision = handles[0]->precision;
+    b->fp32_cut = handles[0]->fp32_cut;
+    if (b->precision == 1) {
+        // every molecule's items of a class in one list; task capacity for the
+        // smallest kets-per-task the tuner may choose
+        size_t dftot = 0;
+        for (int m = 0; m < n; m++) {
+            b->df_off.push_back(dftot);
+            const size_t nb = (size_t)b->hs[m]->basis.num_bas;
+            dftot += nb * (nb + 1) / 2;
+        }
+        if (cudaMalloc((void **)&b->d_Df, std::max<size_t>(dftot, 1) * sizeof(float)) != cudaSuccess ||
+            cudaMalloc((void **)&b->d_maxd, n * sizeof(unsigned long long)) != cudaSuccess)
+            return die(fail(LIBERI_E_NOMEM, "liberi_batch_create: out of device memory"));
+        b->allocs.push_back(b->d_Df);
+        b->allocs.push_back(b->d_maxd);
+        for (int k = 0; k < NKERN; k++) {
+            std::vector<int4> items;
+            long long cap = 0;
+            for (int m = 0; m < n; m++)
+                for (const int4 &it : b->hs[m]->plan[k].items) {
+                    items.push_back(make_int4(it.x, it.y, it.z, m));
+                    cap += (it.z + TUNE_CHUNKS[0] - 1) / TUNE_CHUNKS[0] + 1;
+                }
+            if (items.empty()) continue;
+            if (cap > INT32_MAX) return die(fail(LIBERI_E_UNSUPPORTED, "liberi_batch_create: batch too large"));
+            b->nitems[k] = (int)items.size();
+            b->cap[k] = (int)cap;
+            if (cudaMalloc((void **)&b->d_items[k], items.size() * sizeof(int4)) != cudaSuccess ||
+                cudaMalloc((void **)&b->d_t64[k], cap * sizeof(int4)) != cudaSuccess ||
+                cudaMalloc((void **)&b->d_t32[k], cap * sizeof(int4)) != cudaSuccess ||
+                cudaMalloc((void **)&b->d_counts[k], 4 * sizeof(int)) != cudaSuccess)
+                return die(fail(LIBERI_E_NOMEM, "liberi_batch_create: out of device memory"));
+            for (void *p : {(void *)b->d_items[k], (void *)b->d_t64[k], (void *)b->d_t32[k], (void *)b->d_counts[k]})
+                b->allocs.push_back(p);
+            cudaMemcpy(b->d_items[k], items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice);
+        }
     }
     *out = b;
     return LIBERI_OK;
@@ -977,6 +1041,7 @@ int liberi_c_batch_bind(liberi_batch b, const double *const *d_density, double *
         mv[m].b = dev_basis(b->hs[m]);
         mv[m].D = d_density[m];
         mv[m].F = d_fock[m];
+        mv[m].Df = b->precision == 1 ? b->d_Df + b->df_off[m] : nullptr;
         mv[m].nbf = b->hs[m]->basis.num_bas;
         mv[m].pad = 0;
     }
@@ -1041,7 +1106,6 @@ int liberi_c_batch_destroy(liberi_batch b) {
 }
 
 // ---- autotuner: kets per CTA task, per class ------------------------------------
-static const int TUNE_CHUNKS[] = {128, 256, 512, 1024, 2048};
 
 int liberi_c_batch_autotune(liberi_batch b, int32_t reps, int32_t *chunks_out) {
     if (!b || !b->bound) return fail(LIBERI_E_STATE, "liberi_batch_autotune: batch not bound");

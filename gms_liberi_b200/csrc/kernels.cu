@@ -51,50 +51,33 @@ __device__ __forceinline__ int item_split(const int4 &it, const double *bra_x, c
     return lo;
 }
 
-__global__ void __launch_bounds__(1024) split_tasks_kernel(int nitems, const int4 *items, const double *bra_x,
-                                                           const double *ket_x, const unsigned long long *maxd_bits,
-                                                           double fp32_cut, int chunk, int4 *tasks64,
-                                                           int4 *tasks32, int *counts) {
-    __shared__ int s64[1024], s32[1024];
-    __shared__ unsigned long long sq32[1024];
-    const double maxd = __longlong_as_double((long long)*maxd_bits);
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int per = (nitems + nt - 1) / nt;
-    const int i0 = min(nitems, tid * per), i1 = min(nitems, i0 + per);
-    int c64 = 0, c32 = 0;
-    unsigned long long q32 = 0;
-    for (int i = i0; i < i1; i++) {
-        const int4 it = items[i];
-        const int s = item_split(it, bra_x, ket_x, maxd, fp32_cut);
-        c64 += (s + chunk - 1) / chunk;
-        c32 += (it.z - s + chunk - 1) / chunk;
-        q32 += (unsigned long long)(it.z - s);
+// One thread per item: the split point, then output ranges reserved with
+// atomics (task order only affects load balance).  counts[0..1]: FP64 and
+// FP32 task counts, counts[2..3]: FP32 quartet count (64-bit, low word first);
+// zeroed before the launch.  BATCH: item.w is the molecule, whose Schwarz
+// lists and max|D| are used and which the tasks carry; else one molecule.
+template <bool BATCH>
+__global__ void __launch_bounds__(256) split_tasks_kernel(int nitems, const int4 *items, const double *bra_x1,
+                                                          const double *ket_x1, const ClassView *cviews,
+                                                          const unsigned long long *maxd_bits, double fp32_cut,
+                                                          int chunk, int4 *tasks64, int4 *tasks32, int *counts) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nitems) return;
+    const int4 it = items[i];
+    const double *bx = BATCH ? cviews[it.w].bra_x : bra_x1;
+    const double *kx = BATCH ? cviews[it.w].ket_x : ket_x1;
+    const double maxd = __longlong_as_double((long long)maxd_bits[BATCH ? it.w : 0]);
+    const int s = item_split(it, bx, kx, maxd, fp32_cut);
+    const int n64 = (s + chunk - 1) / chunk, n32 = (it.z - s + chunk - 1) / chunk;
+    const int w = BATCH ? it.w : 0;
+    if (n64) {
+        int o = atomicAdd(counts, n64);
+        for (int k = 0; k < s; k += chunk) tasks64[o++] = make_int4(it.x, it.y + k, min(chunk, s - k), w);
     }
-    s64[tid] = c64;
-    s32[tid] = c32;
-    sq32[tid] = q32;
-    __syncthreads();
-    for (int off = 1; off < nt; off <<= 1) {
-        int a = tid >= off ? s64[tid - off] : 0, b2 = tid >= off ? s32[tid - off] : 0;
-        unsigned long long c = tid >= off ? sq32[tid - off] : 0ull;
-        __syncthreads();
-        s64[tid] += a;
-        s32[tid] += b2;
-        sq32[tid] += c;
-        __syncthreads();
-    }
-    int o64 = tid > 0 ? s64[tid - 1] : 0, o32 = tid > 0 ? s32[tid - 1] : 0;
-    for (int i = i0; i < i1; i++) {
-        const int4 it = items[i];
-        const int s = item_split(it, bra_x, ket_x, maxd, fp32_cut);
-        for (int k = 0; k < s; k += chunk) tasks64[o64++] = make_int4(it.x, it.y + k, min(chunk, s - k), 0);
-        for (int k = s; k < it.z; k += chunk) tasks32[o32++] = make_int4(it.x, it.y + k, min(chunk, it.z - k), 0);
-    }
-    if (tid == nt - 1) {
-        counts[0] = s64[nt - 1];
-        counts[1] = s32[nt - 1];
-        counts[2] = (int)(sq32[nt - 1] & 0xffffffffull);
-        counts[3] = (int)(sq32[nt - 1] >> 32);
+    if (n32) {
+        int o = atomicAdd(counts + 1, n32);
+        for (int k = s; k < it.z; k += chunk) tasks32[o++] = make_int4(it.x, it.y + k, min(chunk, it.z - k), w);
+        atomicAdd(reinterpret_cast<unsigned long long *>(counts + 2), (unsigned long long)(it.z - s));
     }
 }
 
@@ -133,7 +116,8 @@ cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const
 }
 
 cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, int ntasks, int nbf_max,
-                               const MolView *d_mols, const ClassView *d_cviews, bool swapped) {
+                               const MolView *d_mols, const ClassView *d_cviews, bool swapped, int precision,
+                               const int *ntasks_dev) {
     const KernelDesc &kd = KDESC[k];
     ClassArgs a{};
     a.b = DevBasis{};
@@ -146,7 +130,7 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     a.thr = kd.asym;
     a.strict = !kd.rys;
     a.tasks = tasks;
-    a.ntasks_dev = nullptr;
+    a.ntasks_dev = ntasks_dev;
     a.ntasks = ntasks;
     a.nbf = nbf_max;
     // F rows are updated with FP64 atomics in L2 (no shared-memory tile), as
@@ -158,7 +142,7 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     a.mols = d_mols;
     a.cviews = d_cviews;
 #define LIBERI_CASE(kk, A, B, C, D) \
-    case kk: return launch_t<A, B, C, D>(a, 0, 0, ctx.stream);
+    case kk: return launch_t<A, B, C, D>(a, precision, 0, ctx.stream);
     switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
 #undef LIBERI_CASE
     return cudaErrorInvalidValue;
@@ -187,6 +171,33 @@ __global__ void zero_fock_kernel(const MolView *mols, int nmol, long long max_nt
         const long long n = mols[m].nbf;
         if (i < n * (n + 1) / 2) mols[m].F[i] = 0.0;
     }
+}
+
+// per molecule: max|D| (non-negative doubles order as their bits) and D in float
+__global__ void batch_prep_kernel(const MolView *mols, int nmol, long long max_ntri, unsigned long long *maxd) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < (long long)nmol * max_ntri;
+         g += stride) {
+        const int m = (int)(g / max_ntri);
+        const long long i = g - (long long)m * max_ntri;
+        const long long n = mols[m].nbf;
+        if (i >= n * (n + 1) / 2) continue;
+        const double d = mols[m].D[i];
+        mols[m].Df[i] = (float)d;
+        atomicMax(maxd + m, (unsigned long long)__double_as_longlong(fabs(d)));
+    }
+}
+
+cudaError_t launch_batch_prep(const MolView *d_mols, int nmol, long long max_ntri, unsigned long long *maxd,
+                              cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(maxd, 0, (size_t)nmol * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    const long long total = (long long)nmol * max_ntri;
+    const int threads = 256;
+    const long long want = (total + threads - 1) / threads;
+    const int blocks = (int)(want < 148LL * 16 ? (want > 0 ? want : 1) : 148LL * 16);
+    batch_prep_kernel<<<blocks, threads, 0, st>>>(d_mols, nmol, max_ntri, maxd);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_zero_fock(const MolView *d_mols, int nmol, long long max_ntri, cudaStream_t st) {
@@ -228,9 +239,20 @@ cudaError_t launch_maxabs(const double *x, long long n, unsigned long long *out,
 cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_x, const double *ket_x,
                                const unsigned long long *maxd, double fp32_cut, int chunk, int4 *tasks64,
                                int4 *tasks32, int *counts, cudaStream_t st) {
-    if (nitems <= 0) return cudaSuccess;
-    split_tasks_kernel<<<1, 1024, 0, st>>>(nitems, items, bra_x, ket_x, maxd, fp32_cut, chunk, tasks64, tasks32,
-                                           counts);
+    cudaError_t e = cudaMemsetAsync(counts, 0, 4 * sizeof(int), st);
+    if (e != cudaSuccess || nitems <= 0) return e;
+    split_tasks_kernel<false><<<(nitems + 255) / 256, 256, 0, st>>>(nitems, items, bra_x, ket_x, nullptr, maxd,
+                                                                    fp32_cut, chunk, tasks64, tasks32, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split_batch(int nitems, const int4 *items, const ClassView *d_cviews,
+                               const unsigned long long *maxd, double fp32_cut, int chunk, int4 *tasks64,
+                               int4 *tasks32, int *counts, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(counts, 0, 4 * sizeof(int), st);
+    if (e != cudaSuccess || nitems <= 0) return e;
+    split_tasks_kernel<true><<<(nitems + 255) / 256, 256, 0, st>>>(nitems, items, nullptr, nullptr, d_cviews, maxd,
+                                                                   fp32_cut, chunk, tasks64, tasks32, counts);
     return cudaGetLastError();
 }
 

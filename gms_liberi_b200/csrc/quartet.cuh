@@ -651,6 +651,9 @@ struct PassShape {
 };
 
 constexpr int CLASS_THREADS = 128;
+// dynamic shared memory a class CTA may request (below the 227 KB per-CTA
+// limit, leaving room for static shared memory)
+constexpr int CLASS_DYN_SMEM_MAX = 226 * 1024;
 constexpr int ROOT_CACHE_PQ = 32;  // primitive quartets per shell quartet whose roots are kept across passes
 // classes whose passes reuse the roots (measured per class on C60: the FP64
 // multi-pass classes except (pd|pd); FP32 gains nothing)
@@ -907,7 +910,7 @@ __device__ __forceinline__ const DevBasis &mol_basis(const ClassArgs &a, int w) 
 }
 template <bool BATCH, typename T>
 __device__ __forceinline__ const T *mol_D(const ClassArgs &a, int w) {
-    if constexpr (std::is_same<T, float>::value) return a.Dmf;  // FP32 tier (single-molecule launches)
+    if constexpr (std::is_same<T, float>::value) return BATCH ? a.mols[w].Df : a.Dmf;  // FP32 tier
     else if constexpr (BATCH) return a.mols[w].D;
     else return a.Dm;
 }
@@ -1026,9 +1029,8 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
 template <int LA, int LB, int LC, int LD, typename R, bool BATCH, int V>
 __global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD, R, V>::MINB) class_kernel(ClassArgs a) {
     const int ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
-    if ((int)blockIdx.x >= ntasks) return;
-    const int4 t = a.tasks[blockIdx.x];
-    class_task<LA, LB, LC, LD, R, BATCH, V>(a, t);
+    if ((int)blockIdx.x >= ntasks) return;  // lists counted on the device launch their capacity
+    class_task<LA, LB, LC, LD, R, BATCH, V>(a, a.tasks[blockIdx.x]);
 }
 
 // sqrt(max |(ab|ab)|) over the components of one pair, for the Schwarz table.
@@ -1070,12 +1072,12 @@ cudaError_t launch_shape(const ClassArgs &a, cudaStream_t st) {
     // the global atomics it saves.
     constexpr int MINB = PassShape<LA, LB, LC, LD, R, V>::MINB;
     ClassArgs args = a;
-    args.tile_rows = (a.tile_rows && (tile_bytes + slot_bytes) * MINB <= 227 * 1024) ? 1 : 0;
+    args.tile_rows = (a.tile_rows && (tile_bytes + slot_bytes) * MINB <= CLASS_DYN_SMEM_MAX) ? 1 : 0;
     const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes;
     // the opt-in limit is raised to the per-CTA maximum, not to this launch's
     // size: a captured graph may hold a larger launch
     cudaError_t e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, R, BATCH, V>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, CLASS_DYN_SMEM_MAX);
     if (e != cudaSuccess) return e;
     class_kernel<LA, LB, LC, LD, R, BATCH, V><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
     return cudaGetLastError();
@@ -1093,11 +1095,14 @@ cudaError_t launch_variant(const ClassArgs &a, int variant, cudaStream_t st) {
 }
 
 // precision 0: FP64, 1: FP32; variant: shape variant (0..NVARIANT-1; a
-// variant identical to 0 runs 0); batched launches run FP64 variant 0.
+// variant identical to 0 runs 0); batched launches run variant 0.
 template <int LA, int LB, int LC, int LD>
 cudaError_t launch_t(const ClassArgs &a, int precision, int variant, cudaStream_t st) {
     if (a.ntasks <= 0) return cudaSuccess;
-    if (a.mols) return launch_shape<LA, LB, LC, LD, double, true, 0>(a, st);
+    if (a.mols) {
+        if (precision == 0) return launch_shape<LA, LB, LC, LD, double, true, 0>(a, st);
+        return launch_shape<LA, LB, LC, LD, float, true, 0>(a, st);
+    }
     if (precision == 0) return launch_variant<LA, LB, LC, LD, double>(a, variant, st);
     return launch_variant<LA, LB, LC, LD, float>(a, variant, st);
 }

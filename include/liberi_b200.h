@@ -110,7 +110,9 @@ int liberi_c_get_option(liberi_handle handle, const char *name, double *value);
 
 /* Fock build on device-resident packed buffers (no host copies), enqueued on
  * `stream` (a cudaStream_t, NULL = the handle's own stream); does not
- * synchronise.  Used for device-resident benchmarking and graph capture. */
+ * synchronise.  Used for device-resident benchmarking and graph capture.
+ * Builds of one handle share its mixed-precision task lists: enqueue them on
+ * one stream (or order them), as a handle is not thread-safe in the reference. */
 int liberi_c_fock_build_device(liberi_handle handle, const double *d_density, double *d_fock,
                                void *stream);
 
@@ -168,7 +170,9 @@ int liberi_c_setup_bytes(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t m
 /* Batched Fock builds over several set-up handles (one molecule each): one
  * launch per quartet class covers every molecule (a persistent multi-molecule
  * work list), preceded by one launch that zeroes every F.  No counterpart in
- * the reference.  Handles must share device and cuts, use FP64 and one rank.
+ * the reference.  Handles must share device, cuts and precision (FP64, or
+ * mixed with one fp32_cut: each iteration then splits every molecule's work
+ * at its own max|D| on the device, inside the captured graph) and use one rank.
  *   bind:     device density / Fock buffer of every molecule (kept by address);
  *   fock_build: enqueue one SCF iteration of all molecules on `stream` (NULL:
  *             the batch's own stream);

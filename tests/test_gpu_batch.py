@@ -140,3 +140,37 @@ def test_batch_rejects_unusable_handles():
     bt.destroy()
     for h in hs + [idle]:
         liberi.liberi_destroy(h)
+
+
+def test_mixed_precision_batch_matches_single_mixed_builds():
+    # the FP32/FP64 split of every molecule at its own max|D|, made on the
+    # device inside the captured graph each iteration
+    import torch
+    mols = _mols()
+    hs = []
+    for b, _ in mols:
+        h = liberi.liberi_create()
+        h.set_option("precision", 1)
+        h.set_option("fp32_cut", 1e-7)
+        liberi.setup_from_basis(h, b)
+        hs.append(h)
+    Ds, Fs = _device_buffers(mols, seed=21)
+    bt = liberi.Batch(hs)
+    bt.bind([d.data_ptr() for d in Ds], [f.data_ptr() for f in Fs])
+    bt.capture()
+    rng = np.random.default_rng(3)
+    for it in range(2):
+        for D in Ds:
+            D.mul_(1.0 + 0.1 * it).add_(torch.tensor(1e-3 * rng.standard_normal(D.numel()), device="cuda"))
+        torch.cuda.synchronize()
+        bt.launch()
+        bt.synchronize()
+        for (b, _), h, D, F in zip(mols, hs, Ds, Fs):
+            Dh = D.cpu().numpy()
+            alone = liberi.fock(h, Dh)
+            assert np.abs(F.cpu().numpy() - alone).max() <= TOL_SAME, it
+            # and within the mixed-precision bound of the FP64 oracle
+            assert np.abs(F.cpu().numpy() - oracle.fock_build(b, Dh)).max() <= 1e-5
+    bt.destroy()
+    for h in hs:
+        liberi.liberi_destroy(h)
