@@ -67,7 +67,7 @@ def config(n):
                         "RHF two-electron Fock build, Schwarz cut 1e-10",
             "natoms": 60, "num_bas": 900, "nocc": 180, "schwarz_cut": SCHWARZ_CUT,
             "l2": "flushed between timed steps (512 MB device write outside the step events)",
-            "parallelism": "single GPU" if n == 1 else "quartets split across %d ranks, NCCL all-reduce of packed F" % n}
+            "parallelism": "single GPU" if n == 1 else ("quartets split across %d ranks in cost-balanced slices, NCCL all-reduce of packed F" % n)}
 
 
 # ------------------------------------------------------------------ reference arm
@@ -215,6 +215,8 @@ def run_ours(args):
     h = liberi.liberi_create()
     h.set_option("device", local)
     h.set_option("schwarz_cut", SCHWARZ_CUT)
+    if world > 1:
+        h.set_option("rank_split", 1)  # cost-balanced slices: the same F, even time per GPU
     liberi.setup_from_basis(h, basis, my_rank=rank, num_procs=world)
     st0 = h.stats()
     ntri = Dh.size

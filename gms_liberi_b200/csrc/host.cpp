@@ -110,6 +110,7 @@ struct liberi_handle_s {
     int precision = 0;
     int device = 0;
     uint32_t class_mask = (1u << NKERN) - 1;
+    int rank_split = 0;  // 0: the reference's per-kernel split, 1: cost-balanced contiguous slices
     // classes allowed to stage F rows in shared memory: none by default (the
     // tile's shared memory costs more L1, where tables and spills live, than
     // its atomics save; measured on C60 and the batched molecules)
@@ -281,6 +282,18 @@ static double class_max(const PairsHost &pr, int c) {
     return m;
 }
 
+// static CTA tasks of a plan: chunks of at most ph.chunk kets per item; the
+// capacity of the mixed tier's per-build lists follows
+static void build_tasks(PlanHost &ph) {
+    ph.tasks.clear();
+    ph.task_cap = 0;
+    for (const int4 &it : ph.items) {
+        for (int k0 = 0; k0 < it.z; k0 += ph.chunk)
+            ph.tasks.push_back(make_int4(it.x, it.y + k0, std::min(ph.chunk, it.z - k0), 0));
+        ph.task_cap += (it.z + ph.chunk - 1) / ph.chunk + 1;
+    }
+}
+
 static void build_plan(const PairsHost &pr, int k, double cut, int chunk, PlanHost &ph) {
     const KernelDesc &kd = KDESC[k];
     ph = PlanHost();
@@ -359,13 +372,31 @@ static void build_plan(const PairsHost &pr, int k, double cut, int chunk, PlanHo
     }
     ph.total = ph.pref[ph.nbra];
     if (ph.chunk <= 0) ph.chunk = default_chunk(k);
-    ph.tasks.clear();
-    ph.task_cap = 0;
-    for (const int4 &it : ph.items) {
-        for (int k0 = 0; k0 < it.z; k0 += ph.chunk)
-            ph.tasks.push_back(make_int4(it.x, it.y + k0, std::min(ph.chunk, it.z - k0), 0));
-        ph.task_cap += (it.z + ph.chunk - 1) / ph.chunk + 1;
+    build_tasks(ph);
+}
+
+// Cost-balanced rank split: this rank keeps the contiguous run of items
+// whose cost midpoints fall in its 1/nsize share of the class's primitive-
+// quartet total (cost of an item: nprim(row pair) x sum of its kets' nprim).
+static void balance_items(const PairsHost &pr, int rank, int nsize, PlanHost &ph) {
+    std::vector<double> cost(ph.items.size());
+    double total = 0.0;
+    for (size_t i = 0; i < ph.items.size(); i++) {
+        const int4 &it = ph.items[i];
+        double kc = 0.0;
+        for (int j = it.y; j < it.y + it.z; j++) kc += pr.nprim[ph.ket_ids[j]];
+        cost[i] = (double)pr.nprim[ph.bra_ids[it.x]] * kc + 1.0;  // + 1: empty-primitive pairs still cost
+        total += cost[i];
     }
+    std::vector<int4> mine;
+    double before = 0.0;
+    for (size_t i = 0; i < ph.items.size(); i++) {
+        const double mid = (before + 0.5 * cost[i]) / total * nsize;
+        if ((int)mid == rank || (rank == nsize - 1 && mid >= nsize)) mine.push_back(ph.items[i]);
+        before += cost[i];
+    }
+    ph.items.swap(mine);
+    build_tasks(ph);
 }
 
 static void make_tasks(const PlanHost &ph, int chunk, int mol, std::vector<int4> &out) {
@@ -414,7 +445,9 @@ static size_t basis_device_bytes(const BasisHost &b, const PairsHost &pr) {
 static void compute_stats(liberi_handle h) {
     for (int k = 0; k < NKERN; k++) {
         const PlanHost &ph = h->plan[k];
-        h->stats.quartets[k] = ph.total;
+        long long q = 0;
+        for (const int4 &it : ph.items) q += it.z;
+        h->stats.quartets[k] = q;  // this rank's share under the balanced split
         // primitive quartets: sum_i nprim(bra_i) * sum_{j<n_i} nprim(ket_j)
         std::vector<long long> kp(ph.nket + 1, 0);
         for (int j = 0; j < ph.nket; j++) kp[j + 1] = kp[j] + h->pairs.nprim[ph.ket_ids[j]];
@@ -530,7 +563,10 @@ static int replan(liberi_handle h) {
         bool run = (k == 0 && h->pairs.nl[0] > 0) || (k >= 1 && k <= 5 && h->pairs.nl[1] > 0) ||
                    (k >= 6 && h->pairs.nl[2] > 0);
         (void)kd;
-        if (run) build_plan(h->pairs, k, h->schwarz_cut, h->chunk[k], h->plan[k]);
+        if (run) {
+            build_plan(h->pairs, k, h->schwarz_cut, h->chunk[k], h->plan[k]);
+            if (h->rank_split == 1 && h->num_procs > 1) balance_items(h->pairs, h->my_rank, h->num_procs, h->plan[k]);
+        }
         else h->plan[k] = PlanHost();
     }
     (void)b;
@@ -581,7 +617,7 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
         }
         RankSplit rs;
         rs.rank = h->my_rank;
-        rs.nsize = h->num_procs;
+        rs.nsize = h->rank_split == 1 ? 1 : h->num_procs;  // balanced: the plan holds this rank's items
         rs.tile = kd.tile;
         rs.ntot = ph.ntot_ref;
         rs.nbra_ref = ph.nbra_ref;
@@ -1278,6 +1314,10 @@ int liberi_c_set_option(liberi_handle h, const char *name, double value) {
     } else if (n == "class_mask") {
         if (!(value >= 0 && value < (double)(1u << NKERN))) return fail(LIBERI_E_ARG, "class_mask out of range");
         h->class_mask = (uint32_t)value;
+    } else if (n == "rank_split") {
+        if (value != 0 && value != 1) return fail(LIBERI_E_ARG, "rank_split must be 0 or 1");
+        if (h->initialized) return fail(LIBERI_E_STATE, "rank_split must be chosen before setup");
+        h->rank_split = (int)value;
     } else if (n == "tile_mask") {
         if (!(value >= 0 && value < (double)(1u << NKERN))) return fail(LIBERI_E_ARG, "tile_mask out of range");
         h->tile_mask = (uint32_t)value;
@@ -1299,6 +1339,7 @@ int liberi_c_get_option(liberi_handle h, const char *name, double *value) {
     else if (n == "device") *value = h->device;
     else if (n == "class_mask") *value = h->class_mask;
     else if (n == "tile_mask") *value = h->tile_mask;
+    else if (n == "rank_split") *value = h->rank_split;
     else if (n == "timing") *value = h->timing ? 1 : 0;
     else return fail(LIBERI_E_ARG, "unknown option '%s'", name);
     return LIBERI_OK;

@@ -99,6 +99,10 @@ int liberi_c_last_error(char *buf, int32_t len);
  *   "precision"    (0 = all FP64, 1 = mixed FP32/FP64)
  *   "device"       (CUDA device ordinal used by the next setup, default 0)
  *   "class_mask"   (bit k set = run class k of the driver order; default all 21)
+ *   "rank_split"   (0 = the reference's per-kernel split of quartets over
+ *                   my_rank/num_procs, reproducing its partial F per rank;
+ *                   1 = cost-balanced contiguous slices of every class's work,
+ *                   the same total F with even per-rank time; before setup)
  *   "tile_mask"    (bit k set = class k may stage rows of F in a shared-memory
  *                   tile, where it fits; default none: F is updated with FP64
  *                   atomics in L2, faster on B200 for every class measured)

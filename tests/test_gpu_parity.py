@@ -195,3 +195,22 @@ def test_mixed_precision_error_bound(mol):
         dE = abs(energy(D, Fm) - energy(D, Fo))
         assert dE <= 1e-6, (cut, dE)
         assert np.abs(Fm - Fo).max() <= 1e-5
+
+
+@pytest.mark.parametrize("nsize", [2, 3, 7])
+def test_balanced_rank_split(nsize):
+    # cost-balanced contiguous slices: the same total F, even per-rank work
+    b, nocc = _molecule("random_9")
+    D = M.density(b["num_bas"], nocc, seed=8)
+    full, st_full = gpu_fock(b, D, schwarz_cut=1e-10)
+    acc = np.zeros_like(full)
+    q, pq = [], []
+    for r in range(nsize):
+        Fg, st = gpu_fock(b, D, rank=r, nproc=nsize, schwarz_cut=1e-10, rank_split=1)
+        acc += Fg
+        q.append(int(st["quartets"].sum()))
+        pq.append(int(st["prim_quartets"].sum()))
+    assert np.abs(acc - full).max() <= 1e-11
+    assert sum(q) == int(st_full["quartets"].sum())
+    assert sum(pq) == int(st_full["prim_quartets"].sum())
+    assert max(pq) <= 1.25 * (sum(pq) / nsize), pq
