@@ -101,6 +101,21 @@ static int fail(int code, const char *fmt, ...) {
                         "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
     } while (0)
 
+// Makes `dev` current for one C-ABI call and restores the caller's current
+// device on return (a library must not move its caller's CUDA context).
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) err = cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+    }
+};
+
 // ---- handle ------------------------------------------------------------------------
 struct liberi_handle_s {
     // options (defaults reproduce the reference constants)
@@ -847,7 +862,7 @@ int liberi_c_create(liberi_handle *handle) {
 int liberi_c_cleanup(liberi_handle h) {
     if (!h) return fail(LIBERI_E_ARG, "liberi_cleanup: null handle");
     if (!h->initialized) return LIBERI_OK;  // liberi_interface.F90:236
-    cudaSetDevice(h->device);
+    DeviceGuard dev_guard(h->device);
     for (int k = 0; k <= NKERN; k++)
         for (int j = 0; j < 2; j++)
             if (h->ev[k][j]) {
@@ -912,7 +927,8 @@ int liberi_c_setup(liberi_handle h, int32_t nsh, int32_t natoms, int32_t num_bas
     if (rc) return rc;
     rc = validate_basis(b);
     if (rc) return rc;
-    CUDA_TRY(cudaSetDevice(h->device));
+    DeviceGuard dev_guard(h->device);
+    CUDA_TRY(dev_guard.err);
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
     h->num_sms = prop.multiProcessorCount;
@@ -937,7 +953,8 @@ int liberi_c_fock_build_device(liberi_handle h, const double *d_density, double 
     if (!h) return fail(LIBERI_E_ARG, "liberi_fock_build: null handle");
     if (!h->initialized) return fail(LIBERI_E_STATE, "liberi_fock_build called before liberi_setup");
     if (!d_density || !d_fock) return fail(LIBERI_E_ARG, "liberi_fock_build: null device buffer");
-    CUDA_TRY(cudaSetDevice(h->device));
+    DeviceGuard dev_guard(h->device);
+    CUDA_TRY(dev_guard.err);
     cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
     int rc = build_on_device(h, d_density, d_fock, st);
     if (rc) return rc;
@@ -953,7 +970,8 @@ int liberi_c_fock_build(liberi_handle h, const double *density, double *fock, in
         return fail(LIBERI_E_SIZE, "liberi_fock_build: matrix_size %d != num_bas(num_bas+1)/2 = %lld",
                     matrix_size, n * (n + 1) / 2);
     if (!density || !fock) return fail(LIBERI_E_ARG, "liberi_fock_build: null buffer");
-    CUDA_TRY(cudaSetDevice(h->device));
+    DeviceGuard dev_guard(h->device);
+    CUDA_TRY(dev_guard.err);
     cudaStream_t st = h->stream;
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
@@ -1005,7 +1023,7 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
     }
     b->ntri_max = (long long)b->nbf_max * (b->nbf_max + 1) / 2;
     b->device = handles[0]->device;
-    cudaSetDevice(b->device);
+    DeviceGuard dev_guard(b->device);
     int rc = LIBERI_OK;
     auto die = [&](int code) { batch_free(b); delete b; return code; };
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -1070,7 +1088,8 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
 
 int liberi_c_batch_bind(liberi_batch b, const double *const *d_density, double *const *d_fock) {
     if (!b || !d_density || !d_fock) return fail(LIBERI_E_ARG, "liberi_batch_bind: null argument");
-    CUDA_TRY(cudaSetDevice(b->device));
+    DeviceGuard dev_guard(b->device);
+    CUDA_TRY(dev_guard.err);
     std::vector<MolView> mv(b->hs.size());
     for (size_t m = 0; m < b->hs.size(); m++) {
         if (!d_density[m] || !d_fock[m]) return fail(LIBERI_E_ARG, "liberi_batch_bind: null buffer %zu", m);
@@ -1090,14 +1109,16 @@ int liberi_c_batch_bind(liberi_batch b, const double *const *d_density, double *
 int liberi_c_batch_fock_build(liberi_batch b, void *stream) {
     if (!b) return fail(LIBERI_E_ARG, "liberi_batch_fock_build: null batch");
     if (!b->bound) return fail(LIBERI_E_STATE, "liberi_batch_fock_build: call liberi_c_batch_bind first");
-    CUDA_TRY(cudaSetDevice(b->device));
+    DeviceGuard dev_guard(b->device);
+    CUDA_TRY(dev_guard.err);
     return batch_enqueue(b, stream ? (cudaStream_t)stream : b->stream, (1u << NKERN) - 1);
 }
 
 int liberi_c_batch_capture(liberi_batch b) {
     if (!b) return fail(LIBERI_E_ARG, "liberi_batch_capture: null batch");
     if (!b->bound) return fail(LIBERI_E_STATE, "liberi_batch_capture: call liberi_c_batch_bind first");
-    CUDA_TRY(cudaSetDevice(b->device));
+    DeviceGuard dev_guard(b->device);
+    CUDA_TRY(dev_guard.err);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
@@ -1122,7 +1143,8 @@ int liberi_c_batch_capture(liberi_batch b) {
 
 int liberi_c_batch_launch(liberi_batch b, void *stream) {
     if (!b || !b->exec) return fail(LIBERI_E_STATE, "liberi_batch_launch: no captured graph");
-    CUDA_TRY(cudaSetDevice(b->device));
+    DeviceGuard dev_guard(b->device);
+    CUDA_TRY(dev_guard.err);
     CUDA_TRY(cudaGraphLaunch(b->exec, stream ? (cudaStream_t)stream : b->stream));
     return LIBERI_OK;
 }
@@ -1135,7 +1157,7 @@ int liberi_c_batch_synchronize(liberi_batch b) {
 
 int liberi_c_batch_destroy(liberi_batch b) {
     if (!b) return fail(LIBERI_E_ARG, "liberi_batch_destroy: null batch");
-    cudaSetDevice(b->device);
+    DeviceGuard dev_guard(b->device);
     batch_free(b);
     delete b;
     return LIBERI_OK;
@@ -1146,7 +1168,8 @@ int liberi_c_batch_destroy(liberi_batch b) {
 int liberi_c_batch_autotune(liberi_batch b, int32_t reps, int32_t *chunks_out) {
     if (!b || !b->bound) return fail(LIBERI_E_STATE, "liberi_batch_autotune: batch not bound");
     if (reps < 1) reps = 1;
-    CUDA_TRY(cudaSetDevice(b->device));
+    DeviceGuard dev_guard(b->device);
+    CUDA_TRY(dev_guard.err);
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
@@ -1191,7 +1214,8 @@ int liberi_c_batch_autotune(liberi_batch b, int32_t reps, int32_t *chunks_out) {
 int liberi_c_autotune(liberi_handle h, int32_t reps, int32_t *chunks_out) {
     if (!h || !h->initialized) return fail(LIBERI_E_STATE, "liberi_autotune: handle not set up");
     if (reps < 1) reps = 1;
-    CUDA_TRY(cudaSetDevice(h->device));
+    DeviceGuard dev_guard(h->device);
+    CUDA_TRY(dev_guard.err);
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
@@ -1382,7 +1406,7 @@ int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgto
     if (rc) return rc;
     rc = validate_basis(tmp.basis);
     if (rc) return rc;
-    CUDA_TRY(cudaSetDevice(0));
+    CUDA_TRY(cudaGetDevice(&tmp.device));  // the caller's current device
     std::vector<double4> shell_xyz;
     build_pairs(tmp.basis, tmp.pairs, shell_xyz);
     CUDA_TRY(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking));

@@ -214,3 +214,15 @@ def test_balanced_rank_split(nsize):
     assert sum(q) == int(st_full["quartets"].sum())
     assert sum(pq) == int(st_full["prim_quartets"].sum())
     assert max(pq) <= 1.25 * (sum(pq) / nsize), pq
+
+
+def test_calls_keep_the_callers_current_device():
+    # the library makes the handle's device current for a call and restores
+    # the caller's afterwards (torch and other CUDA users share the thread)
+    import torch
+    torch.cuda.set_device(0)
+    b, nocc = _molecule("h2o_like")
+    before = torch.cuda.current_device()
+    liberi.schwarz(b)
+    F, _ = gpu_fock(b, M.density(b["num_bas"], nocc))
+    assert torch.cuda.current_device() == before
