@@ -55,6 +55,19 @@ __device__ __forceinline__ long long tri1(long long i, long long j) {  // 1-base
 }
 
 // ---- Rys roots/weights -------------------------------------------------------
+// 256-bit read-only loads (sm_100): a function's coefficients are 32-byte
+// aligned in both tables (offsets are multiples of 64 bytes from a 256-byte
+// aligned base), so one lane fetches four doubles (or eight floats) per load.
+__device__ __forceinline__ void ldg_v4f64(const double *p, double &a, double &b, double &c, double &d) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(a), "=d"(b), "=d"(c), "=d"(d)
+        : "l"((unsigned long long)__cvta_generic_to_global(p)));
+}
+__device__ __forceinline__ void ldg_v8f32(const float *p, float4 &lo, float4 &hi) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(lo.x), "=f"(lo.y), "=f"(lo.z), "=f"(lo.w), "=f"(hi.x), "=f"(hi.y), "=f"(hi.z), "=f"(hi.w)
+        : "l"((unsigned long long)__cvta_generic_to_global(p)));
+}
 template <int N>
 __device__ __forceinline__ void rys_eval(double T, double thr, bool strict,
                                          const double *__restrict__ tab, double *u, double *w) {
@@ -72,22 +85,23 @@ __device__ __forceinline__ void rys_eval(double T, double thr, bool strict,
     const double t4 = T * (double)RYS_PER_UNIT;
     const int k = (int)t4;
     const double x = 2.0 * (t4 - (double)k) - 1.0;
-    const double2 *base = reinterpret_cast<const double2 *>(tab + rys_table_off(N)) + (size_t)k * (N * RYS_NCOEF);
-    // Estrin evaluation of the degree-7 polynomial: dependency depth 3
+    const double *base = tab + rys_table_off(N) + (size_t)k * (2 * N * RYS_NCOEF);
+    // two 256-bit loads per function; Estrin evaluation, dependency depth 3
     const double x2 = x * x, x4 = x2 * x2;
 #pragma unroll
     for (int f = 0; f < 2 * N; f++) {
-        const double2 *c = base + f * (RYS_NCOEF / 2);
-        const double2 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2), c67 = __ldg(c + 3);
-        const double a0 = fma(c01.y, x, c01.x), a1 = fma(c23.y, x, c23.x);
-        const double a2 = fma(c45.y, x, c45.x), a3 = fma(c67.y, x, c67.x);
+        double c0, c1, c2, c3, c4, c5, c6, c7;
+        ldg_v4f64(base + f * RYS_NCOEF, c0, c1, c2, c3);
+        ldg_v4f64(base + f * RYS_NCOEF + 4, c4, c5, c6, c7);
+        const double a0 = fma(c1, x, c0), a1 = fma(c3, x, c2);
+        const double a2 = fma(c5, x, c4), a3 = fma(c7, x, c6);
         const double b0 = fma(a1, x2, a0), b1 = fma(a3, x2, a2);
         const double v = fma(b1, x4, b0);
         if (f < N) u[f] = v; else w[f - N] = v;
     }
 }
 
-// FP32 tier: width-1/8 intervals, degree 3 (one float4 load per function);
+// FP32 tier: width-1/8 intervals, degree 3 (two functions per 256-bit load);
 // the large-T limit as in FP64.
 template <int N>
 __device__ __forceinline__ void rys_eval(float T, float thr, bool strict, const float *__restrict__ tab, float *u,
@@ -106,13 +120,16 @@ __device__ __forceinline__ void rys_eval(float T, float thr, bool strict, const 
     const float t8 = T * (float)RYSF_PER_UNIT;
     const int k = (int)t8;
     const float x = 2.0f * (t8 - (float)k) - 1.0f;
-    const float4 *base = reinterpret_cast<const float4 *>(tab + rysf_table_off(N)) + (size_t)k * (2 * N);
+    const float *base = tab + rysf_table_off(N) + (size_t)k * (2 * N * RYSF_NCOEF);
     const float x2 = x * x;
 #pragma unroll
-    for (int f = 0; f < 2 * N; f++) {
-        const float4 c0 = __ldg(base + f);
-        const float v = fmaf(fmaf(c0.w, x, c0.z), x2, fmaf(c0.y, x, c0.x));
-        if (f < N) u[f] = v; else w[f - N] = v;
+    for (int f = 0; f < 2 * N; f += 2) {  // two functions per 256-bit load
+        float4 c0, c1;
+        ldg_v8f32(base + f * RYSF_NCOEF, c0, c1);
+        const float v0 = fmaf(fmaf(c0.w, x, c0.z), x2, fmaf(c0.y, x, c0.x));
+        const float v1 = fmaf(fmaf(c1.w, x, c1.z), x2, fmaf(c1.y, x, c1.x));
+        if (f < N) u[f] = v0; else w[f - N] = v0;
+        if (f + 1 < N) u[f + 1] = v1; else w[f + 1 - N] = v1;
     }
 }
 
