@@ -78,8 +78,8 @@ struct DevBasis {
     const int *pair_nprim;     // number of kept primitive pairs
     const double4 *prim_P;     // Px, Py, Pz, p
     const double2 *prim_X;     // sqrt(2 pi^2.5) c_a c_b exp(-mu R^2) / p, 0.5 / p
-    const float4 *prim_Pf;     // FP32 tier: Px, Py, Pz, p
-    const float4 *prim_Af;     // FP32 tier: P - A (x, y, z; rounded once from FP64), prefactor
+    const float4 *prim_PAf;    // FP32 tier, two float4 per primitive pair (one 256-bit load):
+                               // (Px, Py, Pz, p), (P - A rounded once from FP64, prefactor)
 };
 
 // One launch of a class: a list of CTA tasks (bra position, first ket
@@ -165,7 +165,7 @@ struct DeviceBuffers {
     int *pair_prim0 = nullptr, *pair_nprim = nullptr;
     double4 *prim_P = nullptr;
     double2 *prim_X = nullptr;
-    float4 *prim_Pf = nullptr, *prim_Af = nullptr;
+    float4 *prim_PAf = nullptr;
     double *D = nullptr, *F = nullptr;
     float *Df = nullptr;  // FP32 tier: single-precision copy of the build's D
     long long *scratch_total = nullptr;  // device counters (mixed split)

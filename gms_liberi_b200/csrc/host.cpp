@@ -519,17 +519,16 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
     CUDA_TRY(dev_upload(h, &h->dev.prim_X, h->pairs.X.data(), h->pairs.X.size()));
     {  // FP32 tier copies: P - A is formed in FP64 and rounded once
         const PairsHost &pr = h->pairs;
-        std::vector<float4> pf(pr.P.size()), af(pr.P.size());
+        std::vector<float4> paf(2 * pr.P.size());
         for (size_t q = 0; q < pr.shell.size(); q++) {
             const double4 A = shell_xyz[pr.shell[q].x];
             for (int k = pr.prim0[q]; k < pr.prim0[q] + pr.nprim[q]; k++) {
                 const double4 P = pr.P[k];
-                pf[k] = make_float4((float)P.x, (float)P.y, (float)P.z, (float)P.w);
-                af[k] = make_float4((float)(P.x - A.x), (float)(P.y - A.y), (float)(P.z - A.z), (float)pr.X[k].x);
+                paf[2 * k] = make_float4((float)P.x, (float)P.y, (float)P.z, (float)P.w);
+                paf[2 * k + 1] = make_float4((float)(P.x - A.x), (float)(P.y - A.y), (float)(P.z - A.z), (float)pr.X[k].x);
             }
         }
-        CUDA_TRY(dev_upload(h, &h->dev.prim_Pf, pf.data(), pf.size()));
-        CUDA_TRY(dev_upload(h, &h->dev.prim_Af, af.data(), af.size()));
+        CUDA_TRY(dev_upload(h, &h->dev.prim_PAf, paf.data(), paf.size()));
     }
     const std::vector<double> &tab = rys_table_host();
     CUDA_TRY(dev_upload(h, &h->d_tab, tab.data(), tab.size()));
@@ -552,8 +551,7 @@ static DevBasis dev_basis(liberi_handle h) {
     d.pair_nprim = h->dev.pair_nprim;
     d.prim_P = h->dev.prim_P;
     d.prim_X = h->dev.prim_X;
-    d.prim_Pf = h->dev.prim_Pf;
-    d.prim_Af = h->dev.prim_Af;
+    d.prim_PAf = h->dev.prim_PAf;
     return d;
 }
 

@@ -63,6 +63,11 @@ __device__ __forceinline__ void ldg_v4f64(const double *p, double &a, double &b,
         : "=d"(a), "=d"(b), "=d"(c), "=d"(d)
         : "l"((unsigned long long)__cvta_generic_to_global(p)));
 }
+__device__ __forceinline__ double4 ldg_double4(const double4 *p) {
+    double4 v;
+    ldg_v4f64(reinterpret_cast<const double *>(p), v.x, v.y, v.z, v.w);
+    return v;
+}
 __device__ __forceinline__ void ldg_v8f32(const float *p, float4 &lo, float4 &hi) {
     asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
         : "=f"(lo.x), "=f"(lo.y), "=f"(lo.z), "=f"(lo.w), "=f"(hi.x), "=f"(hi.y), "=f"(hi.z), "=f"(hi.w)
@@ -316,11 +321,11 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
     int slot = 0;  // primitive quartet index within the shell quartet (root cache)
     if constexpr (std::is_same<R, double>::value) {
         for (int kq = q0; kq < q0 + nq; kq++) {
-            const double4 Qp = b.prim_P[kq];
+            const double4 Qp = ldg_double4(b.prim_P + kq);
             const double2 Qx = b.prim_X[kq];
             const double q = Qp.w, hq = Qx.y;
             for (int kp = p0; kp < p0 + np; kp++) {
-                const double4 Pp = b.prim_P[kp];
+                const double4 Pp = ldg_double4(b.prim_P + kp);
                 const double2 Px = b.prim_X[kp];
                 const double p = Pp.w, hp = Px.y;
                 const double pqx = Pp.x - Qp.x, pqy = Pp.y - Qp.y, pqz = Pp.z - Qp.z;
@@ -371,14 +376,15 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
         }
     } else {
         // FP32 tier: pair data, roots and recurrences in single precision
-        const float4 *__restrict__ Pf = b.prim_Pf;
-        const float4 *__restrict__ Af = b.prim_Af;
+        const float *__restrict__ PAf = reinterpret_cast<const float *>(b.prim_PAf);
         const float thrf = (float)thr;
         for (int kq = q0; kq < q0 + nq; kq++) {
-            const float4 Qp = __ldg(Pf + kq), Qa = __ldg(Af + kq);
+            float4 Qp, Qa;
+            ldg_v8f32(PAf + 8 * (size_t)kq, Qp, Qa);
             const float q = Qp.w, hq = __fdividef(0.5f, q);
             for (int kp = p0; kp < p0 + np; kp++) {
-                const float4 Pp = __ldg(Pf + kp), Pa = __ldg(Af + kp);
+                float4 Pp, Pa;
+                ldg_v8f32(PAf + 8 * (size_t)kp, Pp, Pa);
                 const float p = Pp.w, hp = __fdividef(0.5f, p);
                 const float pqx = Pp.x - Qp.x, pqy = Pp.y - Qp.y, pqz = Pp.z - Qp.z;
                 float u[NR], w[NR];
