@@ -106,6 +106,10 @@ int liberi_c_last_error(char *buf, int32_t len);
  *   "tile_mask"    (bit k set = class k may stage rows of F in a shared-memory
  *                   tile, where it fits; default none: F is updated with FP64
  *                   atomics in L2, faster on B200 for every class measured)
+ *   "overlap"      (1 = in mixed-precision builds the high-L classes with few
+ *                   quartets run on a second stream beside the others, forked
+ *                   from and joined back into the build's stream; default 1;
+ *                   off while "timing")
  *   "timing"       (1 = record per-class device times for liberi_c_get_stats)
  * Options set before liberi_c_setup apply to it; cut options may also be
  * changed between builds (the quartet plan is rebuilt on the next build). */
