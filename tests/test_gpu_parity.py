@@ -226,3 +226,28 @@ def test_calls_keep_the_callers_current_device():
     liberi.schwarz(b)
     F, _ = gpu_fock(b, M.density(b["num_bas"], nocc))
     assert torch.cuda.current_device() == before
+
+
+@pytest.mark.parametrize("mol", ["ethane", "random_9"])
+def test_launch_options_do_not_change_results(mol):
+    # F-row tile on/off, side-stream overlap on/off, shape variants: the same F
+    # (up to the order of FP64 atomics), FP64 and mixed
+    b, nocc = _molecule(mol)
+    D = M.density(b["num_bas"], nocc, seed=12)
+    Fo = oracle.fock_build(b, D, schwarz_cut=1e-10)
+    for prec in (0, 1):
+        base, _ = gpu_fock(b, D, schwarz_cut=1e-10, precision=prec, fp32_cut=1e-7)
+        variants = [dict(tile_mask=(1 << 21) - 1), dict(overlap=0)]
+        for opts in variants:
+            F, _ = gpu_fock(b, D, schwarz_cut=1e-10, precision=prec, fp32_cut=1e-7, **opts)
+            assert np.abs(F - base).max() <= 1e-11, (prec, opts)
+        h = liberi.liberi_create()
+        for k, v in (("schwarz_cut", 1e-10), ("precision", prec), ("fp32_cut", 1e-7)):
+            h.set_option(k, v)
+        liberi.setup_from_basis(h, b)
+        for k in range(21):
+            h.set_class_variant(k, prec, 1 + (k % 2))
+        F = liberi.fock(h, D)
+        liberi.liberi_destroy(h)
+        assert np.abs(F - base).max() <= 1e-11, (prec, "variants")
+        assert np.abs(base - Fo).max() <= (TOL_F if prec == 0 else 1e-5)
