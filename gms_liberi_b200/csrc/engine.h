@@ -36,7 +36,7 @@ __host__ __device__ constexpr int rys_herm_off(int n) {
 constexpr int RYS_TABLE_SIZE = rys_herm_off(MAXROOT + 1);
 // Single-precision tables for the FP32 tier: intervals of width 1/8 on
 // [0, RYS_TMAX), degree-3 power basis in x = 2(8T - k) - 1 (4 coefficients:
-// one float4 load per function; interpolation error below 5e-8 relative);
+// two functions per 256-bit load; interpolation error below 5e-8 relative);
 // then the large-T limit as above, in float.
 constexpr int RYSF_PER_UNIT = 8;
 constexpr int RYSF_NINT = 60 * RYSF_PER_UNIT;
