@@ -69,3 +69,19 @@ def test_oracle_screening_counts_monotone():
     _, c1 = oracle.fock_build(b, D, schwarz_cut=1e-12, return_counts=True)
     _, c2 = oracle.fock_build(b, D, schwarz_cut=1e-8, return_counts=True)
     assert (c2[:, 0] <= c1[:, 0]).all() and c2[:, 0].sum() < c1[:, 0].sum()
+
+
+def test_oracle_linear_and_symmetric_in_density():
+    """The two properties the full-size GPU tests rest on, pinned on the
+    oracle: F is linear in D, and sum_k D1_k F(D2)_k over the packed elements
+    is symmetric in (D1, D2)."""
+    b = M.ethane()
+    b["schwrz"] = oracle.schwarz(b)
+    n = b["num_bas"]
+    D1, D2 = M.density(n, 9, seed=1), M.density(n, 9, seed=2)
+    F1 = oracle.fock_build(b, D1, schwarz_cut=1e-10)
+    F2 = oracle.fock_build(b, D2, schwarz_cut=1e-10)
+    F12 = oracle.fock_build(b, D1 - 0.5 * D2, schwarz_cut=1e-10)
+    assert np.abs(F12 - (F1 - 0.5 * F2)).max() <= 1e-11 * np.abs(F1).max()
+    b12, b21 = float(np.dot(D1, F2)), float(np.dot(D2, F1))
+    assert abs(b12 - b21) <= 1e-11 * abs(b12)
