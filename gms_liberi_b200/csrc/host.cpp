@@ -232,8 +232,10 @@ static int validate_basis(const BasisHost &b) {
     }
     for (double x : b.schwrz)
         if (!(x >= 0.0)) return fail(LIBERI_E_ARG, "liberi_setup: negative or NaN Schwarz value");
-    if (b.num_bas > 46340)  // packed indices are 32-bit on the device
-        return fail(LIBERI_E_UNSUPPORTED, "liberi_setup: num_bas %d exceeds 46340", b.num_bas);
+    // the packed length n(n+1)/2 must fit the int32 matrix_size of
+    // liberi_fock_build; device packed indices are unsigned 32-bit
+    if (b.num_bas > 65535)
+        return fail(LIBERI_E_UNSUPPORTED, "liberi_setup: num_bas %d exceeds 65535", b.num_bas);
     return LIBERI_OK;
 }
 

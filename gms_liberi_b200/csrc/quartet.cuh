@@ -438,10 +438,12 @@ __device__ __forceinline__ double s3pow(int n3) {
 }
 __device__ __forceinline__ int cs3_rt(int l, int c) { return (l == 2 && c >= 3) ? 1 : 0; }
 
-// 0-based packed index of (i, j): max(i,j)(max+1)/2 + min, 32-bit (nbf < 65536)
-__device__ __forceinline__ int tri0(int i, int j) {
-    const int hi = i > j ? i : j, lo = i > j ? j : i;
-    return ((hi * (hi + 1)) >> 1) + lo;
+// 0-based packed index of (i, j): max(i,j)(max+1)/2 + min in unsigned 32-bit
+// arithmetic, exact for nbf <= 65535: the largest basis whose packed length
+// fits the int32 matrix_size of the interface (setup rejects larger ones)
+__device__ __forceinline__ unsigned tri0(unsigned i, unsigned j) {
+    const unsigned hi = i > j ? i : j, lo = i > j ? j : i;
+    return ((hi * (hi + 1u)) >> 1) + lo;
 }
 
 // target of a K or J update: the CTA's shared tile (rows of A and B of F) or,

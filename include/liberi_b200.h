@@ -36,7 +36,7 @@ enum {
     LIBERI_E_SIZE = -3,       /* matrix_size != num_bas(num_bas+1)/2 */
     LIBERI_E_DEVICE = -4,     /* CUDA error */
     LIBERI_E_NOMEM = -5,      /* device allocation failed or over limit */
-    LIBERI_E_UNSUPPORTED = -6 /* f shells (ang_mom 4) are not built */
+    LIBERI_E_UNSUPPORTED = -6 /* f shells (ang_mom 4) are not built; num_bas > 65535 */
 };
 
 /* ---- handle API: src/interface/liberi_interface.F90 --------------------- */

@@ -58,12 +58,16 @@ def test_options_validate():
         assert e.value.code == -1
 
 
-@pytest.mark.parametrize("bad", ["fshell", "rank", "sizes"])
+@pytest.mark.parametrize("bad", ["fshell", "rank", "sizes", "num_bas"])
 def test_setup_rejects_bad_input(bad):
     h = liberi.liberi_create()
     args = dict(nsh=1, natoms=1, num_bas=1, mxgtot=1, ang=[1], rank=0, nproc=1)
     if bad == "fshell":
         args["ang"] = [4]
+        code = -6
+    elif bad == "num_bas":
+        # n(n+1)/2 of 65536 functions exceeds the int32 matrix_size
+        args["num_bas"] = 65536
         code = -6
     elif bad == "rank":
         args["rank"] = 3
