@@ -88,9 +88,10 @@ struct DevBasis {
 // molecule, whose device data and class lists come from these views.
 struct MolView {
     DevBasis b;
-    const double *D;
+    const double *D;  // packed density (caller's buffer)
+    double *Dsq;      // this iteration's D as a full nbf x nbf matrix (batch-owned)
     double *F;
-    float *Df;  // FP32 tier of a mixed-precision batch: this iteration's D in float
+    float *Df;  // FP32 tier of a mixed-precision batch: the full D in float
     int nbf;
     int pad;
 };
@@ -167,7 +168,8 @@ struct DeviceBuffers {
     double2 *prim_X = nullptr;
     float4 *prim_PAf = nullptr;
     double *D = nullptr, *F = nullptr;
-    float *Df = nullptr;  // FP32 tier: single-precision copy of the build's D
+    double *Dsq = nullptr;  // the build's D as a full n x n matrix (class kernels read it)
+    float *Df = nullptr;    // FP32 tier: the same in single precision
     long long *scratch_total = nullptr;  // device counters (mixed split)
     size_t bytes = 0;
 };
@@ -196,15 +198,17 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
                                const MolView *d_mols, const ClassView *d_cviews, bool swapped, int precision,
                                const int *ntasks_dev);
 cudaError_t launch_zero_fock(const MolView *d_mols, int nmol, long long max_ntri, cudaStream_t stream);
-// mixed-precision batch: per molecule max|D| (as ordered bits) and the float copy of D
-cudaError_t launch_batch_prep(const MolView *d_mols, int nmol, long long max_ntri, unsigned long long *maxd,
+// batch: every molecule's D as a full matrix (Dsq), and for a mixed-precision
+// batch its float copy (Df) and max|D| (as ordered bits, maxd non-null)
+cudaError_t launch_batch_prep(const MolView *d_mols, int nmol, long long max_nsq, unsigned long long *maxd,
                               cudaStream_t stream);
 // mixed-precision batch: FP64/FP32 task lists of one class over every molecule's items
 // (item.w = molecule), as split_tasks_kernel does for one molecule
 cudaError_t launch_split_batch(int nitems, const int4 *items, const ClassView *d_cviews,
                                const unsigned long long *maxd, double fp32_cut, int chunk, int4 *tasks64,
                                int4 *tasks32, int *counts, cudaStream_t stream);
-cudaError_t launch_to_float(const double *src, float *dst, long long n, cudaStream_t st);
+// full n x n copy of a packed density, and its float copy when sqf is non-null
+cudaError_t launch_unpack(const double *packed, int n, double *sq, float *sqf, cudaStream_t st);
 cudaError_t launch_maxabs(const double *x, long long n, unsigned long long *out,
                           cudaStream_t stream);
 cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_x, const double *ket_x,

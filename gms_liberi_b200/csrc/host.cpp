@@ -465,7 +465,8 @@ static size_t basis_device_bytes(const BasisHost &b, const PairsHost &pr) {
     const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
     return sizeof(double4) * b.nsh + sizeof(int) * b.nsh + (sizeof(int2) + 2 * sizeof(int)) * npair +
            (sizeof(double4) + sizeof(double2) + 2 * sizeof(float4)) * nprim + sizeof(double) * RYS_TABLE_SIZE +
-           sizeof(float) * RYSF_TABLE_SIZE + (2 * sizeof(double) + sizeof(float)) * (ntri > 0 ? ntri : 1) +
+           sizeof(float) * RYSF_TABLE_SIZE + 2 * sizeof(double) * (ntri > 0 ? ntri : 1) +
+           (sizeof(double) + sizeof(float)) * ((size_t)b.num_bas * b.num_bas > 0 ? (size_t)b.num_bas * b.num_bas : 1) +
            sizeof(unsigned long long);
 }
 
@@ -549,7 +550,9 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
     const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
     CUDA_TRY(dev_alloc(h, &h->dev.D, ntri));
     CUDA_TRY(dev_alloc(h, &h->dev.F, ntri));
-    CUDA_TRY(dev_alloc(h, &h->dev.Df, ntri));
+    const size_t nsq = (size_t)b.num_bas * b.num_bas;
+    CUDA_TRY(dev_alloc(h, &h->dev.Dsq, nsq));
+    CUDA_TRY(dev_alloc(h, &h->dev.Df, nsq));
     CUDA_TRY(dev_alloc(h, &h->d_maxd, 1));
     return LIBERI_OK;
 }
@@ -616,7 +619,7 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     ctx.basis = dev_basis(h);
     ctx.rys_tab = h->d_tab;
     ctx.rys_tabf = h->d_tabf;
-    ctx.D = dD;
+    ctx.D = h->dev.Dsq;
     ctx.F = dF;
     ctx.schwarz_cut = h->schwarz_cut;
     ctx.eri_cut = h->eri_cut;
@@ -624,10 +627,9 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     ctx.num_sms = h->num_sms;
     const bool mixed = h->precision == 1;
     ctx.Df = h->dev.Df;
-    if (mixed) {
-        CUDA_TRY(launch_maxabs(dD, ntri, h->d_maxd, st));
-        CUDA_TRY(launch_to_float(dD, h->dev.Df, ntri, st));
-    }
+    // the class kernels read D as a full matrix (and in float for the FP32 tier)
+    CUDA_TRY(launch_unpack(dD, b.num_bas, h->dev.Dsq, mixed ? h->dev.Df : nullptr, st));
+    if (mixed) CUDA_TRY(launch_maxabs(dD, ntri, h->d_maxd, st));
     for (int k = 0; k < NKERN; k++) h->ev_recorded[k] = false;
     // mixed precision: the high-L classes with few quartets per row pair (a
     // latency tail) start first on the side stream and overlap the others
@@ -753,8 +755,9 @@ struct liberi_batch_s {
     int4 *d_t64[NKERN] = {}, *d_t32[NKERN] = {};
     int *d_counts[NKERN] = {};
     unsigned long long *d_maxd = nullptr;
-    float *d_Df = nullptr;
-    std::vector<size_t> df_off;
+    double *d_Dsq = nullptr;      // every molecule's D as a full matrix (offsets sq_off)
+    float *d_Df = nullptr;        // mixed: the same in float
+    std::vector<size_t> sq_off;
     bool bound = false;
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -804,7 +807,8 @@ static int batch_enqueue(liberi_batch b, cudaStream_t st, uint32_t mask) {
     ctx.stream = st;
     ctx.num_sms = h0->num_sms;
     const bool mixed = b->precision == 1;
-    if (mixed) CUDA_TRY(launch_batch_prep(b->d_mols, (int)b->hs.size(), b->ntri_max, b->d_maxd, st));
+    CUDA_TRY(launch_batch_prep(b->d_mols, (int)b->hs.size(), (long long)b->nbf_max * b->nbf_max,
+                               mixed ? b->d_maxd : nullptr, st));
     for (int k = 0; k < NKERN; k++) {
         if (!((mask >> k) & 1u) || b->ntasks[k] == 0) continue;
         if (!mixed) {
@@ -1081,19 +1085,27 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
     }
     b->precision = handles[0]->precision;
     b->fp32_cut = handles[0]->fp32_cut;
+    {  // every molecule's D as a full matrix, made per iteration from its packed D
+        size_t sqtot = 0;
+        for (int m = 0; m < n; m++) {
+            b->sq_off.push_back(sqtot);
+            const size_t nb = (size_t)b->hs[m]->basis.num_bas;
+            sqtot += nb * nb;
+        }
+        if (cudaMalloc((void **)&b->d_Dsq, std::max<size_t>(sqtot, 1) * sizeof(double)) != cudaSuccess)
+            return die(fail(LIBERI_E_NOMEM, "liberi_batch_create: out of device memory"));
+        b->allocs.push_back(b->d_Dsq);
+        if (b->precision == 1) {
+            if (cudaMalloc((void **)&b->d_Df, std::max<size_t>(sqtot, 1) * sizeof(float)) != cudaSuccess)
+                return die(fail(LIBERI_E_NOMEM, "liberi_batch_create: out of device memory"));
+            b->allocs.push_back(b->d_Df);
+        }
+    }
     if (b->precision == 1) {
         // every molecule's items of a class in one list; task capacity for the
         // smallest kets-per-task the tuner may choose
-        size_t dftot = 0;
-        for (int m = 0; m < n; m++) {
-            b->df_off.push_back(dftot);
-            const size_t nb = (size_t)b->hs[m]->basis.num_bas;
-            dftot += nb * (nb + 1) / 2;
-        }
-        if (cudaMalloc((void **)&b->d_Df, std::max<size_t>(dftot, 1) * sizeof(float)) != cudaSuccess ||
-            cudaMalloc((void **)&b->d_maxd, n * sizeof(unsigned long long)) != cudaSuccess)
+        if (cudaMalloc((void **)&b->d_maxd, n * sizeof(unsigned long long)) != cudaSuccess)
             return die(fail(LIBERI_E_NOMEM, "liberi_batch_create: out of device memory"));
-        b->allocs.push_back(b->d_Df);
         b->allocs.push_back(b->d_maxd);
         for (int k = 0; k < NKERN; k++) {
             std::vector<int4> items;
@@ -1130,8 +1142,9 @@ int liberi_c_batch_bind(liberi_batch b, const double *const *d_density, double *
         if (!d_density[m] || !d_fock[m]) return fail(LIBERI_E_ARG, "liberi_batch_bind: null buffer %zu", m);
         mv[m].b = dev_basis(b->hs[m]);
         mv[m].D = d_density[m];
+        mv[m].Dsq = b->d_Dsq + b->sq_off[m];
         mv[m].F = d_fock[m];
-        mv[m].Df = b->precision == 1 ? b->d_Df + b->df_off[m] : nullptr;
+        mv[m].Df = b->precision == 1 ? b->d_Df + b->sq_off[m] : nullptr;
         mv[m].nbf = b->hs[m]->basis.num_bas;
         mv[m].pad = 0;
     }

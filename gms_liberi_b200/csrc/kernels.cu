@@ -148,17 +148,24 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     return cudaErrorInvalidValue;
 }
 
-__global__ void to_float_kernel(const double *__restrict__ src, float *__restrict__ dst, long long n) {
+__global__ void unpack_kernel(const double *__restrict__ packed, unsigned n, double *__restrict__ sq,
+                              float *__restrict__ sqf) {
+    const long long total = (long long)n * n;  // n <= 65535: an index fits unsigned 32-bit
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = (float)src[i];
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+        const unsigned i = (unsigned)g, r = i / n, c = i - r * n;
+        const double d = packed[tri0(r, c)];
+        sq[i] = d;
+        if (sqf) sqf[i] = (float)d;
+    }
 }
 
-cudaError_t launch_to_float(const double *src, float *dst, long long n, cudaStream_t st) {
+cudaError_t launch_unpack(const double *packed, int n, double *sq, float *sqf, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const int threads = 256;
-    const long long want = (n + threads - 1) / threads;
+    const long long want = ((long long)n * n + threads - 1) / threads;
     const int blocks = (int)(want < 148LL * 8 ? want : 148LL * 8);
-    to_float_kernel<<<blocks, threads, 0, st>>>(src, dst, n);
+    unpack_kernel<<<blocks, threads, 0, st>>>(packed, (unsigned)n, sq, sqf);
     return cudaGetLastError();
 }
 
@@ -174,29 +181,33 @@ __global__ void zero_fock_kernel(const MolView *mols, int nmol, long long max_nt
 }
 
 // per molecule: max|D| (non-negative doubles order as their bits) and D in float
-__global__ void batch_prep_kernel(const MolView *mols, int nmol, long long max_ntri, unsigned long long *maxd) {
+__global__ void batch_prep_kernel(const MolView *mols, int nmol, long long max_nsq, unsigned long long *maxd) {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < (long long)nmol * max_ntri;
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < (long long)nmol * max_nsq;
          g += stride) {
-        const int m = (int)(g / max_ntri);
-        const long long i = g - (long long)m * max_ntri;
-        const long long n = mols[m].nbf;
-        if (i >= n * (n + 1) / 2) continue;
-        const double d = mols[m].D[i];
-        mols[m].Df[i] = (float)d;
-        atomicMax(maxd + m, (unsigned long long)__double_as_longlong(fabs(d)));
+        const int m = (int)(g / max_nsq);
+        const unsigned i = (unsigned)(g - (long long)m * max_nsq);
+        const unsigned n = (unsigned)mols[m].nbf;
+        if (i >= n * n) continue;
+        const unsigned r = i / n, c = i - r * n;
+        const double d = mols[m].D[tri0(r, c)];
+        mols[m].Dsq[i] = d;
+        if (mols[m].Df) mols[m].Df[i] = (float)d;
+        if (maxd && c <= r) atomicMax(maxd + m, (unsigned long long)__double_as_longlong(fabs(d)));
     }
 }
 
-cudaError_t launch_batch_prep(const MolView *d_mols, int nmol, long long max_ntri, unsigned long long *maxd,
+cudaError_t launch_batch_prep(const MolView *d_mols, int nmol, long long max_nsq, unsigned long long *maxd,
                               cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(maxd, 0, (size_t)nmol * sizeof(unsigned long long), st);
-    if (e != cudaSuccess) return e;
-    const long long total = (long long)nmol * max_ntri;
+    if (maxd) {
+        cudaError_t e = cudaMemsetAsync(maxd, 0, (size_t)nmol * sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
+    }
+    const long long total = (long long)nmol * max_nsq;
     const int threads = 256;
     const long long want = (total + threads - 1) / threads;
     const int blocks = (int)(want < 148LL * 16 ? (want > 0 ? want : 1) : 148LL * 16);
-    batch_prep_kernel<<<blocks, threads, 0, st>>>(d_mols, nmol, max_ntri, maxd);
+    batch_prep_kernel<<<blocks, threads, 0, st>>>(d_mols, nmol, max_nsq, maxd);
     return cudaGetLastError();
 }
 

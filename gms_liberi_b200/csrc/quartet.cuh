@@ -467,12 +467,17 @@ struct QuartetCtx {
     int bfA, bfB, bfC, bfD;
     bool iandj, kandl, same;
     T cut;
-    const T *__restrict__ Dm;
+    const T *__restrict__ Dm;  // the build's density as a full n x n matrix
+    unsigned ld;               // n
 };
 
+// D(i, j) from the full matrix: the row is the CTA's bra shell (A or B) or
+// the ket's first shell, the column runs over a shell's components, so one
+// shell's components share a sector and every lane of a CTA reads the same
+// rows A and B (n <= 65535: i * n + j fits unsigned 32-bit)
 template <typename T>
-__device__ __forceinline__ T dget(const T *__restrict__ Dm, int i, int j) {
-    return __ldg(Dm + tri0(i, j));
+__device__ __forceinline__ T dget(const T *__restrict__ Dm, unsigned ld, unsigned i, unsigned j) {
+    return __ldg(Dm + i * ld + j);
 }
 
 // Per-class compile-time shape: A components per pass (bounds the contracted
@@ -729,11 +734,11 @@ __device__ __forceinline__ void digest_row_distinct(const R (&a)[ncart(LB)][ncar
     const R sa = R(s3pow(cs3_rt(LA, ia)));
     R dAB[NB], dAC[NC], dAD[ND];
 #pragma unroll
-    for (int ib = 0; ib < NB; ib++) dAB[ib] = R(4) * dget(Dm, mu, qc.bfB + ib);
+    for (int ib = 0; ib < NB; ib++) dAB[ib] = R(4) * dget(Dm, qc.ld, mu, qc.bfB + ib);
 #pragma unroll
-    for (int ic = 0; ic < NC; ic++) dAC[ic] = dget(Dm, mu, qc.bfC + ic);
+    for (int ic = 0; ic < NC; ic++) dAC[ic] = dget(Dm, qc.ld, mu, qc.bfC + ic);
 #pragma unroll
-    for (int id = 0; id < ND; id++) dAD[id] = dget(Dm, mu, qc.bfD + id);
+    for (int id = 0; id < ND; id++) dAD[id] = dget(Dm, qc.ld, mu, qc.bfD + id);
     R kac[NC], kad[ND];
 #pragma unroll
     for (int ib = 0; ib < NB; ib++) jab[ib] = R(0);
@@ -784,7 +789,7 @@ __device__ __forceinline__ void digest_row_general(const R (&a)[ncart(LB)][ncart
         jab[ib] = R(0);
         if (LA == LB && qc.iandj && ib > ia) continue;
         const int nu = qc.bfB + ib;
-        const R dmn = dget(qc.Dm, mu, nu);
+        const R dmn = dget(qc.Dm, qc.ld, mu, nu);
 #pragma unroll
         for (int ic = 0; ic < NC; ic++) {
             const int la = qc.bfC + ic;
@@ -803,12 +808,12 @@ __device__ __forceinline__ void digest_row_general(const R (&a)[ncart(LB)][ncart
                 if (mu == nu) v *= R(0.5);
                 if (la == si) v *= R(0.5);
                 if ((mu == la && nu == si) || (mu == si && nu == la)) v *= R(0.5);
-                jab[ib] += R(4) * v * dget(qc.Dm, la, si);
+                jab[ib] += R(4) * v * dget(qc.Dm, qc.ld, la, si);
                 kb.cd(ic, id) += R(4) * v * dmn;
-                kac[ic] += v * dget(qc.Dm, nu, si);
-                kad[id] += v * dget(qc.Dm, nu, la);
-                kb.bc(ib, ic) += v * dget(qc.Dm, mu, si);
-                kb.bd(ib, id) += v * dget(qc.Dm, mu, la);
+                kac[ic] += v * dget(qc.Dm, qc.ld, nu, si);
+                kad[id] += v * dget(qc.Dm, qc.ld, nu, la);
+                kb.bc(ib, ic) += v * dget(qc.Dm, qc.ld, mu, si);
+                kb.bd(ib, id) += v * dget(qc.Dm, qc.ld, mu, la);
             }
         }
     }
@@ -854,13 +859,13 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
 #pragma unroll
             for (int ic = 0; ic < NC; ic++)
 #pragma unroll
-                for (int id = 0; id < ND; id++) dCD[ic][id] = dget(qc.Dm, qc.bfC + ic, qc.bfD + id);
+                for (int id = 0; id < ND; id++) dCD[ic][id] = dget(qc.Dm, qc.ld, qc.bfC + ic, qc.bfD + id);
 #pragma unroll
             for (int ib = 0; ib < NB; ib++) {
 #pragma unroll
-                for (int id = 0; id < ND; id++) dBD[ib][id] = dget(qc.Dm, qc.bfB + ib, qc.bfD + id);
+                for (int id = 0; id < ND; id++) dBD[ib][id] = dget(qc.Dm, qc.ld, qc.bfB + ib, qc.bfD + id);
 #pragma unroll
-                for (int ic = 0; ic < NC; ic++) dBC[ib][ic] = dget(qc.Dm, qc.bfB + ib, qc.bfC + ic);
+                for (int ic = 0; ic < NC; ic++) dBC[ib][ic] = dget(qc.Dm, qc.ld, qc.bfB + ib, qc.bfC + ic);
             }
         }
 #pragma unroll
@@ -908,8 +913,8 @@ struct ClassArgs {
     DevBasis b;
     const double *tab;
     const float *tabf;
-    const double *Dm;
-    const float *Dmf;        // FP32 tier: single-precision copy of D (this build's)
+    const double *Dm;        // this build's D as a full n x n matrix
+    const float *Dmf;        // FP32 tier: the same in single precision
     double *F;
     double cut;
     double thr;
@@ -936,7 +941,7 @@ __device__ __forceinline__ const DevBasis &mol_basis(const ClassArgs &a, int w) 
 template <bool BATCH, typename T>
 __device__ __forceinline__ const T *mol_D(const ClassArgs &a, int w) {
     if constexpr (std::is_same<T, float>::value) return BATCH ? a.mols[w].Df : a.Dmf;  // FP32 tier
-    else if constexpr (BATCH) return a.mols[w].D;
+    else if constexpr (BATCH) return a.mols[w].Dsq;
     else return a.Dm;
 }
 template <bool BATCH>
@@ -1011,7 +1016,7 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
         qc.bfA = bfA; qc.bfB = bfB;
         qc.bfC = bas.shell_bf0[scd.x]; qc.bfD = bas.shell_bf0[scd.y];
         qc.iandj = sab.x == sab.y; qc.kandl = scd.x == scd.y; qc.same = P == Qd;
-        qc.cut = R(a.cut); qc.Dm = LIBERI_D;
+        qc.cut = R(a.cut); qc.Dm = LIBERI_D; qc.ld = (unsigned)LIBERI_NBF;
         constexpr bool SM = PassShape<LA, LB, LC, LD, R, V>::NPASS > 1;
         KBuf<NB, NC, ND, SM, R> kb;
         kb.s = slots + threadIdx.x;

@@ -119,8 +119,9 @@ int liberi_c_get_option(liberi_handle handle, const char *name, double *value);
 /* Fock build on device-resident packed buffers (no host copies), enqueued on
  * `stream` (a cudaStream_t, NULL = the handle's own stream); does not
  * synchronise.  Used for device-resident benchmarking and graph capture.
- * Builds of one handle share its mixed-precision task lists: enqueue them on
- * one stream (or order them), as a handle is not thread-safe in the reference. */
+ * Builds of one handle share its device scratch (the full copy of D the
+ * kernels read, the mixed-precision task lists): enqueue them on one stream
+ * (or order them), as a handle is not thread-safe in the reference. */
 int liberi_c_fock_build_device(liberi_handle handle, const double *d_density, double *d_fock,
                                void *stream);
 
