@@ -98,10 +98,18 @@ struct MolView {
 struct ClassView {
     const int *bra_ids, *ket_ids;
     const double *bra_x, *ket_x;  // Schwarz values of the lists (mixed-precision split)
+    const double4 *ket_rec;       // ket records of the list (two double4 per position)
 };
+
+// Per ket position of a class plan, what a quartet needs of its ket pair (C,D)
+// in two 256-bit loads that are contiguous across the lanes of a warp:
+//   [0] = (C-D x, y, z, C.x), [1] = (C.y, C.z, bits of first functions
+//   bf0(C) | bf0(D) << 32, bits of first primitive pair | kept count << 32).
+constexpr int KET_REC = 2;
 
 struct DevPlan {
     const int *bra_ids, *ket_ids;    // global pair ids, sorted by xint desc
+    const double4 *ket_rec;          // ket records (KET_REC double4 per ket position)
     const int *bra_orig, *ket_orig;  // positions in the reference's compacted lists
     const int4 *tasks;
     const int *ntasks_dev;           // task count on the device (per-build lists) or null
@@ -133,6 +141,7 @@ struct PlanHost {
     // device copies
     int *d_bra = nullptr, *d_ket = nullptr, *d_bra_orig = nullptr, *d_ket_orig = nullptr;
     double *d_bra_x = nullptr, *d_ket_x = nullptr;
+    double4 *d_ket_rec = nullptr;
     int4 *d_items = nullptr;
     int4 *d_tasks = nullptr;
     // mixed precision: per-build task lists

@@ -431,10 +431,37 @@ static void make_tasks(const PlanHost &ph, int chunk, int mol, std::vector<int4>
         for (int k0 = 0; k0 < it.z; k0 += chunk) out.push_back(make_int4(it.x, it.y + k0, std::min(chunk, it.z - k0), mol));
 }
 
+// Ket records of a plan (layout beside KET_REC): C - D, C, the first basis
+// functions of C and D and the ket pair's primitive range, per ket position.
+static void build_ket_records(const BasisHost &b, const PairsHost &pr, const std::vector<int> &ket_ids,
+                              std::vector<double4> &rec) {
+    auto bits = [](unsigned lo, unsigned hi) {
+        const unsigned long long v = (unsigned long long)lo | ((unsigned long long)hi << 32);
+        double d;
+        std::memcpy(&d, &v, sizeof d);
+        return d;
+    };
+    rec.resize(KET_REC * ket_ids.size());
+    for (size_t j = 0; j < ket_ids.size(); j++) {
+        const int Q = ket_ids[j];
+        const int C = pr.shell[Q].x, D = pr.shell[Q].y;
+        const double *xc = &b.coords[3 * (size_t)(b.atom_num[C] - 1)];
+        const double *xd = &b.coords[3 * (size_t)(b.atom_num[D] - 1)];
+        rec[KET_REC * j] = make_double4(xc[0] - xd[0], xc[1] - xd[1], xc[2] - xd[2], xc[0]);
+        rec[KET_REC * j + 1] = make_double4(xc[1], xc[2], bits(b.atom_loc[C] - 1, b.atom_loc[D] - 1),
+                                            bits(pr.prim0[Q], pr.nprim[Q]));
+    }
+}
+
 static int upload_plans(liberi_handle h) {
     for (int k = 0; k < NKERN; k++) {
         PlanHost &ph = h->plan[k];
         if (ph.nbra == 0) continue;
+        {
+            std::vector<double4> rec;
+            build_ket_records(h->basis, h->pairs, ph.ket_ids, rec);
+            CUDA_TRY(dev_upload(h, &ph.d_ket_rec, rec.data(), rec.size()));
+        }
         CUDA_TRY(dev_upload(h, &ph.d_bra, ph.bra_ids.data(), ph.bra_ids.size()));
         CUDA_TRY(dev_upload(h, &ph.d_ket, ph.ket_ids.data(), ph.ket_ids.size()));
         CUDA_TRY(dev_upload(h, &ph.d_bra_orig, ph.bra_orig.data(), ph.bra_orig.size()));
@@ -455,8 +482,8 @@ static size_t plan_device_bytes(const PlanHost &ph) {
     if (ph.nbra == 0) return 0;
     const size_t nb = ph.bra_ids.size(), nk = ph.ket_ids.size();
     const size_t cap = ph.task_cap > 0 ? (size_t)ph.task_cap : 1;
-    return 4 * (nb + nk) * 2 + 8 * (nb + nk) + sizeof(int4) * (ph.items.size() + ph.tasks.size()) +
-           2 * sizeof(int4) * cap + 4 * sizeof(int);
+    return 4 * (nb + nk) * 2 + 8 * (nb + nk) + sizeof(double4) * KET_REC * nk +
+           sizeof(int4) * (ph.items.size() + ph.tasks.size()) + 2 * sizeof(int4) * cap + 4 * sizeof(int);
 }
 
 // Device bytes that upload_basis allocates.
@@ -675,6 +702,7 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
         DevPlan dp;
         dp.bra_ids = ph.d_bra;
         dp.ket_ids = ph.d_ket;
+        dp.ket_rec = ph.d_ket_rec;
         dp.bra_orig = ph.d_bra_orig;
         dp.ket_orig = ph.d_ket_orig;
         dp.swapped = kd.swap;
@@ -1074,7 +1102,7 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
         std::vector<ClassView> cv(n);
         for (int m = 0; m < n; m++)
             cv[m] = ClassView{b->hs[m]->plan[k].d_bra, b->hs[m]->plan[k].d_ket, b->hs[m]->plan[k].d_bra_x,
-                              b->hs[m]->plan[k].d_ket_x};
+                              b->hs[m]->plan[k].d_ket_x, b->hs[m]->plan[k].d_ket_rec};
         if (cudaMalloc((void **)&b->d_cv[k], n * sizeof(ClassView)) != cudaSuccess)
             return die(fail(LIBERI_E_NOMEM, "liberi_batch_create: out of device memory"));
         b->allocs.push_back(b->d_cv[k]);

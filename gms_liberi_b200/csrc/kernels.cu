@@ -102,6 +102,7 @@ cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const
     a.tile_rows = tile_rows;
     a.bra_ids = plan.bra_ids;
     a.ket_ids = plan.ket_ids;
+    a.ket_rec = plan.ket_rec;
     a.bra_orig = plan.bra_orig;
     a.ket_orig = plan.ket_orig;
     a.swapped = plan.swapped ? 1 : 0;
@@ -137,6 +138,7 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     // for single-molecule builds by default
     a.tile_rows = 0;
     a.bra_ids = a.ket_ids = a.bra_orig = a.ket_orig = nullptr;
+    a.ket_rec = nullptr;
     a.swapped = swapped ? 1 : 0;
     a.rs = RankSplit{0, 1, 0, 0, 0, 0, 0, 0};
     a.mols = d_mols;

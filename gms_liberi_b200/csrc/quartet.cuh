@@ -925,6 +925,7 @@ struct ClassArgs {
     int nbf;
     int tile_rows;           // 1: stage rows of A and B of F in shared memory
     const int *bra_ids, *ket_ids, *bra_orig, *ket_orig;
+    const double4 *ket_rec;  // ket records (KET_REC per ket position)
     int swapped;             // plan bra list is the reference's ket list
     RankSplit rs;
     const MolView *mols;     // batched launch: per-molecule data (task.w), else null
@@ -957,8 +958,8 @@ __device__ __forceinline__ const int *mol_bra(const ClassArgs &a, int w) {
     if constexpr (BATCH) return a.cviews[w].bra_ids; else return a.bra_ids;
 }
 template <bool BATCH>
-__device__ __forceinline__ const int *mol_ket(const ClassArgs &a, int w) {
-    if constexpr (BATCH) return a.cviews[w].ket_ids; else return a.ket_ids;
+__device__ __forceinline__ const double4 *mol_ketrec(const ClassArgs &a, int w) {
+    if constexpr (BATCH) return a.cviews[w].ket_rec; else return a.ket_rec;
 }
 
 // One CTA task: row pair t.x against kets t.y .. t.y+t.z-1 of one molecule.
@@ -1008,21 +1009,24 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
             else it = bo * a.rs.nket_ref + ko + 1;
             act = rank_owns(a.rs, it);
         }
-        const int Qd = __ldg(mol_ket<BATCH>(a, t.w) + j);
-        const int2 scd = bas.pair_shell[Qd];
-        const double4 C = bas.shell_xyz[scd.x], D = bas.shell_xyz[scd.y];
-        const R cdx = R(C.x - D.x), cdy = R(C.y - D.y), cdz = R(C.z - D.z);
+        const double4 *krec = mol_ketrec<BATCH>(a, t.w) + KET_REC * j;
+        const double4 r0 = ldg_double4(krec), r1 = ldg_double4(krec + 1);
+        const double4 C = make_double4(r0.w, r1.x, r1.y, 0.0);
+        const R cdx = R(r0.x), cdy = R(r0.y), cdz = R(r0.z);
+        const unsigned long long kbf = (unsigned long long)__double_as_longlong(r1.z);
+        const unsigned long long kpr = (unsigned long long)__double_as_longlong(r1.w);
         QuartetCtx<R> qc;
         qc.bfA = bfA; qc.bfB = bfB;
-        qc.bfC = bas.shell_bf0[scd.x]; qc.bfD = bas.shell_bf0[scd.y];
-        qc.iandj = sab.x == sab.y; qc.kandl = scd.x == scd.y; qc.same = P == Qd;
+        qc.bfC = (int)(unsigned)kbf; qc.bfD = (int)(unsigned)(kbf >> 32);
+        // shells have distinct first functions: same shells <=> same first functions
+        qc.iandj = sab.x == sab.y; qc.kandl = qc.bfC == qc.bfD; qc.same = bfA == qc.bfC && bfB == qc.bfD;
         qc.cut = R(a.cut); qc.Dm = LIBERI_D; qc.ld = (unsigned)LIBERI_NBF;
         constexpr bool SM = PassShape<LA, LB, LC, LD, R, V>::NPASS > 1;
         KBuf<NB, NC, ND, SM, R> kb;
         kb.s = slots + threadIdx.x;
 #pragma unroll
         for (int i = 0; i < KBuf<NB, NC, ND, SM, R>::N; i++) kb.at(i) = R(0);
-        run_passes<LA, LB, LC, LD, R, V>(bas, p0, np, bas.pair_prim0[Qd], act ? bas.pair_nprim[Qd] : 0, A, C, abx, aby,
+        run_passes<LA, LB, LC, LD, R, V>(bas, p0, np, (int)(unsigned)kpr, act ? (int)(unsigned)(kpr >> 32) : 0, A, C, abx, aby,
                                       abz, cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
