@@ -581,7 +581,7 @@ constexpr int tuned_minb_f32(int key) {
         case 0: return 8;
         case 1000: return 8;
         case 1010: return 8;
-        case 1100: return 6;
+        case 1100: return 8;
         case 1110: return 5;
         case 1111: return 3;
         case 1120: return 3;
@@ -590,7 +590,7 @@ constexpr int tuned_minb_f32(int key) {
         case 2020: return 4;
         case 2100: return 5;
         case 2110: return 3;
-        case 2111: return 2;
+        case 2111: return 3;
         case 2120: return 3;
         case 2121: return 2;
         case 2200: return 3;
@@ -637,13 +637,13 @@ constexpr int alt_nmu(int key, bool f32, int v) {
 constexpr int alt_minb(int key, bool f32, int v) {
     if (f32) {
         switch (key * 10 + v) {
-            case 11001: return 8;
+            case 11001: return 6;
             case 11101: return 6;
             case 11102: return 8;
             case 11111: return 3;
             case 11112: return 4;
             case 21101: return 4;
-            case 21111: return 3;
+            case 21111: return 2;
             case 21112: return 4;
             case 21211: return 3;
             default: return 0;
