@@ -155,6 +155,56 @@ struct liberi_handle_s {
     int num_sms = 148;
     liberi_stats stats;
     std::vector<void *> allocs;
+    // one allocation each for the basis data and for the class plans, carved
+    // into the handle's buffers (arena: the one being carved, or null)
+    struct Arena {
+        char *base = nullptr;
+        size_t size = 0, used = 0;
+    } arena_basis, arena_plans, *arena = nullptr;
+};
+
+// Handle buffers are carved from one stream-ordered allocation per group
+// (basis data, class plans) at DEV_ALIGN-byte offsets: a few hundred small
+// cudaMallocAsync calls per handle made the allocator's bookkeeping, and so
+// every further setup, grow with the number of live handles.
+constexpr size_t DEV_ALIGN = 256;
+static size_t dev_round(size_t bytes) { return (bytes + DEV_ALIGN - 1) & ~(DEV_ALIGN - 1); }
+// bytes one dev_upload of n elements takes (none for n == 0), and one dev_alloc
+static size_t up_bytes(size_t n, size_t elem) { return n ? dev_round(n * elem) : 0; }
+static size_t al_bytes(size_t n, size_t elem) { return dev_round((n ? n : 1) * elem); }
+
+static cudaError_t dev_get(liberi_handle h, size_t bytes, void **p) {
+    bytes = dev_round(bytes);
+    if (h->arena) {
+        if (h->arena->used + bytes > h->arena->size) return cudaErrorMemoryAllocation;  // accounting mismatch
+        *p = h->arena->base + h->arena->used;
+        h->arena->used += bytes;
+    } else {
+        cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
+        if (e != cudaSuccess) return e;
+        h->allocs.push_back(*p);
+    }
+    h->dev.bytes += bytes;
+    return cudaSuccess;
+}
+
+// opens an arena of exactly `bytes` for the uploads of one group
+static cudaError_t arena_open(liberi_handle h, liberi_handle_s::Arena &a, size_t bytes) {
+    a = liberi_handle_s::Arena();
+    if (bytes) {
+        void *p = nullptr;
+        cudaError_t e = cudaMallocAsync(&p, bytes, h->stream);
+        if (e != cudaSuccess) return e;
+        h->allocs.push_back(p);
+        a.base = static_cast<char *>(p);
+        a.size = bytes;
+    }
+    h->arena = &a;
+    return cudaSuccess;
+}
+struct ArenaScope {  // stops carving when the group's uploads end, on every path
+    liberi_handle h;
+    ~ArenaScope() { h->arena = nullptr; }
 };
 
 // Handle memory is stream-ordered on the handle's stream (cudaMallocAsync /
@@ -168,10 +218,8 @@ template <typename T>
 static cudaError_t dev_upload(liberi_handle h, T **dst, const T *src, size_t n) {
     *dst = nullptr;
     if (n == 0) return cudaSuccess;
-    cudaError_t e = cudaMallocAsync((void **)dst, n * sizeof(T), h->stream);
+    cudaError_t e = dev_get(h, n * sizeof(T), (void **)dst);
     if (e != cudaSuccess) return e;
-    h->allocs.push_back(*dst);
-    h->dev.bytes += n * sizeof(T);
     return cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, h->stream);
 }
 
@@ -179,21 +227,22 @@ template <typename T>
 static cudaError_t dev_alloc(liberi_handle h, T **dst, size_t n) {
     *dst = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = cudaMallocAsync((void **)dst, n * sizeof(T), h->stream);
-    if (e != cudaSuccess) return e;
-    h->allocs.push_back(*dst);
-    h->dev.bytes += n * sizeof(T);
-    return cudaSuccess;
+    return dev_get(h, n * sizeof(T), (void **)dst);
 }
 
+// frees an allocation of its own (not a piece carved from an arena)
 static void dev_release(liberi_handle h, void *p) {
+    auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
+    if (it == h->allocs.end()) return;
     cudaFreeAsync(p, h->stream);
-    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), p), h->allocs.end());
+    h->allocs.erase(it);
 }
 
 static void free_device(liberi_handle h) {
     for (void *p : h->allocs) cudaFreeAsync(p, h->stream);
     h->allocs.clear();
+    h->arena_basis = h->arena_plans = liberi_handle_s::Arena();
+    h->arena = nullptr;
     h->dev = DeviceBuffers();
     h->d_tab = nullptr;
     h->d_tabf = nullptr;
@@ -453,7 +502,13 @@ static void build_ket_records(const BasisHost &b, const PairsHost &pr, const std
     }
 }
 
+static size_t plan_device_bytes(const PlanHost &ph);
+
 static int upload_plans(liberi_handle h) {
+    size_t total = 0;
+    for (int k = 0; k < NKERN; k++) total += plan_device_bytes(h->plan[k]);
+    CUDA_TRY(arena_open(h, h->arena_plans, total));
+    ArenaScope scope{h};
     for (int k = 0; k < NKERN; k++) {
         PlanHost &ph = h->plan[k];
         if (ph.nbra == 0) continue;
@@ -480,21 +535,23 @@ static int upload_plans(liberi_handle h) {
 // Device bytes that upload_plans allocates for one class plan.
 static size_t plan_device_bytes(const PlanHost &ph) {
     if (ph.nbra == 0) return 0;
-    const size_t nb = ph.bra_ids.size(), nk = ph.ket_ids.size();
-    const size_t cap = ph.task_cap > 0 ? (size_t)ph.task_cap : 1;
-    return 4 * (nb + nk) * 2 + 8 * (nb + nk) + sizeof(double4) * KET_REC * nk +
-           sizeof(int4) * (ph.items.size() + ph.tasks.size()) + 2 * sizeof(int4) * cap + 4 * sizeof(int);
+    return up_bytes(KET_REC * ph.ket_ids.size(), sizeof(double4)) + up_bytes(ph.bra_ids.size(), sizeof(int)) +
+           up_bytes(ph.ket_ids.size(), sizeof(int)) + up_bytes(ph.bra_orig.size(), sizeof(int)) +
+           up_bytes(ph.ket_orig.size(), sizeof(int)) + up_bytes(ph.bra_x.size(), sizeof(double)) +
+           up_bytes(ph.ket_x.size(), sizeof(double)) + up_bytes(ph.items.size(), sizeof(int4)) +
+           up_bytes(ph.tasks.size(), sizeof(int4)) + 2 * al_bytes((size_t)ph.task_cap, sizeof(int4)) +
+           al_bytes(4, sizeof(int));
 }
 
 // Device bytes that upload_basis allocates.
 static size_t basis_device_bytes(const BasisHost &b, const PairsHost &pr) {
-    const size_t npair = pr.shell.size(), nprim = pr.P.size();
-    const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
-    return sizeof(double4) * b.nsh + sizeof(int) * b.nsh + (sizeof(int2) + 2 * sizeof(int)) * npair +
-           (sizeof(double4) + sizeof(double2) + 2 * sizeof(float4)) * nprim + sizeof(double) * RYS_TABLE_SIZE +
-           sizeof(float) * RYSF_TABLE_SIZE + 2 * sizeof(double) * (ntri > 0 ? ntri : 1) +
-           (sizeof(double) + sizeof(float)) * ((size_t)b.num_bas * b.num_bas > 0 ? (size_t)b.num_bas * b.num_bas : 1) +
-           sizeof(unsigned long long);
+    const size_t npair = pr.shell.size(), nprim = pr.P.size(), nsh = (size_t)b.nsh;
+    const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2, nsq = (size_t)b.num_bas * b.num_bas;
+    return up_bytes(nsh, sizeof(double4)) + up_bytes(nsh, sizeof(int)) + up_bytes(npair, sizeof(int2)) +
+           2 * up_bytes(npair, sizeof(int)) + up_bytes(nprim, sizeof(double4)) + up_bytes(nprim, sizeof(double2)) +
+           up_bytes(2 * nprim, sizeof(float4)) + up_bytes(RYS_TABLE_SIZE, sizeof(double)) +
+           up_bytes(RYSF_TABLE_SIZE, sizeof(float)) + 2 * al_bytes(ntri, sizeof(double)) +
+           al_bytes(nsq, sizeof(double)) + al_bytes(nsq, sizeof(float)) + al_bytes(1, sizeof(unsigned long long));
 }
 
 static void compute_stats(liberi_handle h) {
@@ -546,8 +603,12 @@ static int copy_basis(BasisHost &b, int nsh, int natoms, int num_bas, int mxgtot
     return LIBERI_OK;
 }
 
+static size_t basis_device_bytes(const BasisHost &b, const PairsHost &pr);
+
 static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) {
     const BasisHost &b = h->basis;
+    CUDA_TRY(arena_open(h, h->arena_basis, basis_device_bytes(b, h->pairs)));
+    ArenaScope scope{h};
     std::vector<int> bf0(b.nsh);
     for (int s = 0; s < b.nsh; s++) bf0[s] = b.atom_loc[s] - 1;
     CUDA_TRY(dev_upload(h, &h->dev.shell_xyz, shell_xyz.data(), shell_xyz.size()));
@@ -606,12 +667,16 @@ static int replan(liberi_handle h) {
     if (had_plans) CUDA_TRY(cudaDeviceSynchronize());
     for (int k = 0; k < NKERN; k++) {
         PlanHost &ph = h->plan[k];
-        h->dev.bytes -= plan_device_bytes(ph);
-        for (void *p : {(void *)ph.d_bra, (void *)ph.d_ket, (void *)ph.d_bra_orig, (void *)ph.d_ket_orig,
-                        (void *)ph.d_bra_x, (void *)ph.d_ket_x, (void *)ph.d_items, (void *)ph.d_tasks,
-                        (void *)ph.d_tasks64, (void *)ph.d_tasks32, (void *)ph.d_ntasks})
+        // pieces of the plan arena are released with it; a task list the
+        // tuner uploaded on its own is released here
+        for (void *p : {(void *)ph.d_ket_rec, (void *)ph.d_bra, (void *)ph.d_ket, (void *)ph.d_bra_orig,
+                        (void *)ph.d_ket_orig, (void *)ph.d_bra_x, (void *)ph.d_ket_x, (void *)ph.d_items,
+                        (void *)ph.d_tasks, (void *)ph.d_tasks64, (void *)ph.d_tasks32, (void *)ph.d_ntasks})
             if (p) dev_release(h, p);
     }
+    if (h->arena_plans.base) dev_release(h, h->arena_plans.base);
+    h->arena_plans = liberi_handle_s::Arena();
+    h->dev.bytes = h->arena_basis.size;
     const BasisHost &b = h->basis;
     for (int k = 0; k < NKERN; k++) {
         const KernelDesc &kd = KDESC[k];
