@@ -147,8 +147,8 @@ struct liberi_handle_s {
     float *d_tabf = nullptr;
     unsigned long long *d_maxd = nullptr;
     cudaStream_t stream = nullptr;
-    // classes that cannot fill the GPU on their own run on a second stream
-    // beside the others (forked from and joined back into the build's stream)
+    // mixed builds run their FP64 task lists on a second stream beside the
+    // FP32 lists (forked from and joined back into the build's stream)
     bool overlap = true;
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
@@ -723,13 +723,22 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     CUDA_TRY(launch_unpack(dD, b.num_bas, h->dev.Dsq, mixed ? h->dev.Df : nullptr, st));
     if (mixed) CUDA_TRY(launch_maxabs(dD, ntri, h->d_maxd, st));
     for (int k = 0; k < NKERN; k++) h->ev_recorded[k] = false;
-    // mixed precision: the high-L classes with few quartets per row pair (a
-    // latency tail) start first on the side stream and overlap the others
-    // (measured on C60: 1 ms faster mixed, 5 ms slower FP64, where the
-    // co-running high-register classes crowd the large ones); per-class
-    // timing keeps one stream
+    // mixed precision: every class's FP64 task list (the few quartets above
+    // fp32_cut, the costliest ones, in small low-occupancy launches) runs on
+    // the side stream beside the FP32 lists on the build's stream.  Measured
+    // on C60: 1.5 ms faster at cut 1e-2 than running them in turn, where
+    // putting the high-L classes on the side instead gained 1 ms; FP64
+    // builds keep one stream (co-running classes crowd each other there).
+    // The task splits of every class come first; per-class timing keeps one
+    // stream.
     const bool fork = h->overlap && !h->timing && mixed;
     if (fork) {
+        for (int k = 0; k < NKERN; k++) {
+            PlanHost &ph = h->plan[k];
+            if (ph.total == 0 || !((h->class_mask >> k) & 1u)) continue;
+            CUDA_TRY(launch_split_tasks((int)ph.items.size(), ph.d_items, ph.d_bra_x, ph.d_ket_x, h->d_maxd,
+                                        h->fp32_cut, ph.chunk, ph.d_tasks64, ph.d_tasks32, ph.d_ntasks, st));
+        }
         if (!h->side) {
             CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
             CUDA_TRY(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
@@ -738,16 +747,14 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
         CUDA_TRY(cudaEventRecord(h->fork_ev, st));
         CUDA_TRY(cudaStreamWaitEvent(h->side, h->fork_ev, 0));
     }
-    static const int ORDER[NKERN] = {20, 19, 18, 14, 11, 13, 10,  // side stream when forked
-                                     0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 12, 15, 16, 17};
-    const int NSIDE = 7;
+    // high-L classes (few quartets per row pair, a latency tail) first
+    static const int ORDER[NKERN] = {20, 19, 18, 14, 11, 13, 10, 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 12, 15, 16, 17};
     for (int oi = 0; oi < NKERN; oi++) {
         const int k = ORDER[oi];
         PlanHost &ph = h->plan[k];
         if (ph.total == 0 || !((h->class_mask >> k) & 1u)) continue;
         const KernelDesc &kd = KDESC[k];
-        const cudaStream_t cs = (fork && oi < NSIDE) ? h->side : st;
-        ctx.stream = cs;
+        ctx.stream = st;
         if (h->timing) {
             if (!h->ev[k][0]) {
                 CUDA_TRY(cudaEventCreate(&h->ev[k][0]));
@@ -780,14 +787,17 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
             dp.ntasks = (int)ph.tasks.size();
             CUDA_TRY(launch_class(k, ctx, dp, rs, 0, nbf, tile_rows, h->variant[0][k]));
         } else {
-            CUDA_TRY(launch_split_tasks((int)ph.items.size(), ph.d_items, ph.d_bra_x, ph.d_ket_x, h->d_maxd,
-                                        h->fp32_cut, ph.chunk, ph.d_tasks64, ph.d_tasks32, ph.d_ntasks, cs));
+            if (!fork)
+                CUDA_TRY(launch_split_tasks((int)ph.items.size(), ph.d_items, ph.d_bra_x, ph.d_ket_x, h->d_maxd,
+                                            h->fp32_cut, ph.chunk, ph.d_tasks64, ph.d_tasks32, ph.d_ntasks, st));
             dp.ntasks = ph.task_cap;
             dp.tasks = ph.d_tasks64;
             dp.ntasks_dev = ph.d_ntasks;
+            ctx.stream = fork ? h->side : st;
             CUDA_TRY(launch_class(k, ctx, dp, rs, 0, nbf, tile_rows, h->variant[0][k]));
             dp.tasks = ph.d_tasks32;
             dp.ntasks_dev = ph.d_ntasks + 1;
+            ctx.stream = st;
             CUDA_TRY(launch_class(k, ctx, dp, rs, 1, nbf, tile_rows, h->variant[1][k]));
         }
         if (h->timing) {

@@ -106,8 +106,8 @@ int liberi_c_last_error(char *buf, int32_t len);
  *   "tile_mask"    (bit k set = class k may stage rows of F in a shared-memory
  *                   tile, where it fits; default none: F is updated with FP64
  *                   atomics in L2, faster on B200 for every class measured)
- *   "overlap"      (1 = in mixed-precision builds the high-L classes with few
- *                   quartets run on a second stream beside the others, forked
+ *   "overlap"      (1 = in mixed-precision builds every class's FP64 task
+ *                   list runs on a second stream beside the FP32 lists, forked
  *                   from and joined back into the build's stream; default 1;
  *                   off while "timing")
  *   "timing"       (1 = record per-class device times for liberi_c_get_stats)
