@@ -863,6 +863,9 @@ struct liberi_batch_s {
     std::vector<size_t> sq_off;
     bool bound = false;
     cudaStream_t stream = nullptr;
+    // mixed: the FP64 lists run on a second stream beside the FP32 lists
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<void *> allocs;
@@ -877,6 +880,11 @@ static void batch_free(liberi_batch b) {
     b->allocs.clear();
     if (b->stream) cudaStreamDestroy(b->stream);
     b->stream = nullptr;
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+    if (b->join_ev) cudaEventDestroy(b->join_ev);
+    b->side = nullptr;
+    b->fork_ev = b->join_ev = nullptr;
 }
 
 static int batch_build_tasks(liberi_batch b, int k) {
@@ -912,20 +920,34 @@ static int batch_enqueue(liberi_batch b, cudaStream_t st, uint32_t mask) {
     const bool mixed = b->precision == 1;
     CUDA_TRY(launch_batch_prep(b->d_mols, (int)b->hs.size(), (long long)b->nbf_max * b->nbf_max,
                                mixed ? b->d_maxd : nullptr, st));
-    for (int k = 0; k < NKERN; k++) {
-        if (!((mask >> k) & 1u) || b->ntasks[k] == 0) continue;
-        if (!mixed) {
+    if (!mixed) {
+        for (int k = 0; k < NKERN; k++) {
+            if (!((mask >> k) & 1u) || b->ntasks[k] == 0) continue;
             CUDA_TRY(launch_class_batch(k, ctx, b->d_tasks[k], b->ntasks[k], b->nbf_max, b->d_mols, b->d_cv[k],
                                         KDESC[k].swap, 0, nullptr));
-            continue;
         }
+        return LIBERI_OK;
+    }
+    // mixed: every class's task split, then the FP64 lists on the side stream
+    // beside the FP32 lists (as for single-molecule builds), joined back
+    for (int k = 0; k < NKERN; k++) {
+        if (!((mask >> k) & 1u) || b->ntasks[k] == 0) continue;
         CUDA_TRY(launch_split_batch(b->nitems[k], b->d_items[k], b->d_cv[k], b->d_maxd, b->fp32_cut, b->chunk[k],
                                     b->d_t64[k], b->d_t32[k], b->d_counts[k], st));
+    }
+    CUDA_TRY(cudaEventRecord(b->fork_ev, st));
+    CUDA_TRY(cudaStreamWaitEvent(b->side, b->fork_ev, 0));
+    for (int k = 0; k < NKERN; k++) {
+        if (!((mask >> k) & 1u) || b->ntasks[k] == 0) continue;
+        ctx.stream = b->side;
         CUDA_TRY(launch_class_batch(k, ctx, b->d_t64[k], b->cap[k], b->nbf_max, b->d_mols, b->d_cv[k],
                                     KDESC[k].swap, 0, b->d_counts[k]));
+        ctx.stream = st;
         CUDA_TRY(launch_class_batch(k, ctx, b->d_t32[k], b->cap[k], b->nbf_max, b->d_mols, b->d_cv[k],
                                     KDESC[k].swap, 1, b->d_counts[k] + 1));
     }
+    CUDA_TRY(cudaEventRecord(b->join_ev, b->side));
+    CUDA_TRY(cudaStreamWaitEvent(st, b->join_ev, 0));
     return LIBERI_OK;
 }
 
@@ -1168,6 +1190,10 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
     DeviceGuard dev_guard(b->device);
     int rc = LIBERI_OK;
     auto die = [&](int code) { batch_free(b); delete b; return code; };
+    if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming) != cudaSuccess)
+        return die(fail(LIBERI_E_DEVICE, "liberi_batch_create: stream or event creation failed"));
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
         return die(fail(LIBERI_E_DEVICE, "liberi_batch_create: stream creation failed"));
     if (cudaMalloc((void **)&b->d_mols, n * sizeof(MolView)) != cudaSuccess)
