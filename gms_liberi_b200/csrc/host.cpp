@@ -148,7 +148,8 @@ struct liberi_handle_s {
     unsigned long long *d_maxd = nullptr;
     cudaStream_t stream = nullptr;
     // mixed builds run their FP64 task lists on a second stream beside the
-    // FP32 lists (forked from and joined back into the build's stream)
+    // FP32 lists, FP64 builds the classes (dd|dd) and (dd|pd) (forked from and
+    // joined back into the build's stream)
     bool overlap = true;
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
@@ -728,17 +729,21 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     // the side stream beside the FP32 lists on the build's stream.  Measured
     // on C60: 1.5 ms faster at cut 1e-2 than running them in turn, where
     // putting the high-L classes on the side instead gained 1 ms; FP64
-    // builds keep one stream (co-running classes crowd each other there).
-    // The task splits of every class come first; per-class timing keeps one
-    // stream.
-    const bool fork = h->overlap && !h->timing && mixed;
-    if (fork) {
+    // builds put only (dd|dd) and (dd|pd) there, two classes of few long
+    // CTAs at low occupancy (0.8 ms faster; more classes on the side crowd
+    // the large ones: the seven high-L classes cost 5 ms).  The task splits
+    // of every class come first; per-class timing keeps one stream.
+    const bool fork = h->overlap && !h->timing;
+    const uint32_t side64 = mixed ? 0u : (1u << 20) | (1u << 19);
+    if (fork && mixed) {
         for (int k = 0; k < NKERN; k++) {
             PlanHost &ph = h->plan[k];
             if (ph.total == 0 || !((h->class_mask >> k) & 1u)) continue;
             CUDA_TRY(launch_split_tasks((int)ph.items.size(), ph.d_items, ph.d_bra_x, ph.d_ket_x, h->d_maxd,
                                         h->fp32_cut, ph.chunk, ph.d_tasks64, ph.d_tasks32, ph.d_ntasks, st));
         }
+    }
+    if (fork) {
         if (!h->side) {
             CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
             CUDA_TRY(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
@@ -785,7 +790,9 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
             dp.tasks = ph.d_tasks;
             dp.ntasks_dev = nullptr;
             dp.ntasks = (int)ph.tasks.size();
+            ctx.stream = (fork && ((side64 >> k) & 1u)) ? h->side : st;
             CUDA_TRY(launch_class(k, ctx, dp, rs, 0, nbf, tile_rows, h->variant[0][k]));
+            ctx.stream = st;
         } else {
             if (!fork)
                 CUDA_TRY(launch_split_tasks((int)ph.items.size(), ph.d_items, ph.d_bra_x, ph.d_ket_x, h->d_maxd,
