@@ -188,6 +188,11 @@ const std::vector<double> &rys_table_host();
 const std::vector<float> &rys_table_f32_host();
 
 // Launchers (kernels.cu) ------------------------------------------------------
+// builds of at most FAN_MAX_QUARTETS screened quartets spread their classes
+// over FAN_STREAMS streams (option "overlap")
+constexpr int FAN_STREAMS = 8;
+constexpr long long FAN_MAX_QUARTETS = 25000000;
+
 struct LaunchCtx {
     DevBasis basis;
     const double *rys_tab;

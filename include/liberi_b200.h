@@ -106,11 +106,13 @@ int liberi_c_last_error(char *buf, int32_t len);
  *   "tile_mask"    (bit k set = class k may stage rows of F in a shared-memory
  *                   tile, where it fits; default none: F is updated with FP64
  *                   atomics in L2, faster on B200 for every class measured)
- *   "overlap"      (1 = a second stream, forked from and joined back into
- *                   the build's stream, runs every class's FP64 task list
- *                   beside the FP32 lists in mixed-precision builds, and the
- *                   (dd|dd) and (dd|pd) classes beside the others in FP64
- *                   builds; default 1; off while "timing")
+ *   "overlap"      (1 = streams forked from and joined back into the
+ *                   build's stream: builds of at most 25 million screened
+ *                   quartets spread their classes over 8 streams; larger ones
+ *                   run every class's FP64 task list beside the FP32 lists
+ *                   (mixed precision) or the (dd|dd) and (dd|pd) classes beside
+ *                   the others (FP64) on a second stream; default 1; off while
+ *                   "timing")
  *   "timing"       (1 = record per-class device times for liberi_c_get_stats)
  * Options set before liberi_c_setup apply to it; cut options may also be
  * changed between builds (the quartet plan is rebuilt on the next build). */
