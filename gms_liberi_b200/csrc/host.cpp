@@ -153,7 +153,8 @@ struct liberi_handle_s {
     bool overlap = true;
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
-    // small builds spread their classes over FAN_STREAMS streams
+    // small builds spread their classes over FAN_STREAMS streams (option "fan")
+    bool fan_out = true;
     cudaStream_t fan[FAN_STREAMS] = {};
     cudaEvent_t fan_ev[FAN_STREAMS] = {};
     int num_sms = 148;
@@ -750,7 +751,7 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     long long nquart = 0;
     for (int k = 0; k < NKERN; k++)
         if ((h->class_mask >> k) & 1u) nquart += h->stats.quartets[k];
-    const bool fan = h->overlap && !h->timing && nquart <= FAN_MAX_QUARTETS;
+    const bool fan = h->fan_out && h->overlap && !h->timing && nquart <= FAN_MAX_QUARTETS;
     const bool fork = h->overlap && !h->timing && !fan;
     const uint32_t side64 = mixed ? 0u : (1u << 20) | (1u << 19);
     if (fan) {
@@ -1587,6 +1588,8 @@ int liberi_c_set_option(liberi_handle h, const char *name, double value) {
         h->rank_split = (int)value;
     } else if (n == "overlap") {
         h->overlap = value != 0;
+    } else if (n == "fan") {
+        h->fan_out = value != 0;
     } else if (n == "tile_mask") {
         if (!(value >= 0 && value < (double)(1u << NKERN))) return fail(LIBERI_E_ARG, "tile_mask out of range");
         h->tile_mask = (uint32_t)value;
@@ -1609,6 +1612,7 @@ int liberi_c_get_option(liberi_handle h, const char *name, double *value) {
     else if (n == "class_mask") *value = h->class_mask;
     else if (n == "tile_mask") *value = h->tile_mask;
     else if (n == "overlap") *value = h->overlap ? 1 : 0;
+    else if (n == "fan") *value = h->fan_out ? 1 : 0;
     else if (n == "rank_split") *value = h->rank_split;
     else if (n == "timing") *value = h->timing ? 1 : 0;
     else return fail(LIBERI_E_ARG, "unknown option '%s'", name);

@@ -237,6 +237,8 @@ class LiberiEngine(Engine):
         h.set_option("schwarz_cut", self.schwarz_cut)
         h.set_option("precision", self.precision)
         h.set_option("fp32_cut", self.fp32_cut)
+        # concurrent sessions fill the GPU: no multi-stream spread of one build
+        h.set_option("fan", 0)
         liberi.setup_from_basis(h, b)
         stream = torch.cuda.Stream(device=self.dev)
         D0 = s.D0 if s.D0 is not None else M.density(b["num_bas"], M.nocc_of(b), seed=s.seed)

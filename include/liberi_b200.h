@@ -108,11 +108,14 @@ int liberi_c_last_error(char *buf, int32_t len);
  *                   atomics in L2, faster on B200 for every class measured)
  *   "overlap"      (1 = streams forked from and joined back into the
  *                   build's stream: builds of at most 25 million screened
- *                   quartets spread their classes over 8 streams; larger ones
- *                   run every class's FP64 task list beside the FP32 lists
- *                   (mixed precision) or the (dd|dd) and (dd|pd) classes beside
- *                   the others (FP64) on a second stream; default 1; off while
- *                   "timing")
+ *                   quartets spread their classes over 8 streams (while "fan"
+ *                   is 1); larger ones run every class's FP64 task list beside
+ *                   the FP32 lists (mixed precision) or the (dd|dd) and (dd|pd)
+ *                   classes beside the others (FP64) on a second stream;
+ *                   default 1; off while "timing")
+ *   "fan"          (1 = the 8-stream spread of small builds above, default 1;
+ *                   set 0 where many handles build at once and already fill
+ *                   the GPU, as the serving loop does)
  *   "timing"       (1 = record per-class device times for liberi_c_get_stats)
  * Options set before liberi_c_setup apply to it; cut options may also be
  * changed between builds (the quartet plan is rebuilt on the next build). */
