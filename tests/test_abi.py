@@ -58,6 +58,21 @@ def test_options_validate():
         assert e.value.code == -1
 
 
+def test_launch_options_round_trip():
+    # the scheduling and tiling options: defaults, set/get, rejected values
+    h = liberi.liberi_create()
+    assert h.get_option("overlap") == 1 and h.get_option("fan") == 1
+    assert h.get_option("tile_mask") == 0 and h.get_option("rank_split") == 0
+    for name, val in [("overlap", 0), ("fan", 0), ("tile_mask", 5), ("rank_split", 1)]:
+        h.set_option(name, val)
+        assert h.get_option(name) == val
+    for name, val in [("tile_mask", -1), ("tile_mask", float(1 << 21)), ("rank_split", 2)]:
+        with pytest.raises(liberi.LiberiError) as e:
+            h.set_option(name, val)
+        assert e.value.code == -1
+    liberi.liberi_destroy(h)
+
+
 @pytest.mark.parametrize("bad", ["fshell", "rank", "sizes", "num_bas"])
 def test_setup_rejects_bad_input(bad):
     h = liberi.liberi_create()
