@@ -2,9 +2,11 @@
 plumbing.
 
 Every rank sets up its handle with (my_rank, num_procs); the engine then
-evaluates exactly the quartets the reference assigns that rank (the per-kernel
-tile/chunk split of src/rhf/rot_axis/int0000.F90:76-91 and
-int0001.F90:89-104) and returns a partial packed F.  The caller's reduction
+evaluates either exactly the quartets the reference assigns that rank (the
+per-kernel tile/chunk split of src/rhf/rot_axis/int0000.F90:76-91 and
+int0001.F90:89-104, option rank_split 0) or a contiguous slice of every
+class's work of equal primitive-quartet cost (rank_split 1), and returns a
+partial packed F; the partials sum to the same F.  The caller's reduction
 (GAMESS: DDI_GSUMF, liberi_interface.F90:13-15) is one all-reduce (sum) of the
 packed F over NCCL.  There is no other data exchange: D is replicated.
 """
