@@ -139,3 +139,26 @@ def test_class_variant_arguments():
             h.set_class_variant(*bad)
         assert e.value.code == -1
     liberi.liberi_destroy(h)
+
+
+def test_fortran_shim_matches_the_c_abi():
+    """The Fortran iso_c_binding shim (shipped as source: no Fortran compiler
+    here) binds only functions the header declares and the library exports,
+    each with the header's number of arguments."""
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = open(os.path.join(root, "gms_liberi_b200", "fortran", "liberi_b200_interface.F90")).read()
+    src = re.sub(r"&\s*\n\s*", " ", src)  # join continuation lines
+    header = open(os.path.join(root, "include", "liberi_b200.h")).read()
+    binds = re.findall(r"function\s+(\w+)\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)", src, re.I)
+    assert len(binds) >= 6
+    lib = liberi.lib()
+    for fname, args, cname in binds:
+        assert fname == cname
+        m = re.search(r"\bint\s+%s\s*\(([^)]*)\)\s*;" % cname, header, re.S)
+        assert m, cname
+        n_c = 0 if m.group(1).strip() in ("", "void") else len(m.group(1).split(","))
+        n_f = 0 if not args.strip() else len(args.split(","))
+        assert n_f == n_c, (cname, n_f, n_c)
+        assert hasattr(lib, cname), cname
