@@ -8,6 +8,9 @@ disables screening with schwrz_int = 1e10, uses an identity density, and
 compares every packed Fock element against hard-coded values at tol = 1e-10.
 This script parses those assignments and the `fa_ref` arrays and writes one
 JSON fixture per test, so the parity tests never need the reference tree.
+It also writes h2o_ccpvtz.json from the f-shell known-answer program
+(tests/fortran/test_h2o_ccpvtz.F90 with fa_h2o_ccpvtz_reference.dat), kept
+for the f-shell classes.
 
 Usage (needs the reference checkout; the fixtures are committed):
     python tests/golden/make_golden.py /path/to/gms_libERI
@@ -37,6 +40,8 @@ def gto_norm(kind, a):
         return 2.0 * math.sqrt(a) * base
     if kind == "d":
         return 4.0 * a * base
+    if kind == "f":
+        return 8.0 * a * math.sqrt(a) * base
     raise ValueError(kind)
 
 
@@ -131,6 +136,115 @@ def build(ref_root, key, rel):
     return out
 
 
+# ---- the f-shell known answer (tests/fortran/test_h2o_ccpvtz.F90) ------------
+# That test fills its basis in two subroutines (oxygen; hydrogen with the atom
+# and first shell as arguments) through integer variables, and reads its 2145
+# reference values from fa_h2o_ccpvtz_reference.dat.  The small interpreter
+# below runs exactly those statement forms; every expression is checked
+# against a whitelist before evaluation (the reference is read as data).
+F_TEST = "tests/fortran/test_h2o_ccpvtz.F90"
+F_DAT = "tests/fortran/fa_h2o_ccpvtz_reference.dat"
+_SAFE = re.compile(r"^[\w\s+\-*/().]*$")
+
+
+def _fexpr(expr, env, arrs):
+    expr = expr.strip()
+    m = re.fullmatch(r"(%s)\s*\*\s*gto_norm_([spdf])\(\s*(%s)\s*\)" % (REAL, REAL), expr)
+    if m:
+        return fnum(m.group(1)) * gto_norm(m.group(2), fnum(m.group(3)))
+    if re.fullmatch(REAL, expr):
+        return fnum(expr)
+    # integer arithmetic over the subroutine's variables and array reads
+    expr = re.sub(r"(\w+_arr)\(([^()]*)\)",
+                  lambda mm: repr(arrs[ALIASES[mm.group(1)]][int(_fexpr(mm.group(2), env, arrs))]), expr)
+    if not _SAFE.match(expr):
+        raise ValueError("unexpected expression: %r" % expr)
+    for name in re.findall(r"[A-Za-z_]\w*", expr):
+        if name not in env:
+            raise ValueError("unknown name %r in %r" % (name, expr))
+    return eval(expr, {"__builtins__": {}}, dict(env))
+
+
+def _run_body(lines, env, arrs):
+    active = [True]
+    for raw in lines:
+        code = raw.split("!")[0].strip()
+        if not code:
+            continue
+        m = re.fullmatch(r"if\s*\((\w+)\s*==\s*(\d+)\)\s*then", code)
+        if m:
+            active.append(active[-1] and env[m.group(1)] == int(m.group(2)))
+            continue
+        if code == "else":
+            active[-1] = active[-2] and not active[-1]
+            continue
+        if code in ("end if", "endif"):
+            active.pop()
+            continue
+        if not active[-1] or code.startswith("integer"):
+            continue
+        for stmt in code.split(";"):
+            stmt = stmt.strip()
+            m = re.fullmatch(r"(\w+)\(([^=]*)\)\s*=\s*(.+)", stmt)
+            if m and m.group(1) in ALIASES:
+                idx = int(_fexpr(m.group(2), env, arrs))
+                arrs.setdefault(ALIASES[m.group(1)], {})[idx] = _fexpr(m.group(3), env, arrs)
+                continue
+            m = re.fullmatch(r"(\w+)\s*=\s*(.+)", stmt)
+            if m:
+                env[m.group(1)] = int(_fexpr(m.group(2), env, arrs))
+                continue
+            raise ValueError("unexpected statement: %r" % stmt)
+
+
+def build_f(ref_root):
+    text = open(os.path.join(ref_root, F_TEST)).read().splitlines()
+    subs, cur = {}, None
+    for raw in text:
+        code = raw.split("!")[0].strip()
+        m = re.match(r"subroutine\s+(\w+)\s*\(([^)]*)\)", code)
+        if m:
+            cur = m.group(1)
+            subs[cur] = ([a.strip() for a in m.group(2).split(",") if a.strip()], [])
+            continue
+        if code.startswith("end subroutine"):
+            cur = None
+            continue
+        if cur:
+            subs[cur][1].append(raw)
+    scal, arrs, _, _ = parse(os.path.join(ref_root, F_TEST))  # scalars and coordinates
+    for raw in text:
+        m = re.match(r"\s*call\s+(setup_\w+)\s*\(([^)]*)\)", raw.split("!")[0])
+        if not m:
+            continue
+        params, body = subs[m.group(1)]
+        args = [int(a) for a in m.group(2).split(",") if a.strip()]
+        _run_body(body, dict(zip(params, args)), arrs)
+    vals = open(os.path.join(ref_root, F_DAT)).read().split()
+    count, fa_ref = int(vals[0]), [fnum(v) for v in vals[1:]]
+    assert count == len(fa_ref)
+    nsh, mx = scal["nsh"], scal["mxgtot"]
+    out = dict(scal)
+    for name in ["ang_mom", "contr_num", "sh_loc", "atom_num", "atom_loc", "start_bas", "end_bas"]:
+        out[name] = [int(arrs[name][i]) for i in range(1, nsh + 1)]
+    for name in ["exponents", "coef_s", "coef_p", "coef_d", "coef_f"]:
+        d = arrs.get(name, {})
+        out[name] = [float(d.get(i, 0.0)) for i in range(1, mx * nsh + 1)]
+    out["coords"] = [float(arrs["coords"][i]) for i in range(1, 3 * scal["natoms"] + 1)]
+    n = scal["num_bas"]
+    ntri = n * (n + 1) // 2
+    assert len(fa_ref) == ntri, (len(fa_ref), ntri)
+    out["schwrz"] = [1.0e10] * (nsh * (nsh + 1) // 2)
+    dens = [0.0] * ntri
+    for i in range(1, n + 1):
+        dens[i * (i + 1) // 2 - 1] = 1.0
+    out["density"] = dens
+    out["fa_ref"] = fa_ref
+    out["tol"] = 1.0e-10
+    out["source"] = "%s (basis), %s (values)" % (F_TEST, F_DAT)
+    return out
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LIBERI_REFERENCE", "")
     if not ref_root or not os.path.isdir(ref_root):
@@ -141,6 +255,10 @@ def main():
         with open(os.path.join(here, key + ".json"), "w") as f:
             json.dump(fx, f, indent=0)
         print(key, "nsh", fx["nsh"], "nbf", fx["num_bas"], "values", len(fx["fa_ref"]))
+    fx = build_f(ref_root)
+    with open(os.path.join(here, "h2o_ccpvtz.json"), "w") as f:
+        json.dump(fx, f, indent=0)
+    print("h2o_ccpvtz", "nsh", fx["nsh"], "nbf", fx["num_bas"], "values", len(fx["fa_ref"]))
 
 
 if __name__ == "__main__":
