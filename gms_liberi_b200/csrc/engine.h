@@ -207,6 +207,10 @@ struct LaunchCtx {
 
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
                          int precision, int nbf, int tile_rows, int variant);  // precision 0: FP64, 1: FP32
+// adds {count, sum, xor} of the hashes of the quartets a launch of class k over
+// this plan's task list would evaluate to out[0..2] (zeroed by the caller)
+cudaError_t launch_quartet_fp(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
+                              unsigned long long *out);
 // one launch of class k over the tasks of several molecules (task.w = molecule)
 cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, int ntasks, int nbf_max,
                                const MolView *d_mols, const ClassView *d_cviews, bool swapped, int precision,

@@ -136,6 +136,7 @@ struct liberi_handle_s {
     int chunk[NKERN] = {};  // kets per CTA task per class (0 = default)
     int variant[2][NKERN] = {};  // kernel shape variant per class, FP64 / FP32 tier
     bool timing = false;
+    bool last_split_lists = false;  // the last build ran the per-build FP64/FP32 task lists
     cudaEvent_t ev[NKERN + 1][2] = {};
     bool ev_recorded[NKERN] = {};
     bool plan_dirty = false;
@@ -733,11 +734,45 @@ static int replan(liberi_handle h) {
     return LIBERI_OK;
 }
 
+// The reference's rank split of class k as the class kernels apply it
+// (balanced split: the plan already holds only this rank's items).
+static RankSplit rank_split_of(liberi_handle h, int k) {
+    const KernelDesc &kd = KDESC[k];
+    const PlanHost &ph = h->plan[k];
+    RankSplit rs;
+    rs.rank = h->my_rank;
+    rs.nsize = h->rank_split == 1 ? 1 : h->num_procs;
+    rs.tile = kd.tile;
+    rs.ntot = ph.ntot_ref;
+    rs.nbra_ref = ph.nbra_ref;
+    rs.nket_ref = ph.nket_ref;
+    rs.tri = kd.tri;
+    rs.ketmajor = kd.ketmajor;
+    return rs;
+}
+
+// Device lists of class k's plan (the task list is filled in by the caller).
+static DevPlan dev_plan_of(liberi_handle h, int k) {
+    const PlanHost &ph = h->plan[k];
+    DevPlan dp;
+    dp.bra_ids = ph.d_bra;
+    dp.ket_ids = ph.d_ket;
+    dp.ket_rec = ph.d_ket_rec;
+    dp.bra_orig = ph.d_bra_orig;
+    dp.ket_orig = ph.d_ket_orig;
+    dp.tasks = ph.d_tasks;
+    dp.ntasks_dev = nullptr;
+    dp.ntasks = (int)ph.tasks.size();
+    dp.swapped = KDESC[k].swap;
+    return dp;
+}
+
 static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaStream_t st) {
     if (h->plan_dirty) {
         int rc = replan(h);
         if (rc) return rc;
     }
+    h->last_split_lists = h->precision == 1;
     const BasisHost &b = h->basis;
     const long long ntri = (long long)b.num_bas * (b.num_bas + 1) / 2;
     CUDA_TRY(cudaMemsetAsync(dF, 0, ntri * sizeof(double), st));  // liberi_driver.F90:64
@@ -805,11 +840,11 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
         }
     }
     if (fork) {
-        if (!h->side) {
-            CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
-            CUDA_TRY(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
-            CUDA_TRY(cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming));
-        }
+        // each object is created once per handle (the fan-out path may have
+        // made the fork event already)
+        if (!h->side) CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+        if (!h->fork_ev) CUDA_TRY(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
+        if (!h->join_ev) CUDA_TRY(cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming));
         CUDA_TRY(cudaEventRecord(h->fork_ev, st));
         CUDA_TRY(cudaStreamWaitEvent(h->side, h->fork_ev, 0));
     }
@@ -828,22 +863,8 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
             }
             CUDA_TRY(cudaEventRecord(h->ev[k][0], st));
         }
-        RankSplit rs;
-        rs.rank = h->my_rank;
-        rs.nsize = h->rank_split == 1 ? 1 : h->num_procs;  // balanced: the plan holds this rank's items
-        rs.tile = kd.tile;
-        rs.ntot = ph.ntot_ref;
-        rs.nbra_ref = ph.nbra_ref;
-        rs.nket_ref = ph.nket_ref;
-        rs.tri = kd.tri;
-        rs.ketmajor = kd.ketmajor;
-        DevPlan dp;
-        dp.bra_ids = ph.d_bra;
-        dp.ket_ids = ph.d_ket;
-        dp.ket_rec = ph.d_ket_rec;
-        dp.bra_orig = ph.d_bra_orig;
-        dp.ket_orig = ph.d_ket_orig;
-        dp.swapped = kd.swap;
+        const RankSplit rs = rank_split_of(h, k);
+        DevPlan dp = dev_plan_of(h, k);
         const int nbf = b.num_bas;
         const size_t tile_bytes = (size_t)(ncart_l(kd.la) + ncart_l(kd.lb)) * nbf * sizeof(double);
         const int tile_rows = (tile_bytes <= TILE_MAX_BYTES && ((h->tile_mask >> k) & 1u)) ? 1 : 0;
@@ -1658,6 +1679,47 @@ int liberi_c_get_stats(liberi_handle h, liberi_stats *stats) {
         }
     }
     *stats = h->stats;
+    return LIBERI_OK;
+}
+
+int liberi_c_quartet_fingerprint(liberi_handle h, uint64_t *out) {
+    if (!h || !out) return fail(LIBERI_E_ARG, "liberi_quartet_fingerprint: null argument");
+    if (!h->initialized) return fail(LIBERI_E_STATE, "liberi_quartet_fingerprint called before liberi_setup");
+    if (h->plan_dirty) return fail(LIBERI_E_STATE, "liberi_quartet_fingerprint: options changed since the last build");
+    DeviceGuard dev_guard(h->device);
+    CUDA_TRY(dev_guard.err);
+    cudaStream_t st = h->stream;
+    unsigned long long *d_out = nullptr;
+    CUDA_TRY(cudaMallocAsync((void **)&d_out, 3 * NKERN * sizeof(unsigned long long), st));
+    cudaError_t e = cudaMemsetAsync(d_out, 0, 3 * NKERN * sizeof(unsigned long long), st);
+    LaunchCtx ctx{};
+    ctx.basis = dev_basis(h);
+    ctx.stream = st;
+    for (int k = 0; k < NKERN && e == cudaSuccess; k++) {
+        const PlanHost &ph = h->plan[k];
+        if (ph.total == 0 || !((h->class_mask >> k) & 1u)) continue;
+        const RankSplit rs = rank_split_of(h, k);
+        DevPlan dp = dev_plan_of(h, k);
+        if (!h->last_split_lists) {
+            e = launch_quartet_fp(k, ctx, dp, rs, d_out + 3 * k);
+            continue;
+        }
+        // the lists the last (mixed-precision) build split and launched
+        dp.ntasks = ph.task_cap;
+        dp.tasks = ph.d_tasks64;
+        dp.ntasks_dev = ph.d_ntasks;
+        e = launch_quartet_fp(k, ctx, dp, rs, d_out + 3 * k);
+        if (e != cudaSuccess) break;
+        dp.tasks = ph.d_tasks32;
+        dp.ntasks_dev = ph.d_ntasks + 1;
+        e = launch_quartet_fp(k, ctx, dp, rs, d_out + 3 * k);
+    }
+    unsigned long long host[3 * NKERN];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, d_out, sizeof(host), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d_out, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    CUDA_TRY(e);
+    for (int i = 0; i < 3 * NKERN; i++) out[i] = host[i];
     return LIBERI_OK;
 }
 

@@ -81,9 +81,79 @@ __global__ void __launch_bounds__(256) split_tasks_kernel(int nitems, const int4
     }
 }
 
+// ---- fingerprint of the evaluated quartet set -------------------------------------
+// Per class {count, sum, xor} of a 64-bit hash of every quartet a launch over
+// the same task list evaluates: the task walk and the rank-ownership test of
+// class_task, the quartet's shells from the plan's pair ids.  The hash is
+// the oracle's quartet_fp (oracle/liberi_oracle.c): unordered shell pairs,
+// unordered pair of pairs, one 64-bit mix; sum and xor do not depend on the
+// order of evaluation.
+__device__ __forceinline__ unsigned long long fp_mix64(unsigned long long x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return x;
+}
+__device__ __forceinline__ unsigned long long quartet_fp(int2 ab, int2 cd) {
+    const unsigned long long a = (unsigned)ab.x, b = (unsigned)ab.y, c = (unsigned)cd.x, d = (unsigned)cd.y;
+    const unsigned long long p1 = a > b ? (a << 16 | b) : (b << 16 | a);
+    const unsigned long long p2 = c > d ? (c << 16 | d) : (d << 16 | c);
+    return fp_mix64(p1 > p2 ? (p1 << 32 | p2) : (p2 << 32 | p1));
+}
+
+__global__ void __launch_bounds__(CLASS_THREADS) quartet_fp_kernel(ClassArgs a, unsigned long long *out) {
+    const int ntasks = a.ntasks_dev ? *a.ntasks_dev : a.ntasks;
+    if ((int)blockIdx.x >= ntasks) return;
+    const int4 t = a.tasks[blockIdx.x];
+    const int2 ab = a.b.pair_shell[a.bra_ids[t.x]];
+    unsigned long long n = 0, sum = 0, x = 0;
+    for (int qi = threadIdx.x; qi < t.z; qi += CLASS_THREADS) {
+        const int j = t.y + qi;
+        if (!quartet_owned(a, t.x, j)) continue;
+        const unsigned long long f = quartet_fp(ab, a.b.pair_shell[a.ket_ids[j]]);
+        n++;
+        sum += f;
+        x ^= f;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        x ^= __shfl_xor_sync(0xffffffffu, x, o);
+    }
+    if ((threadIdx.x & 31) == 0 && n) {
+        atomicAdd(out, n);
+        atomicAdd(out + 1, sum);
+        atomicXor(out + 2, x);
+    }
+}
+
 // ---- launchers -------------------------------------------------------------------
+static ClassArgs single_args(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs, int nbf,
+                             int tile_rows);
+
+cudaError_t launch_quartet_fp(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
+                              unsigned long long *out) {
+    if (plan.ntasks <= 0) return cudaSuccess;
+    const ClassArgs a = single_args(k, ctx, plan, rs, 0, 0);
+    quartet_fp_kernel<<<(unsigned)plan.ntasks, CLASS_THREADS, 0, ctx.stream>>>(a, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs, int precision,
                          int nbf, int tile_rows, int variant) {
+    const ClassArgs a = single_args(k, ctx, plan, rs, nbf, tile_rows);
+#define LIBERI_CASE(kk, A, B, C, D) \
+    case kk: return launch_t<A, B, C, D>(a, precision, variant, ctx.stream);
+    switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
+#undef LIBERI_CASE
+    return cudaErrorInvalidValue;
+}
+
+// kernel arguments of one single-molecule class launch over a plan's task list
+static ClassArgs single_args(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs, int nbf,
+                             int tile_rows) {
     const KernelDesc &kd = KDESC[k];
     ClassArgs a;
     a.b = ctx.basis;
@@ -109,11 +179,7 @@ cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const
     a.rs = rs;
     a.mols = nullptr;
     a.cviews = nullptr;
-#define LIBERI_CASE(kk, A, B, C, D) \
-    case kk: return launch_t<A, B, C, D>(a, precision, variant, ctx.stream);
-    switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
-#undef LIBERI_CASE
-    return cudaErrorInvalidValue;
+    return a;
 }
 
 cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, int ntasks, int nbf_max,

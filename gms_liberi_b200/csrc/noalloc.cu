@@ -11,20 +11,25 @@
 // table from a fixed, file-scope device array instead.
 //
 // Contract:
-//   * LIBERI_NOALLOC_SCRATCH_BYTES (8 MiB) of device memory is reserved by
-//     every GPU that loads the library, from load until process exit;
-//   * the first call on a device looks the array up with
-//     cudaGetSymbolAddress and copies the Rys tables into it, so that first
-//     call should come before any stream capture on that device;
+//   * LIBERI_NOALLOC_SCRATCH_BYTES (8 MiB) of device memory is held by every
+//     GPU on which this entry point has run, until process exit.  CUDA loads
+//     a library's device code lazily by default, so the array is committed
+//     by the first call on each device, not when the library is loaded: a
+//     caller whose pool will claim nearly all of the GPU's memory should make
+//     one call per device at start-up, before the pool does.  If that first
+//     call cannot get the memory it fails with LIBERI_E_NOMEM;
+//   * the first call on a device also loads the module, so it should come
+//     before any stream capture on that device;
 //   * bases whose device data does not fit are rejected (LIBERI_E_NOMEM, the
 //     message states the bytes needed and the limit) before any GPU work;
 //   * no cudaMalloc, cudaFree or other allocating routine is called; work
 //     runs on the legacy default stream and the call returns after the
 //     results have been copied back;
 //   * every call reuses the same array, which keeps the previous call's
-//     contents; the result region is cleared before each launch.  Calls are
-//     serialised by a process-wide lock; uses of the array that overlap on
-//     the GPU (from code that bypasses this entry point) would race.
+//     contents: the Rys tables are copied in and the result region is
+//     cleared on every call.  Calls are serialised by a process-wide lock;
+//     uses of the array that overlap on the GPU (from code that bypasses this
+//     entry point) would race.
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -39,31 +44,31 @@ namespace {
 constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)LIBERI_NOALLOC_SCRATCH_BYTES;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
-unsigned char *g_dev_ptr[MAX_DEVICES] = {};  // device address of the array, per device
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// once per device, with that device current: resolve the array's device
-// address (the host-side symbol is only a stand-in) and load the Rys tables
-int setup_device(int dev, unsigned char **out) {
-    if (g_dev_ptr[dev]) {
-        *out = g_dev_ptr[dev];
-        return LIBERI_OK;
-    }
+// With the caller's device current: the array's device address (the host-side
+// symbol is only a stand-in) and the Rys tables copied into its head.  The
+// address is looked up on every call, never cached: a context that was
+// destroyed and re-created (cudaDeviceReset) gets a new module instance whose
+// array may sit elsewhere and holds no tables.  Once the module is loaded the
+// lookup allocates nothing; the table copy is 0.46 MB.
+int setup_device(unsigned char **out) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-        return set_error(LIBERI_E_DEVICE, (std::string("liberi_schwarz_noalloc: cudaGetSymbolAddress failed: ") +
-                                           cudaGetErrorString(e)).c_str());
+    if (e != cudaSuccess || !p) {
+        // the first use on a device loads the module and commits the array
+        const int code = e == cudaErrorMemoryAllocation ? LIBERI_E_NOMEM : LIBERI_E_DEVICE;
+        return set_error(code, (std::string("liberi_schwarz_noalloc: cudaGetSymbolAddress failed: ") +
+                                cudaGetErrorString(e)).c_str());
+    }
     const std::vector<double> &tab = rys_table_host();
     e = cudaMemcpy(p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
     if (e != cudaSuccess)
         return set_error(LIBERI_E_DEVICE, (std::string("liberi_schwarz_noalloc: table upload failed: ") +
                                            cudaGetErrorString(e)).c_str());
-    g_dev_ptr[dev] = (unsigned char *)p;
-    *out = g_dev_ptr[dev];
+    *out = (unsigned char *)p;
     return LIBERI_OK;
 }
 
@@ -115,14 +120,11 @@ extern "C" int liberi_c_schwarz_noalloc(int32_t nsh, int32_t natoms, int32_t num
         return set_error(LIBERI_E_NOMEM, msg);
     }
     std::lock_guard<std::mutex> lock(g_mu);
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
-        return set_error(LIBERI_E_DEVICE, "liberi_schwarz_noalloc: no usable current device");
     unsigned char *base = nullptr;
-    rc = setup_device(dev, &base);
+    rc = setup_device(&base);
     if (rc) return rc;
     (void)o_tab;
+    cudaError_t e = cudaSuccess;
     std::vector<int> bf0(nsh);
     for (int s = 0; s < nsh; s++) bf0[s] = basis.atom_loc[s] - 1;
     struct Part {

@@ -932,6 +932,21 @@ struct ClassArgs {
     const ClassView *cviews; // batched launch: per-molecule lists of this class
 };
 
+// Does this rank evaluate the quartet (bra position ibra, ket position j) under
+// the reference's rank split?  The flat iteration index of the reference
+// kernel from the positions in its compacted lists (int0001.F90:117,
+// int2211_rysgen.F90:351, triangle kernels by bra position).
+__device__ __forceinline__ bool quartet_owned(const ClassArgs &a, int ibra, int j) {
+    if (a.rs.nsize <= 1) return true;
+    long long bo = a.bra_orig[ibra], ko = a.ket_orig[j];
+    if (a.swapped) { long long tmp = bo; bo = ko; ko = tmp; }
+    long long it;
+    if (a.rs.tri) it = (bo > ko ? bo : ko) + 1;
+    else if (a.rs.ketmajor) it = ko * a.rs.nbra_ref + bo + 1;
+    else it = bo * a.rs.nket_ref + ko + 1;
+    return rank_owns(a.rs, it);
+}
+
 // Per-molecule data of a task.  A single-molecule launch reads the kernel
 // parameters at every use (constant-bank operands, no registers held across
 // the quartet loop); a batched launch reads the task's molecule view (task.w).
@@ -1000,15 +1015,7 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
         const int qi = qb + (threadIdx.x & 31);
         bool act = qi < cnt;
         const int j = k0 + (act ? qi : 0);
-        if (act && a.rs.nsize > 1) {
-            long long bo = a.bra_orig[ibra], ko = a.ket_orig[j];
-            if (a.swapped) { long long tmp = bo; bo = ko; ko = tmp; }
-            long long it;
-            if (a.rs.tri) it = (bo > ko ? bo : ko) + 1;
-            else if (a.rs.ketmajor) it = ko * a.rs.nbra_ref + bo + 1;
-            else it = bo * a.rs.nket_ref + ko + 1;
-            act = rank_owns(a.rs, it);
-        }
+        if (act && a.rs.nsize > 1) act = quartet_owned(a, ibra, j);
         const double4 *krec = mol_ketrec<BATCH>(a, t.w) + KET_REC * j;
         const double4 r0 = ldg_double4(krec), r1 = ldg_double4(krec + 1);
         const double4 C = make_double4(r0.w, r1.x, r1.y, 0.0);

@@ -36,7 +36,8 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_batch_synchronize", "liberi_c_batch_autotune", "liberi_c_batch_destroy",
            "liberi_c_autotune", "liberi_c_rys_eval_f32", "liberi_c_setup_bytes",
            "liberi_c_set_class_variant", "liberi_c_get_class_variant", "liberi_c_mdi_create",
-           "liberi_c_mdi_payload", "liberi_c_mdi_execute", "liberi_c_mdi_destroy"]
+           "liberi_c_mdi_payload", "liberi_c_mdi_execute", "liberi_c_mdi_destroy",
+           "liberi_c_quartet_fingerprint"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -89,6 +90,7 @@ def lib():
                                        _I32P, _I32P, _I32P, _I32P, _I32P,
                                        _F64P, _F64P, _F64P, _F64P, _F64P, _F64P]
         L.liberi_c_get_stats.argtypes = [H, ctypes.POINTER(Stats)]
+        L.liberi_c_quartet_fingerprint.argtypes = [H, ctypes.POINTER(ctypes.c_uint64)]
         L.liberi_c_setup_bytes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                            _I32P, _I32P, _I32P, _I32P, _I32P,
                                            _F64P, _F64P, _F64P, _F64P, _F64P, _F64P, ctypes.c_double,
@@ -177,6 +179,14 @@ class LiberiHandle:
         return {"quartets": np.array(s.quartets[:]), "fp32_quartets": np.array(s.fp32_quartets[:]),
                 "prim_quartets": np.array(s.prim_quartets[:]), "kernel_ms": np.array(s.kernel_ms[:]),
                 "build_ms": s.build_ms, "device_bytes": s.device_bytes}
+
+    def quartet_fingerprint(self):
+        """(21, 3) uint64: per class in driver order the number, sum and xor of
+        the 64-bit hashes of the quartets the last build evaluated (on the
+        device, over the same task lists; see liberi_c_quartet_fingerprint)."""
+        out = (ctypes.c_uint64 * 63)()
+        _check(lib().liberi_c_quartet_fingerprint(self._h, out))
+        return np.array(out[:], dtype=np.uint64).reshape(21, 3)
 
     def destroy(self):
         if self._h:
@@ -436,7 +446,8 @@ def schwarz_noalloc(basis):
     For callers that cannot call cudaMalloc: their device memory is already
     committed to their own pool, or their allocation policy forbids ad-hoc
     cudaMalloc/cudaFree.  The engine's device working memory for this call is
-    a fixed 8 MiB array reserved when the library loads; bases that need more
+    a fixed 8 MiB array, committed by the first call on each device (make that
+    call at start-up, before a pool claims the memory); bases that need more
     raise LiberiError (LIBERI_E_NOMEM) and should use schwarz() instead."""
     (nsh, natoms, nbf, mx, ang, cn, sl, an, al, sb, eb, ex, cs, cp, cd, cf, xyz) = _basis_args(basis)
     k = []

@@ -145,10 +145,12 @@ int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgto
  * cudaMalloc (their device memory is already committed to their own pool, or
  * their allocation policy forbids ad-hoc cudaMalloc/cudaFree).  Its device
  * scratch is one static array of LIBERI_NOALLOC_SCRATCH_BYTES that every GPU
- * loading the library holds until exit; bases that need more are rejected
- * with LIBERI_E_NOMEM before any GPU work.  The first call on a device sets
- * the array up (symbol lookup, table upload) and should come before any
- * stream capture.  Calls are serialised and share the array. */
+ * it has run on holds until exit.  CUDA loads device code lazily, so the
+ * array is committed by the first call on each device (LIBERI_E_NOMEM if that
+ * fails): make that call at start-up, before a pool claims the memory, and
+ * before any stream capture.  Bases that need more scratch are rejected with
+ * LIBERI_E_NOMEM before any GPU work.  Calls are serialised and share the
+ * array; uses that overlap on the GPU would race. */
 #define LIBERI_NOALLOC_SCRATCH_BYTES (8u << 20)
 int liberi_c_schwarz_noalloc(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot,
                              const int32_t *ang_mom, const int32_t *contr_num, const int32_t *sh_loc,
@@ -171,6 +173,22 @@ typedef struct {
     int64_t device_bytes;
 } liberi_stats;
 int liberi_c_get_stats(liberi_handle handle, liberi_stats *stats);
+
+/* Fingerprint of the screened-quartet set, for parity checks.  No counterpart
+ * in the reference (its kernels enumerate the set implicitly: pre-screen and
+ * product test, e.g. int0001.F90:67-121; no product test in
+ * int2222_rysgen.F90:428-436).  For each class in driver order, out[3k+0..2]
+ * = {number of quartets, sum, xor} of a 64-bit hash of every quartet that the
+ * class kernels evaluate for this rank over the task lists of the last build
+ * (the static plan for an FP64 build or before any build; the per-build FP64
+ * and FP32 lists of a mixed-precision build).  The hash of a quartet depends
+ * only on its four shells (0-based), not on pair orientation or bra/ket
+ * order: unordered shell pairs s1<<16|s2 (s1 >= s2), the larger pair key
+ * <<32 | the smaller, mixed by the 64-bit finaliser x ^= x>>33,
+ * x *= 0xff51afd7ed558ccd, x ^= x>>33, x *= 0xc4ceb9fe1a85ec53, x ^= x>>33.
+ * Runs on the device, synchronous; fails if options changed since the last
+ * build (the plan would be rebuilt first). */
+int liberi_c_quartet_fingerprint(liberi_handle handle, uint64_t *out);
 
 /* Device bytes liberi_c_setup would allocate for this basis at this Schwarz
  * cut (host-only dry run of the pair and plan construction, no device

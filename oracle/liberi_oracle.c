@@ -102,8 +102,17 @@ typedef struct {
 /* per kernel: [0] screened shell quartets, [1] primitive quartets evaluated,
  * [2] integrals digested (|v| >= cut), [3] evaluated shell quartets (sample);
  * t_wall[k]: wall seconds of the kernel, t_eval[k]: seconds spent evaluating
- * and digesting quartets summed over threads */
-typedef struct { int64_t c[21][4]; double t_wall[21]; double t_eval[21]; int32_t nthreads; } oracle_counts;
+ * and digesting quartets summed over threads; fp[k]: fingerprint of the
+ * screened-quartet set owned by this rank, {sum, xor} over its quartets of
+ * quartet_fp() (order independent, so any evaluation order gives the same
+ * pair of words; the engine computes the same function over its task lists) */
+typedef struct {
+    int64_t c[21][4];
+    double t_wall[21];
+    double t_eval[21];
+    int32_t nthreads;
+    uint64_t fp[21][2];
+} oracle_counts;
 
 /* ---- pair classes ---------------------------------------------------------- */
 enum { SS = 0, SP, PP, SD, PD, DD, NPC };
@@ -737,6 +746,15 @@ static uint64_t mix64(uint64_t x) {
     return x;
 }
 
+/* 64-bit fingerprint of one shell quartet, independent of the orientation of
+ * each pair and of bra/ket order: shells (0-based, < 65536) form unordered
+ * pair keys, the two pair keys an unordered quartet key, mixed by mix64 */
+static uint64_t quartet_fp(int A, int B, int C, int D) {
+    uint64_t p1 = A > B ? ((uint64_t)A << 16 | (uint64_t)B) : ((uint64_t)B << 16 | (uint64_t)A);
+    uint64_t p2 = C > D ? ((uint64_t)C << 16 | (uint64_t)D) : ((uint64_t)D << 16 | (uint64_t)C);
+    return mix64(p1 > p2 ? (p1 << 32 | p2) : (p2 << 32 | p1));
+}
+
 /* ============================== driver ====================================== */
 int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double *Dm,
                       double *F, oracle_counts *cnt) {
@@ -773,8 +791,9 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
         double dcut = kd->digest_schwarz ? o->schwarz_cut : o->eri_cut;
         int64_t niter = kd->tri ? nbl : nbl * nkl;
         int64_t c_scr = 0, c_prim = 0, c_dig = 0, c_eval = 0;
+        uint64_t fp_sum = 0, fp_xor = 0;
         double t_eval = 0.0, t_k0 = now_s();
-#pragma omp parallel num_threads(nth) reduction(+ : c_scr, c_prim, c_dig, c_eval, t_eval)
+#pragma omp parallel num_threads(nth) reduction(+ : c_scr, c_prim, c_dig, c_eval, t_eval, fp_sum) reduction(^ : fp_xor)
         {
             int tid = 0;
 #ifdef _OPENMP
@@ -797,6 +816,11 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
                     if (kd->op == OP_GE && !(test >= o->schwarz_cut)) continue;
                     if (kd->op == OP_GT && !(test > o->schwarz_cut)) continue;
                     c_scr++;
+                    {
+                        const uint64_t f = quartet_fp(pb->ish[bi], pb->jsh[bi], pk->ish[ki], pk->jsh[ki]);
+                        fp_sum += f;
+                        fp_xor ^= f;
+                    }
                     if (o->sample_mod > 1) {
                         /* sample whole bra pairs (all their kets), so the sampled
                          * work keeps the cache behaviour of a full run */
@@ -818,6 +842,8 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
             cnt->t_wall[kk] = now_s() - t_k0;
             cnt->t_eval[kk] = t_eval;
             cnt->nthreads = nth;
+            cnt->fp[kk][0] = fp_sum;
+            cnt->fp[kk][1] = fp_xor;
         }
         free(lb); free(lk);
     }

@@ -44,7 +44,8 @@ class _Opts(ctypes.Structure):
 
 class _Counts(ctypes.Structure):
     _fields_ = [("c", (ctypes.c_int64 * 4) * 21), ("t_wall", ctypes.c_double * 21),
-                ("t_eval", ctypes.c_double * 21), ("nthreads", ctypes.c_int32)]
+                ("t_eval", ctypes.c_double * 21), ("nthreads", ctypes.c_int32),
+                ("fp", (ctypes.c_uint64 * 2) * 21)]
 
 
 _lib = None
@@ -94,11 +95,13 @@ def _basis_struct(b, keep):
 
 def fock_build(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, my_rank=0,
                num_procs=1, sample_mod=1, sample_seed=0, nthreads=0, only_kernel=-1,
-               return_counts=False, return_times=False):
+               return_counts=False, return_times=False, return_info=False):
     """Packed F (this rank's partial) for packed D; optional per-kernel counts
     [screened quartets, primitive quartets, digested integrals, evaluated] and
     times (wall seconds per kernel, evaluation seconds summed over threads,
-    thread count)."""
+    thread count).  return_info: (F, dict) with "counts", "t_wall", "t_eval",
+    "nthreads" and "fingerprint", a (21, 3) uint64 array per kernel of the
+    screened-quartet set [count, sum, xor] (see quartet_fp in the C file)."""
     keep = []
     bs = _basis_struct(basis, keep)
     n = int(basis["num_bas"])
@@ -114,6 +117,12 @@ def fock_build(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, my_rank=0,
     if rc != 0:
         raise RuntimeError("oracle_fock_build failed: %d" % rc)
     counts = np.array([[cnt.c[k][j] for j in range(4)] for k in range(21)], dtype=np.int64)
+    if return_info:
+        fp = np.zeros((21, 3), dtype=np.uint64)
+        for k in range(21):
+            fp[k] = (np.uint64(counts[k, 0]), np.uint64(cnt.fp[k][0]), np.uint64(cnt.fp[k][1]))
+        return f, {"counts": counts, "t_wall": np.array(cnt.t_wall[:]), "t_eval": np.array(cnt.t_eval[:]),
+                   "nthreads": int(cnt.nthreads), "fingerprint": fp}
     if return_times:
         return f, counts, (np.array(cnt.t_wall[:]), np.array(cnt.t_eval[:]), int(cnt.nthreads))
     if return_counts:

@@ -4,7 +4,8 @@ known-answer vectors and the CPU oracle.
 Tolerances are the ones the reference and its task state:
   * known-answer vectors: max|dF| <= 1e-10 (tests/fortran/test_*.F90:25);
   * plain FP64 path vs the oracle: max|dF| <= 1e-10 and |dE| <= 1e-9 Eh with
-    the same screened-quartet set (per-class counts equal);
+    the same screened-quartet set (per class, the count, sum and xor of a
+    64-bit hash of every quartet the kernels evaluate equal the oracle's);
   * mixed FP32/FP64 path vs the oracle: |dE| <= 1e-6 Eh.
 E here is the two-electron energy functional 1/2 sum_ij D_ij G_ij of the
 symmetrised packed accumulation, identical for both sides.
@@ -38,6 +39,7 @@ def gpu_fock(basis, D, schwrz=None, rank=0, nproc=1, **opts):
     liberi.setup_from_basis(h, basis, schwrz=schwrz, my_rank=rank, num_procs=nproc)
     F = liberi.fock(h, D)
     st = h.stats()
+    st["fingerprint"] = h.quartet_fingerprint()
     liberi.liberi_cleanup(h)
     liberi.liberi_destroy(h)
     return F, st
@@ -97,12 +99,15 @@ def _molecule(name):
 def test_fp64_parity_screened(mol, cut):
     b, nocc = _molecule(mol)
     D = M.density(b["num_bas"], nocc, seed=5)
-    Fo, cnt = oracle.fock_build(b, D, schwarz_cut=cut, return_counts=True)
+    Fo, info = oracle.fock_build(b, D, schwarz_cut=cut, return_info=True)
     Fg, st = gpu_fock(b, D, schwarz_cut=cut)
     assert np.abs(Fg - Fo).max() <= TOL_F
     assert abs(energy(D, Fg) - energy(D, Fo)) <= TOL_E
-    # the same screened-quartet set, class by class
-    assert (st["quartets"] == cnt[:, 0]).all(), (st["quartets"], cnt[:, 0])
+    # the same screened-quartet set, class by class: counts, and the
+    # fingerprint of the quartets the class kernels walk
+    assert (st["quartets"] == info["counts"][:, 0]).all(), (st["quartets"], info["counts"][:, 0])
+    assert (st["fingerprint"] == info["fingerprint"]).all(), (st["fingerprint"], info["fingerprint"])
+
 
 
 def test_identity_and_general_density_kat_basis():
@@ -137,9 +142,11 @@ def test_rank_partials_match_reference_split(nsize):
     full, _ = gpu_fock(b, D, schwarz_cut=1e-10)
     acc = np.zeros_like(full)
     for r in range(nsize):
-        Fg, _ = gpu_fock(b, D, rank=r, nproc=nsize, schwarz_cut=1e-10)
-        Fo = oracle.fock_build(b, D, schwarz_cut=1e-10, my_rank=r, num_procs=nsize)
+        Fg, st = gpu_fock(b, D, rank=r, nproc=nsize, schwarz_cut=1e-10)
+        Fo, info = oracle.fock_build(b, D, schwarz_cut=1e-10, my_rank=r, num_procs=nsize, return_info=True)
         assert np.abs(Fg - Fo).max() <= TOL_F, r
+        # each rank evaluates exactly the reference's share of the quartets
+        assert (st["fingerprint"] == info["fingerprint"]).all(), r
         acc += Fg
     assert np.abs(acc - full).max() <= 1e-11
 
@@ -190,8 +197,11 @@ def test_mixed_precision_error_bound(mol):
     b, nocc = _molecule(mol)
     D = M.density(b["num_bas"], nocc, seed=6)
     Fo = oracle.fock_build(b, D, schwarz_cut=1e-10)
+    _, info = oracle.fock_build(b, D, schwarz_cut=1e-10, sample_mod=1000000, return_info=True)
     for cut in (1e-5, 1e-7):
-        Fm, _ = gpu_fock(b, D, schwarz_cut=1e-10, precision=1, fp32_cut=cut)
+        Fm, st = gpu_fock(b, D, schwarz_cut=1e-10, precision=1, fp32_cut=cut)
+        # the per-build FP64 and FP32 task lists cover the screened set once
+        assert (st["fingerprint"] == info["fingerprint"]).all(), cut
         dE = abs(energy(D, Fm) - energy(D, Fo))
         assert dE <= 1e-6, (cut, dE)
         assert np.abs(Fm - Fo).max() <= 1e-5
