@@ -195,6 +195,217 @@ __device__ __forceinline__ void hrr(const R (&g)[LA + LB + 1][LC + LD + 1], R ab
         }
 }
 
+// ---- (e0|c0) intermediates: contraction before the bra transfer ---------------
+// Cartesian components of angular momentum l <= 4 in a fixed order: the
+// engine's order for l <= 2 (x,y,z; xx,yy,zz,xy,xz,yz), otherwise x exponent
+// descending, then y descending.  Switch tables (not loops), so that the
+// compiler folds them at once inside the unrolled contraction and transfer.
+__host__ __device__ constexpr int cart_x(int l, int i) {
+    if (l <= 2) return cxp(l, i);
+    switch (l * 16 + i) {
+        case 0: return 0;
+        case 16: return 1;
+        case 17: return 0;
+        case 18: return 0;
+        case 32: return 2;
+        case 33: return 0;
+        case 34: return 0;
+        case 35: return 1;
+        case 36: return 1;
+        case 37: return 0;
+        case 48: return 3;
+        case 49: return 2;
+        case 50: return 2;
+        case 51: return 1;
+        case 52: return 1;
+        case 53: return 1;
+        case 54: return 0;
+        case 55: return 0;
+        case 56: return 0;
+        case 57: return 0;
+        case 64: return 4;
+        case 65: return 3;
+        case 66: return 3;
+        case 67: return 2;
+        case 68: return 2;
+        case 69: return 2;
+        case 70: return 1;
+        case 71: return 1;
+        case 72: return 1;
+        case 73: return 1;
+        case 74: return 0;
+        case 75: return 0;
+        case 76: return 0;
+        case 77: return 0;
+        case 78: return 0;
+        default: return 0;
+    }
+}
+__host__ __device__ constexpr int cart_y(int l, int i) {
+    if (l <= 2) return cyp(l, i);
+    switch (l * 16 + i) {
+        case 0: return 0;
+        case 16: return 0;
+        case 17: return 1;
+        case 18: return 0;
+        case 32: return 0;
+        case 33: return 2;
+        case 34: return 0;
+        case 35: return 1;
+        case 36: return 0;
+        case 37: return 1;
+        case 48: return 0;
+        case 49: return 1;
+        case 50: return 0;
+        case 51: return 2;
+        case 52: return 1;
+        case 53: return 0;
+        case 54: return 3;
+        case 55: return 2;
+        case 56: return 1;
+        case 57: return 0;
+        case 64: return 0;
+        case 65: return 1;
+        case 66: return 0;
+        case 67: return 2;
+        case 68: return 1;
+        case 69: return 0;
+        case 70: return 3;
+        case 71: return 2;
+        case 72: return 1;
+        case 73: return 0;
+        case 74: return 4;
+        case 75: return 3;
+        case 76: return 2;
+        case 77: return 1;
+        case 78: return 0;
+        default: return 0;
+    }
+}
+__host__ __device__ constexpr int cart_z(int l, int i) { return l - cart_x(l, i) - cart_y(l, i); }
+// index of the component (x, y, l-x-y) within angular momentum l
+__host__ __device__ constexpr int cart_pos(int l, int x, int y) {
+    if (l == 0) return 0;
+    if (l == 1) return x == 1 ? 0 : (y == 1 ? 1 : 2);
+    if (l == 2) return x == 2 ? 0 : (y == 2 ? 1 : (x + y == 0 ? 2 : (x == 1 && y == 1 ? 3 : (x == 1 ? 4 : 5))));
+    switch (l * 100 + x * 10 + y) {
+        case 0: return 0;
+        case 110: return 0;
+        case 101: return 1;
+        case 100: return 2;
+        case 220: return 0;
+        case 202: return 1;
+        case 200: return 2;
+        case 211: return 3;
+        case 210: return 4;
+        case 201: return 5;
+        case 330: return 0;
+        case 321: return 1;
+        case 320: return 2;
+        case 312: return 3;
+        case 311: return 4;
+        case 310: return 5;
+        case 303: return 6;
+        case 302: return 7;
+        case 301: return 8;
+        case 300: return 9;
+        case 440: return 0;
+        case 431: return 1;
+        case 430: return 2;
+        case 422: return 3;
+        case 421: return 4;
+        case 420: return 5;
+        case 413: return 6;
+        case 412: return 7;
+        case 411: return 8;
+        case 410: return 9;
+        case 404: return 10;
+        case 403: return 11;
+        case 402: return 12;
+        case 401: return 13;
+        case 400: return 14;
+        default: return 0;
+    }
+}
+// Cartesian functions with angular momentum LA..LA+LB, in order of l
+// (closed forms and ternaries, not recursion: the compiler must fold every
+// index below before it places the arrays they address)
+__host__ __device__ constexpr int ncart_upto(int n) { return n < 0 ? 0 : (n + 1) * (n + 2) * (n + 3) / 6; }
+__host__ __device__ constexpr int nrange(int l0, int l1) { return l1 < l0 ? 0 : ncart_upto(l1) - ncart_upto(l0 - 1); }
+__host__ __device__ constexpr int range_pos(int l0, int x, int y, int z) {
+    return nrange(l0, x + y + z - 1) + cart_pos(x + y + z, x, y);
+}
+__host__ __device__ constexpr int binom2(int n, int k) { return (k == 0 || k == n) ? 1 : n; }  // n <= 2
+
+// Classes evaluated as (e0|c0) intermediates: single-pass classes with a
+// p or d second bra shell and an s second ket shell.  The VRR blocks of each
+// root are contracted straight into (e0|c0), e over the Cartesian functions
+// of angular momentum L_A..L_A+L_B (the transfer to (ab|c0) needs only A-B,
+// the same for every primitive), and the bra transfer runs once per quartet
+// instead of once per root: fewer FP64 operations per root and no per-root
+// transfer block held in registers.
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr bool hgp_class(int npass) {
+    return npass == 1 && LB > 0 && LD == 0;
+}
+
+// angular momentum and component of the e-th function of the range starting at l0
+__host__ __device__ constexpr int range_l(int l0, int e) {
+    return e < nrange(l0, l0) ? l0
+         : e < nrange(l0, l0 + 1) ? l0 + 1
+         : e < nrange(l0, l0 + 2) ? l0 + 2
+         : e < nrange(l0, l0 + 3) ? l0 + 3
+                                  : l0 + 4;
+}
+__host__ __device__ constexpr int range_i(int l0, int e) { return e - nrange(l0, range_l(l0, e) - 1); }
+
+// Loop bounds below are compile-time constants (the flat range index e, and
+// transfer exponents up to L_B with guards): a bound that depends on an outer
+// loop index is not fully unrolled, and the arrays it indexes then live in
+// local memory.
+template <int LA, int LB, int LC, typename R>
+__device__ __forceinline__ void contract_hgp(const R (&gx)[LA + LB + 1][LC + 1], const R (&gy)[LA + LB + 1][LC + 1],
+                                             const R (&gz)[LA + LB + 1][LC + 1],
+                                             R (&acc)[nrange(LA, LA + LB)][ncart(LC)]) {
+#pragma unroll
+    for (int e = 0; e < nrange(LA, LA + LB); e++) {
+        const int le = range_l(LA, e), ie = range_i(LA, e);
+#pragma unroll
+        for (int ic = 0; ic < ncart(LC); ic++)
+            acc[e][ic] = fma(gx[cart_x(le, ie)][cxp(LC, ic)] * gy[cart_y(le, ie)][cyp(LC, ic)],
+                             gz[cart_z(le, ie)][czp(LC, ic)], acc[e][ic]);
+    }
+}
+
+// (a b|c0) for A component ia (a compile-time index) from the contracted
+// (e0|c0): (a b| = sum_{t <= b} prod_i binom(b_i, t_i) (A-B)_i^(b_i - t_i) (a+t 0|
+template <int LA, int LB, int LC, typename R>
+__device__ __forceinline__ void bra_transfer(const R (&acc)[nrange(LA, LA + LB)][ncart(LC)], int ia, R abx, R aby,
+                                             R abz, R (&sl)[ncart(LB)][ncart(LC)][1]) {
+    const int ax = cxp(LA, ia), ay = cyp(LA, ia), az = czp(LA, ia);
+    const R px[3] = {R(1), abx, abx * abx}, py[3] = {R(1), aby, aby * aby}, pz[3] = {R(1), abz, abz * abz};
+#pragma unroll
+    for (int ib = 0; ib < ncart(LB); ib++) {
+        const int bx = cxp(LB, ib), by = cyp(LB, ib), bz = czp(LB, ib);
+#pragma unroll
+        for (int ic = 0; ic < ncart(LC); ic++) {
+            R v = R(0);
+#pragma unroll
+            for (int tx = 0; tx <= LB; tx++)
+#pragma unroll
+                for (int ty = 0; ty <= LB; ty++)
+#pragma unroll
+                    for (int tz = 0; tz <= LB; tz++) {
+                        if (tx > bx || ty > by || tz > bz) continue;
+                        const R c = R(binom2(bx, tx) * binom2(by, ty) * binom2(bz, tz)) * px[bx - tx] * py[by - ty] *
+                                    pz[bz - tz];
+                        v = fma(c, acc[range_pos(LA, ax + tx, ay + ty, az + tz)][ic], v);
+                    }
+            sl[ib][ic][0] = v;
+        }
+    }
+}
+
 // ---- contracted Cartesian block of one shell quartet -------------------------
 // Component tables as runtime values (used to select one A component).
 __device__ __forceinline__ int cx_rt(int l, int c) { return l == 0 ? 0 : (l == 1 ? (c == 0) : (c == 0 ? 2 : ((c == 3 || c == 4) ? 1 : 0))); }
@@ -291,17 +502,19 @@ __device__ __forceinline__ void contract_root(const R (&gx)[LA + LB + 1][LC + LD
 // B, C, D.  A single pass (NMU == NA) uses compile-time component indices; a
 // multi-pass class selects the A exponent at run time, so one copy of the
 // primitive loop serves every pass and the root loop is not unrolled.
-template <int LA, int LB, int LC, int LD, typename R, int NMU>
+// HGP: acc is the (e0|c0) block of contract_hgp (L_D = 0, one pass), else the
+// (ab|cd) block of NMU A components.
+template <int LA, int LB, int LC, int LD, typename R, int NMU, bool HGP, typename ACC>
 __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, int q0, int nq,
                                            const double4 &A, const double4 &C, R abx, R aby, R abz,
                                            R cdx, R cdy, R cdz, double thr, bool strict,
                                            const double *__restrict__ tab, const float *__restrict__ tabf,
-                                           int mu0, R (&acc)[NMU][ncart(LB)][ncart(LC)][ncart(LD)],
-                                           R *cache_u, R *cache_w, int cache) {
-    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+                                           int mu0, ACC &acc, R *cache_u, R *cache_w, int cache) {
+    constexpr int NA = ncart(LA);
     constexpr int LAB = LA + LB, LCD = LC + LD;
     constexpr int NR = (LAB + LCD) / 2 + 1;
     constexpr bool FULL = (NMU == NA);
+    static_assert(!HGP || (LD == 0 && FULL), "(e0|c0) contraction: one pass, s second ket shell");
     int ex[NMU], ey[NMU], ez[NMU];
 #pragma unroll
     for (int m = 0; m < NMU; m++) {
@@ -310,14 +523,21 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
         ey[m] = cy_rt(LA, ia);
         ez[m] = cz_rt(LA, ia);
     }
+    if constexpr (HGP) {
 #pragma unroll
-    for (int m = 0; m < NMU; m++)
+        for (int e = 0; e < nrange(LA, LA + LB); e++)
 #pragma unroll
-        for (int ib = 0; ib < NB; ib++)
+            for (int ic = 0; ic < ncart(LC); ic++) acc[e][ic] = R(0);
+    } else {
 #pragma unroll
-            for (int ic = 0; ic < NC; ic++)
+        for (int m = 0; m < NMU; m++)
 #pragma unroll
-                for (int id = 0; id < ND; id++) acc[m][ib][ic][id] = R(0);
+            for (int ib = 0; ib < ncart(LB); ib++)
+#pragma unroll
+                for (int ic = 0; ic < ncart(LC); ic++)
+#pragma unroll
+                    for (int id = 0; id < ncart(LD); id++) acc[m][ib][ic][id] = R(0);
+    }
     int slot = 0;  // primitive quartet index within the shell quartet (root cache)
     if constexpr (std::is_same<R, double>::value) {
         for (int kq = q0; kq < q0 + nq; kq++) {
@@ -370,7 +590,8 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                     vrr<LAB, LCD, R>(gy, R((Pp.y - A.y) - fq * pqy), R((Qp.y - C.y) + fp * pqy), b10, b01, b00, R(1));
                     vrr<LAB, LCD, R>(gz, R((Pp.z - A.z) - fq * pqz), R((Qp.z - C.z) + fp * pqz), b10, b01, b00,
                                      R(wr));
-                    contract_root<LA, LB, LC, LD, R, NMU>(gx, gy, gz, abx, aby, abz, cdx, cdy, cdz, ex, ey, ez, acc);
+                    if constexpr (HGP) contract_hgp<LA, LB, LC, R>(gx, gy, gz, acc);
+                    else contract_root<LA, LB, LC, LD, R, NMU>(gx, gy, gz, abx, aby, abz, cdx, cdy, cdz, ex, ey, ez, acc);
                 }
             }
         }
@@ -425,7 +646,8 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                     vrr<LAB, LCD, R>(gx, Pa.x - fq * pqx, Qa.x + fp * pqx, b10, b01, b00, 1.0f);
                     vrr<LAB, LCD, R>(gy, Pa.y - fq * pqy, Qa.y + fp * pqy, b10, b01, b00, 1.0f);
                     vrr<LAB, LCD, R>(gz, Pa.z - fq * pqz, Qa.z + fp * pqz, b10, b01, b00, wr);
-                    contract_root<LA, LB, LC, LD, R, NMU>(gx, gy, gz, abx, aby, abz, cdx, cdy, cdz, ex, ey, ez, acc);
+                    if constexpr (HGP) contract_hgp<LA, LB, LC, R>(gx, gy, gz, acc);
+                    else contract_root<LA, LB, LC, LD, R, NMU>(gx, gy, gz, abx, aby, abz, cdx, cdy, cdz, ex, ey, ez, acc);
                 }
             }
         }
@@ -522,7 +744,7 @@ constexpr int tuned_minb(int key) {
         case 1000: return 6;
         case 1010: return 4;
         case 1100: return 5;
-        case 1110: return 3;
+        case 1110: return 4;
         case 1111: return 3;
         case 1120: return 2;
         case 2000: return 6;
@@ -655,7 +877,7 @@ constexpr int alt_minb(int key, bool f32, int v) {
         case 10102: return 6;
         case 11001: return 5;
         case 11002: return 6;
-        case 11101: return 4;
+        case 11101: return 3;
         case 21101: return 3;
         default: return 0;
     }
@@ -843,12 +1065,15 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
     constexpr int CAP = CACHE ? ROOT_CACHE_PQ : 1;
     R cache_u[CAP * NR], cache_w[CAP * NR];
     const bool cache_ok = CACHE && np * nq <= CAP;
+    constexpr bool HGP = hgp_class<LA, LB, LC, LD>(PS::NPASS);
 #pragma unroll 1
     for (int pass = 0; pass < PS::NPASS; pass++) {
         const int mu0 = pass * M;
-        R acc[M][NB][NC][ND];
-        eval_block<LA, LB, LC, LD, R, M>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict, tab, tabf,
-                                         mu0, acc, cache_u, cache_w, cache_ok ? (pass == 0 ? 1 : 2) : 0);
+        // (e0|c0) intermediates (HGP) or the (ab|cd) block of this pass's A components
+        using Acc = typename std::conditional<HGP, R[nrange(LA, LA + LB)][NC], R[M][NB][NC][ND]>::type;
+        Acc acc;
+        eval_block<LA, LB, LC, LD, R, M, HGP>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict, tab,
+                                              tabf, mu0, acc, cache_u, cache_w, cache_ok ? (pass == 0 ? 1 : 2) : 0);
         // The J update of the row pair (mu nu) is the same address for every
         // lane of the warp (one bra per CTA): it is summed over the warp and
         // added once.  Every lane reaches the reduction (the quartet loop is
@@ -873,10 +1098,21 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
             const int ia = mu0 + m;
             if (ia >= NA) break;
             R jab[NB];
-            if (distinct)
-                digest_row_distinct<LA, LB, LC, LD, R>(acc[m], ia, qc, dCD, dBD, dBC, rows, kb, jab);
-            else
-                digest_row_general<LA, LB, LC, LD, R>(acc[m], ia, qc, rows, kb, jab);
+            if constexpr (HGP) {
+                // one pass: the component index is the unrolled m (a compile-time
+                // index into acc; the run-time ia would put acc in local memory)
+                R sl[NB][NC][ND];
+                bra_transfer<LA, LB, LC, R>(acc, m, abx, aby, abz, sl);
+                if (distinct)
+                    digest_row_distinct<LA, LB, LC, LD, R>(sl, ia, qc, dCD, dBD, dBC, rows, kb, jab);
+                else
+                    digest_row_general<LA, LB, LC, LD, R>(sl, ia, qc, rows, kb, jab);
+            } else {
+                if (distinct)
+                    digest_row_distinct<LA, LB, LC, LD, R>(acc[m], ia, qc, dCD, dBD, dBC, rows, kb, jab);
+                else
+                    digest_row_general<LA, LB, LC, LD, R>(acc[m], ia, qc, rows, kb, jab);
+            }
 #pragma unroll
             for (int ib = 0; ib < NB; ib++) jab[ib] = warp_sum(jab[ib]);
             if ((threadIdx.x & 31) == 0) {
@@ -1086,7 +1322,7 @@ __device__ __forceinline__ double schwarz_diag(const DevBasis &b, int P, const d
 #pragma unroll 1
     for (int ia = 0; ia < NA; ia++) {
         double acc[1][NB][NA][NB];
-        eval_block<LA, LB, LA, LB, double, 1>(b, p0, np, p0, np, A, A, abx, aby, abz, abx, aby, abz, RYS_TMAX,
+        eval_block<LA, LB, LA, LB, double, 1, false>(b, p0, np, p0, np, A, A, abx, aby, abz, abx, aby, abz, RYS_TMAX,
                                               false, tab, nullptr, ia, acc, nullptr, nullptr, 0);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
