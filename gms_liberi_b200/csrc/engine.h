@@ -80,6 +80,8 @@ struct DevBasis {
     const double2 *prim_X;     // sqrt(2 pi^2.5) c_a c_b exp(-mu R^2) / p, 0.5 / p
     const float4 *prim_PAf;    // FP32 tier, two float4 per primitive pair (one 256-bit load):
                                // (Px, Py, Pz, p), (P - A rounded once from FP64, prefactor)
+    const float *prim_bound;   // per primitive pair sqrt(max |(ab|ab)|) of that primitive alone
+                               // (the FP32 tier's primitive screening), or null
 };
 
 // One launch of a class: a list of CTA tasks (bra position, first ket
@@ -176,6 +178,7 @@ struct DeviceBuffers {
     double4 *prim_P = nullptr;
     double2 *prim_X = nullptr;
     float4 *prim_PAf = nullptr;
+    float *prim_bound = nullptr;
     double *D = nullptr, *F = nullptr;
     double *Dsq = nullptr;  // the build's D as a full n x n matrix (class kernels read it)
     float *Df = nullptr;    // FP32 tier: the same in single precision
@@ -203,6 +206,10 @@ struct LaunchCtx {
     double schwarz_cut, eri_cut;
     cudaStream_t stream;
     int num_sms;
+    // FP32 tier: max|D| of the build (ordered bits; per molecule for batches)
+    // and the primitive screening cut (fp32_prim * fp32_cut; 0 = off)
+    const unsigned long long *maxd = nullptr;
+    double prim_cut = 0.0;
 };
 
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
@@ -234,6 +241,9 @@ cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_
                                int4 *tasks64, int4 *tasks32, int *counts, cudaStream_t stream);
 cudaError_t launch_schwarz(int pair_class, int npairs, int pair_off, const DevBasis &b,
                            const double *rys_tab, double *out_per_pair, cudaStream_t stream);
+// per primitive pair of one pair class: sqrt(max |(ab|ab)|) of the primitive alone, rounded up to float
+cudaError_t launch_prim_bound(int pair_class, int npairs, int pair_off, const DevBasis &b, const double *rys_tab,
+                              float *out_per_prim, cudaStream_t stream);
 
 // host-side inputs of the Schwarz generator (host.cpp) and the thread's
 // last-error message, for the allocation-free entry point (noalloc.cu)

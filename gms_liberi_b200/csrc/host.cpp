@@ -125,6 +125,8 @@ struct liberi_handle_s {
     double schwarz_cut = 5.00000000000000018e-11;  // liberi_parameters.F90:38
     double eri_cut = 5.0e-11;
     double fp32_cut = 1.0e-7;
+    // FP32 tier: primitive quartets with bound * max|D| below fp32_prim * fp32_cut are skipped
+    double fp32_prim = 1.0e-8;
     int precision = 0;
     int device = 0;
     uint32_t class_mask = (1u << NKERN) - 1;
@@ -598,7 +600,8 @@ static size_t basis_device_bytes(const BasisHost &b, const PairsHost &pr) {
            2 * up_bytes(npair, sizeof(int)) + up_bytes(nprim, sizeof(double4)) + up_bytes(nprim, sizeof(double2)) +
            up_bytes(2 * nprim, sizeof(float4)) + up_bytes(RYS_TABLE_SIZE, sizeof(double)) +
            up_bytes(RYSF_TABLE_SIZE, sizeof(float)) + 2 * al_bytes(ntri, sizeof(double)) +
-           al_bytes(nsq, sizeof(double)) + al_bytes(nsq, sizeof(float)) + al_bytes(1, sizeof(unsigned long long));
+           al_bytes(nsq, sizeof(double)) + al_bytes(nsq, sizeof(float)) + al_bytes(1, sizeof(unsigned long long)) +
+           al_bytes(nprim, sizeof(float));
 }
 
 static void compute_stats(liberi_handle h) {
@@ -652,6 +655,8 @@ static int copy_basis(BasisHost &b, int nsh, int natoms, int num_bas, int mxgtot
 
 static size_t basis_device_bytes(const BasisHost &b, const PairsHost &pr);
 
+static DevBasis dev_basis(liberi_handle h);
+
 static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) {
     const BasisHost &b = h->basis;
     CUDA_TRY(arena_open(h, h->arena_basis, basis_device_bytes(b, h->pairs)));
@@ -665,8 +670,52 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
     CUDA_TRY(dev_upload(h, &h->dev.pair_nprim, h->pairs.nprim.data(), h->pairs.nprim.size()));
     CUDA_TRY(dev_upload(h, &h->dev.prim_P, h->pairs.P.data(), h->pairs.P.size()));
     CUDA_TRY(dev_upload(h, &h->dev.prim_X, h->pairs.X.data(), h->pairs.X.size()));
+    const std::vector<double> &tab = rys_table_host();
+    CUDA_TRY(dev_upload(h, &h->d_tab, tab.data(), tab.size()));
+    const std::vector<float> &tabf = rys_table_f32_host();
+    CUDA_TRY(dev_upload(h, &h->d_tabf, tabf.data(), tabf.size()));
+    // Bounds of the single primitive pairs (the FP32 tier's primitive
+    // screening), computed on the device from the pair data and tables; then
+    // every pair's primitives are put in order of decreasing bound, so that
+    // the FP32 loops stop at the first primitive below the cut.  The FP64
+    // sums only change order.
+    PairsHost &pr = h->pairs;
+    const size_t nprim = pr.P.size();
+    CUDA_TRY(dev_alloc(h, &h->dev.prim_bound, nprim));
+    std::vector<float> bound(nprim);
+    if (nprim) {
+        DevBasis db = dev_basis(h);
+        for (int c = 0; c < NPC; c++) {
+            const int o = pr.class_off[c], n = pr.class_off[c + 1] - o;
+            CUDA_TRY(launch_prim_bound(c, n, o, db, h->d_tab, h->dev.prim_bound, h->stream));
+        }
+        CUDA_TRY(cudaMemcpyAsync(bound.data(), h->dev.prim_bound, nprim * sizeof(float), cudaMemcpyDeviceToHost,
+                                 h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        std::vector<int> ord;
+        std::vector<double4> P2(pr.P.size());
+        std::vector<double2> X2(pr.X.size());
+        std::vector<float> bound2(nprim);
+        for (size_t q = 0; q < pr.shell.size(); q++) {
+            const int k0 = pr.prim0[q], n = pr.nprim[q];
+            ord.resize(n);
+            std::iota(ord.begin(), ord.end(), k0);
+            std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return bound[x] > bound[y]; });
+            for (int i = 0; i < n; i++) {
+                P2[k0 + i] = pr.P[ord[i]];
+                X2[k0 + i] = pr.X[ord[i]];
+                bound2[k0 + i] = bound[ord[i]];
+            }
+        }
+        pr.P.swap(P2);
+        pr.X.swap(X2);
+        bound.swap(bound2);
+        CUDA_TRY(cudaMemcpyAsync(h->dev.prim_P, pr.P.data(), nprim * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(cudaMemcpyAsync(h->dev.prim_X, pr.X.data(), nprim * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(cudaMemcpyAsync(h->dev.prim_bound, bound.data(), nprim * sizeof(float), cudaMemcpyHostToDevice,
+                                 h->stream));
+    }
     {  // FP32 tier copies: P - A is formed in FP64 and rounded once
-        const PairsHost &pr = h->pairs;
         std::vector<float4> paf(2 * pr.P.size());
         for (size_t q = 0; q < pr.shell.size(); q++) {
             const double4 A = shell_xyz[pr.shell[q].x];
@@ -678,10 +727,6 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
         }
         CUDA_TRY(dev_upload(h, &h->dev.prim_PAf, paf.data(), paf.size()));
     }
-    const std::vector<double> &tab = rys_table_host();
-    CUDA_TRY(dev_upload(h, &h->d_tab, tab.data(), tab.size()));
-    const std::vector<float> &tabf = rys_table_f32_host();
-    CUDA_TRY(dev_upload(h, &h->d_tabf, tabf.data(), tabf.size()));
     const size_t ntri = (size_t)b.num_bas * (b.num_bas + 1) / 2;
     CUDA_TRY(dev_alloc(h, &h->dev.D, ntri));
     CUDA_TRY(dev_alloc(h, &h->dev.F, ntri));
@@ -689,6 +734,8 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
     CUDA_TRY(dev_alloc(h, &h->dev.Dsq, nsq));
     CUDA_TRY(dev_alloc(h, &h->dev.Df, nsq));
     CUDA_TRY(dev_alloc(h, &h->d_maxd, 1));
+    // the host copies above are pageable: the uploads complete before return
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
     return LIBERI_OK;
 }
 
@@ -702,6 +749,7 @@ static DevBasis dev_basis(liberi_handle h) {
     d.prim_P = h->dev.prim_P;
     d.prim_X = h->dev.prim_X;
     d.prim_PAf = h->dev.prim_PAf;
+    d.prim_bound = h->dev.prim_bound;
     return d;
 }
 
@@ -788,6 +836,8 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     ctx.num_sms = h->num_sms;
     const bool mixed = h->precision == 1;
     ctx.Df = h->dev.Df;
+    ctx.maxd = mixed ? h->d_maxd : nullptr;
+    ctx.prim_cut = mixed ? h->fp32_prim * h->fp32_cut : 0.0;
     // the class kernels read D as a full matrix (and in float for the FP32 tier)
     CUDA_TRY(launch_unpack(dD, b.num_bas, h->dev.Dsq, mixed ? h->dev.Df : nullptr, st));
     if (mixed) CUDA_TRY(launch_maxabs(dD, ntri, h->d_maxd, st));
@@ -962,7 +1012,7 @@ struct liberi_batch_s {
     int chunk[NKERN] = {};
     // mixed precision: every molecule's items per class (w = molecule), per-build task lists
     int precision = 0;
-    double fp32_cut = 0.0;
+    double fp32_cut = 0.0, fp32_prim = 0.0;
     int4 *d_items[NKERN] = {};
     int nitems[NKERN] = {};
     int cap[NKERN] = {};
@@ -1029,6 +1079,8 @@ static int batch_enqueue(liberi_batch b, cudaStream_t st, uint32_t mask) {
     ctx.stream = st;
     ctx.num_sms = h0->num_sms;
     const bool mixed = b->precision == 1;
+    ctx.maxd = mixed ? b->d_maxd : nullptr;
+    ctx.prim_cut = mixed ? b->fp32_prim * b->fp32_cut : 0.0;
     CUDA_TRY(launch_batch_prep(b->d_mols, (int)b->hs.size(), (long long)b->nbf_max * b->nbf_max,
                                mixed ? b->d_maxd : nullptr, st));
     if (!mixed) {
@@ -1278,7 +1330,7 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
         }
         if (h->num_procs != 1 || h->device != handles[0]->device || h->precision != handles[0]->precision ||
             h->schwarz_cut != handles[0]->schwarz_cut || h->eri_cut != handles[0]->eri_cut ||
-            (h->precision == 1 && h->fp32_cut != handles[0]->fp32_cut)) {
+            (h->precision == 1 && (h->fp32_cut != handles[0]->fp32_cut || h->fp32_prim != handles[0]->fp32_prim))) {
             delete b;
             return fail(LIBERI_E_ARG, "liberi_batch_create: handle %d differs in device, rank split, precision or cuts", i);
         }
@@ -1321,6 +1373,7 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
     }
     b->precision = handles[0]->precision;
     b->fp32_cut = handles[0]->fp32_cut;
+    b->fp32_prim = handles[0]->fp32_prim;
     {  // every molecule's D as a full matrix, made per iteration from its packed D
         size_t sqtot = 0;
         for (int m = 0; m < n; m++) {
@@ -1613,6 +1666,9 @@ int liberi_c_set_option(liberi_handle h, const char *name, double value) {
     } else if (n == "fp32_cut") {
         if (!(value >= 0)) return fail(LIBERI_E_ARG, "fp32_cut must be >= 0");
         h->fp32_cut = value;
+    } else if (n == "fp32_prim") {
+        if (!(value >= 0 && value <= 1)) return fail(LIBERI_E_ARG, "fp32_prim must be in [0, 1]");
+        h->fp32_prim = value;
     } else if (n == "precision") {
         if (value != 0 && value != 1) return fail(LIBERI_E_ARG, "precision must be 0 or 1");
         h->precision = (int)value;
@@ -1647,6 +1703,7 @@ int liberi_c_get_option(liberi_handle h, const char *name, double *value) {
     if (n == "schwarz_cut") *value = h->schwarz_cut;
     else if (n == "eri_cut") *value = h->eri_cut;
     else if (n == "fp32_cut") *value = h->fp32_cut;
+    else if (n == "fp32_prim") *value = h->fp32_prim;
     else if (n == "precision") *value = h->precision;
     else if (n == "device") *value = h->device;
     else if (n == "class_mask") *value = h->class_mask;

@@ -23,7 +23,24 @@ __global__ void __launch_bounds__(64) schwarz_kernel(DevBasis b, int pair_off, i
                                                      const double *tab, double *out) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= npairs) return;
-    out[t] = schwarz_diag<LA, LB>(b, pair_off + t, tab);
+    const int P = pair_off + t;
+    out[t] = schwarz_diag<LA, LB>(b, P, tab, b.pair_prim0[P], b.pair_nprim[P]);
+}
+
+// Primitive-pair bounds: for every kept primitive pair k of pair P,
+// sqrt(max |(ab|ab)|) of that primitive alone (with its contraction
+// coefficients), rounded up to float: |(ab|cd)_prim| <= out[k] * out[l].
+template <int LA, int LB>
+__global__ void __launch_bounds__(64) prim_bound_kernel(DevBasis b, int pair_off, int npairs, const double *tab,
+                                                        float *out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npairs) return;
+    const int P = pair_off + t;
+    const int p0 = b.pair_prim0[P], np = b.pair_nprim[P];
+    for (int k = p0; k < p0 + np; k++) {
+        const double v = schwarz_diag<LA, LB>(b, P, tab, k, 1);
+        out[k] = __double2float_ru(v * (1.0 + 1e-6));
+    }
 }
 
 __global__ void maxabs_kernel(const double *x, long long n, unsigned long long *out) {
@@ -79,6 +96,23 @@ __global__ void __launch_bounds__(256) split_tasks_kernel(int nitems, const int4
         for (int k = s; k < it.z; k += chunk) tasks32[o++] = make_int4(it.x, it.y + k, min(chunk, it.z - k), w);
         atomicAdd(reinterpret_cast<unsigned long long *>(counts + 2), (unsigned long long)(it.z - s));
     }
+}
+
+cudaError_t launch_prim_bound(int pc, int npairs, int pair_off, const DevBasis &b, const double *tab, float *out,
+                              cudaStream_t st) {
+    if (npairs <= 0) return cudaSuccess;
+    const int threads = 64;
+    const unsigned blocks = (unsigned)((npairs + threads - 1) / threads);
+    switch (pc) {
+        case SS: prim_bound_kernel<0, 0><<<blocks, threads, 0, st>>>(b, pair_off, npairs, tab, out); break;
+        case SP: prim_bound_kernel<1, 0><<<blocks, threads, 0, st>>>(b, pair_off, npairs, tab, out); break;
+        case PP: prim_bound_kernel<1, 1><<<blocks, threads, 0, st>>>(b, pair_off, npairs, tab, out); break;
+        case SD: prim_bound_kernel<2, 0><<<blocks, threads, 0, st>>>(b, pair_off, npairs, tab, out); break;
+        case PD: prim_bound_kernel<2, 1><<<blocks, threads, 0, st>>>(b, pair_off, npairs, tab, out); break;
+        case DD: prim_bound_kernel<2, 2><<<blocks, threads, 0, st>>>(b, pair_off, npairs, tab, out); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 // ---- fingerprint of the evaluated quartet set -------------------------------------
@@ -179,6 +213,8 @@ static ClassArgs single_args(int k, const LaunchCtx &ctx, const DevPlan &plan, c
     a.rs = rs;
     a.mols = nullptr;
     a.cviews = nullptr;
+    a.maxd = ctx.maxd;
+    a.prim_cut = ctx.prim_cut;
     return a;
 }
 
@@ -209,6 +245,8 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     a.rs = RankSplit{0, 1, 0, 0, 0, 0, 0, 0};
     a.mols = d_mols;
     a.cviews = d_cviews;
+    a.maxd = ctx.maxd;
+    a.prim_cut = ctx.prim_cut;
 #define LIBERI_CASE(kk, A, B, C, D) \
     case kk: return launch_t<A, B, C, D>(a, precision, 0, ctx.stream);
     switch (k) { LIBERI_CLASSES(LIBERI_CASE) }

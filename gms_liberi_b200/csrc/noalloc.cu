@@ -156,6 +156,7 @@ extern "C" int liberi_c_schwarz_noalloc(int32_t nsh, int32_t natoms, int32_t num
     db.prim_P = (const double4 *)(base + o_P);
     db.prim_X = (const double2 *)(base + o_X);
     db.prim_PAf = nullptr;  // the Schwarz kernels are FP64 only
+    db.prim_bound = nullptr;
     const double *tab = (const double *)(base + o_tab);
     for (int c = 0; c < NPC && e == cudaSuccess; c++) {
         const int o = pairs.class_off[c], n = pairs.class_off[c + 1] - o;

@@ -509,7 +509,8 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                                            const double4 &A, const double4 &C, R abx, R aby, R abz,
                                            R cdx, R cdy, R cdz, double thr, bool strict,
                                            const double *__restrict__ tab, const float *__restrict__ tabf,
-                                           int mu0, ACC &acc, R *cache_u, R *cache_w, int cache) {
+                                           int mu0, ACC &acc, R *cache_u, R *cache_w, int cache,
+                                           float pthr = 0.f, float bpmax = 0.f) {
     constexpr int NA = ncart(LA);
     constexpr int LAB = LA + LB, LCD = LC + LD;
     constexpr int NR = (LAB + LCD) / 2 + 1;
@@ -599,11 +600,19 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
         // FP32 tier: pair data, roots and recurrences in single precision
         const float *__restrict__ PAf = reinterpret_cast<const float *>(b.prim_PAf);
         const float thrf = (float)thr;
+        // Primitive screening of the FP32 tier: a primitive quartet whose
+        // Schwarz bound bp*bq is below pthr (fp32_prim * fp32_cut / max|D|,
+        // far below the rounding error of this tier's quartets) is skipped.
+        // Every pair's primitives are stored by decreasing bound, so both
+        // loops end at the first primitive below the cut.
         for (int kq = q0; kq < q0 + nq; kq++) {
+            const float bq = pthr > 0.f ? __ldg(b.prim_bound + kq) : 1.f;
+            if (bq * bpmax < pthr) break;
             float4 Qp, Qa;
             ldg_v8f32(PAf + 8 * (size_t)kq, Qp, Qa);
             const float q = Qp.w, hq = __fdividef(0.5f, q);
             for (int kp = p0; kp < p0 + np; kp++) {
+                if (pthr > 0.f && __ldg(b.prim_bound + kp) * bq < pthr) break;
                 float4 Pp, Pa;
                 ldg_v8f32(PAf + 8 * (size_t)kp, Pp, Pa);
                 const float p = Pp.w, hp = __fdividef(0.5f, p);
@@ -1051,7 +1060,7 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
                                            const double4 &C, R abx, R aby, R abz, R cdx, R cdy, R cdz,
                                            double thr, bool strict, const double *__restrict__ tab,
                                            const float *__restrict__ tabf, const QuartetCtx<R> &qc,
-                                           const Rows<R> &rows, KB &kb) {
+                                           const Rows<R> &rows, KB &kb, float pthr, float bpmax) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     using PS = PassShape<LA, LB, LC, LD, R, V>;
     constexpr int M = PS::NMU;
@@ -1073,7 +1082,8 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
         using Acc = typename std::conditional<HGP, R[nrange(LA, LA + LB)][NC], R[M][NB][NC][ND]>::type;
         Acc acc;
         eval_block<LA, LB, LC, LD, R, M, HGP>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict, tab,
-                                              tabf, mu0, acc, cache_u, cache_w, cache_ok ? (pass == 0 ? 1 : 2) : 0);
+                                              tabf, mu0, acc, cache_u, cache_w, cache_ok ? (pass == 0 ? 1 : 2) : 0,
+                                              pthr, bpmax);
         // The J update of the row pair (mu nu) is the same address for every
         // lane of the warp (one bra per CTA): it is summed over the warp and
         // added once.  Every lane reaches the reduction (the quartet loop is
@@ -1166,6 +1176,8 @@ struct ClassArgs {
     RankSplit rs;
     const MolView *mols;     // batched launch: per-molecule data (task.w), else null
     const ClassView *cviews; // batched launch: per-molecule lists of this class
+    const unsigned long long *maxd;  // FP32 tier: max|D| bits (per molecule for batches)
+    double prim_cut;                 // FP32 tier: primitive screening cut (0 = off)
 };
 
 // Does this rank evaluate the quartet (bra position ibra, ket position j) under
@@ -1243,6 +1255,18 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     Rows<R> rowsB{use_tile ? tile + NA * LIBERI_NBF : nullptr, LIBERI_F, LIBERI_NBF};
     const R abx = R(A.x - B.x), aby = R(A.y - B.y), abz = R(A.z - B.z);
     const int p0 = bas.pair_prim0[P], np = bas.pair_nprim[P];
+    // FP32 tier: the task's primitive screening threshold and the largest
+    // primitive bound of its bra pair (its first primitive)
+    float pthr = 0.f, bpmax = 0.f;
+    if constexpr (std::is_same<R, float>::value) {
+        if (a.prim_cut > 0.0 && a.maxd && bas.prim_bound) {
+            const double md = __longlong_as_double((long long)a.maxd[BATCH ? t.w : 0]);
+            if (md > 0.0 && np > 0) {
+                pthr = (float)(a.prim_cut / md);
+                bpmax = __ldg(bas.prim_bound + p0);  // primitives in order of decreasing bound
+            }
+        }
+    }
     // Warp-uniform loop: every lane of a warp runs the same iterations (the
     // digestion sums the row pair's J over the warp); a lane past the end of
     // the task, or holding a quartet of another rank, evaluates no primitives
@@ -1270,7 +1294,7 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
 #pragma unroll
         for (int i = 0; i < KBuf<NB, NC, ND, SM, R>::N; i++) kb.at(i) = R(0);
         run_passes<LA, LB, LC, LD, R, V>(bas, p0, np, (int)(unsigned)kpr, act ? (int)(unsigned)(kpr >> 32) : 0, A, C, abx, aby,
-                                      abz, cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb);
+                                      abz, cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb, pthr, bpmax);
 #pragma unroll
         for (int ib = 0; ib < NB; ib++) {
 #pragma unroll
@@ -1311,13 +1335,14 @@ __global__ void __launch_bounds__(CLASS_THREADS, PassShape<LA, LB, LC, LD, R, V>
 }
 
 // sqrt(max |(ab|ab)|) over the components of one pair, for the Schwarz table.
+// (primitive pairs p0 .. p0+np-1 of pair P: all of them for the pair's
+// Schwarz value, one for the bound of a single primitive pair)
 template <int LA, int LB>
-__device__ __forceinline__ double schwarz_diag(const DevBasis &b, int P, const double *tab) {
+__device__ __forceinline__ double schwarz_diag(const DevBasis &b, int P, const double *tab, int p0, int np) {
     constexpr int NA = ncart(LA), NB = ncart(LB);
     const int2 sab = b.pair_shell[P];
     const double4 A = b.shell_xyz[sab.x], B = b.shell_xyz[sab.y];
     const double abx = A.x - B.x, aby = A.y - B.y, abz = A.z - B.z;
-    const int p0 = b.pair_prim0[P], np = b.pair_nprim[P];
     double m = 0.0;
 #pragma unroll 1
     for (int ia = 0; ia < NA; ia++) {

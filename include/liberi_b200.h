@@ -96,6 +96,12 @@ int liberi_c_last_error(char *buf, int32_t len);
  *   "eri_cut"      (5e-11, the digestion literal, e.g. int0002.F90:403)
  *   "fp32_cut"     (1e-7; quartets with xint_ab*xint_cd*max|D| below it run
  *                   in FP32 when "precision" is 1)
+ *   "fp32_prim"    (1e-8; inside those FP32 quartets, a primitive quartet
+ *                   whose Schwarz bound b_ab*b_cd*max|D| is below
+ *                   fp32_prim*fp32_cut is skipped: each skipped contribution
+ *                   to F is below 1e-8 of the cut, about the tier's own
+ *                   rounding error; 0 keeps every primitive; FP64 quartets
+ *                   never skip primitives)
  *   "precision"    (0 = all FP64, 1 = mixed FP32/FP64)
  *   "device"       (CUDA device ordinal used by the next setup, default 0)
  *   "class_mask"   (bit k set = run class k of the driver order; default all 21)
