@@ -48,11 +48,11 @@ def parse_args():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--per-class", action="store_true", help="add per-class device ms to the JSON line")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-molecule batched SCF section")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop section")
-    ap.add_argument("--serve-rate", type=float, default=50.0, help="Poisson build-request rate (req/s)")
-    ap.add_argument("--serve-sessions", type=int, default=12, help="SCF sessions (15 builds each) served")
+    ap.add_argument("--serve-rates", type=str, default="50,100,200,500",
+                    help="Poisson build-request rates (req/s) of the serving capacity curve")
+    ap.add_argument("--serve-sessions", type=int, default=40, help="SCF sessions (15 builds each) served per rate")
     return ap.parse_args()
 
 
@@ -315,18 +315,31 @@ def run_ours(args):
     _, cls_ms = timed_loop(max(3, args.steps // 2), per_class=True)
     h.set_option("timing", 0)
 
-    # roofline of the dominant class kernel
+    # roofline of the dominant class kernel: numerator = operations of the
+    # reference algorithm (flop_constants.json, the oracle's op-counting
+    # build); the engine's own arithmetic as a second figure
     k_dom = int(np.argmax(cls_ms))
     kname = liberi.KERNELS[k_dom]
-    fl = flops.class_flops(k_dom, int(st0["prim_quartets"][k_dom]), int(st0["quartets"][k_dom]))
+    npq, nsq = int(st0["prim_quartets"][k_dom]), int(st0["quartets"][k_dom])
+    fl = flops.class_flops(k_dom, npq, nsq)
+    fl_eng = flops.engine_class_flops(k_dom, npq, nsq)
     peak_fp64 = liberi.microbench(0)
-    achieved = fl / (cls_ms[k_dom] * 1e-3) / 1e12
+    t_dom = cls_ms[k_dom] * 1e-3
+    achieved = fl / t_dom / 1e12
     build_tf = flops.build_flops(st0) / (ms_local * 1e-3) / 1e12
+    build_tf_eng = flops.engine_build_flops(st0) / (ms_local * 1e-3) / 1e12
     roofline = {"bound": "fp64", "kernel": "class_kernel<%s>" % kname, "achieved": round(achieved, 3),
                 "peak": round(peak_fp64, 3), "unit": "TFLOP/s", "frac": round(achieved / peak_fp64, 4),
-                "peak_source": "measured FP64 FMA throughput on this GPU (liberi_c_microbench 0)",
+                "numerator": "operations of the reference algorithm per primitive and shell quartet "
+                             "(gms_liberi_b200/flop_constants.json, oracle op-counting build) x exact counts",
+                "peak_source": "measured FP64 FMA throughput on this GPU (liberi_c_microbench 0); "
+                               "MEASURED_PEAKS.json carries no FP64 figure",
                 "traffic": traffic_per_launch(kname), "share": round(float(cls_ms[k_dom] / cls_ms.sum()), 3),
-                "build_achieved_tflops": round(build_tf, 3)}
+                "engine_count": {"achieved": round(fl_eng / t_dom / 1e12, 3),
+                                 "frac": round(fl_eng / t_dom / 1e12 / peak_fp64, 4),
+                                 "note": "the engine's own arithmetic (gms_liberi_b200/flops.py engine_costs)"},
+                "build_achieved_tflops": round(build_tf, 3), "build_achieved_tflops_engine_count": round(build_tf_eng, 3),
+                "per_class_ms": {liberi.KERNELS[k]: round(float(cls_ms[k]), 3) for k in range(21)}}
 
     # end to end through the public API with host buffers
     pin_D = torch.from_numpy(Dh).pin_memory()
@@ -367,6 +380,8 @@ def run_ours(args):
     if not args.no_mixed:
         h.set_option("precision", 1)
         sweep = []
+        mixed_roofline = None
+        peak_fp32 = liberi.microbench(1)
         # the configured sweep is 1e-5..1e-8; 1e-2..1e-4 are added to
         # locate the loosest cut that still meets |dE| <= 1e-6 Eh
         for cut in (1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8):
@@ -381,11 +396,33 @@ def run_ours(args):
             sweep.append({"fp32_cut": cut, "ms": round(m_ms, 3), "speedup_vs_fp64": round(ms / m_ms, 3),
                           "fp32_quartet_share": round(f32, 4),
                           "max_dF_vs_fp64": dF, "dE_vs_fp64": dE})
+            if cut == 1e-5:
+                # FP32+FP64 roofline of the mixed build: the time the reference-
+                # algorithm operations would take at the measured FP64 and FP32
+                # peaks (each class's operations split between the tiers by its
+                # FP32 quartet share) over the measured time
+                t_ideal = 0.0
+                for k in range(21):
+                    q = float(st_m["quartets"][k])
+                    if q <= 0:
+                        continue
+                    s32 = float(st_m["fp32_quartets"][k]) / q
+                    w = flops.class_flops(k, int(st0["prim_quartets"][k]), int(st0["quartets"][k]))
+                    t_ideal += w * (1.0 - s32) / (peak_fp64 * 1e12) + w * s32 / (peak_fp32 * 1e12)
+                mixed_roofline = {"fp32_cut": cut, "ideal_ms": round(t_ideal * 1e3, 3), "ms": round(m_ms, 3),
+                                  "frac": round(t_ideal * 1e3 / m_ms, 4), "peak_fp64_tflops": round(peak_fp64, 3),
+                                  "peak_fp32_tflops": round(peak_fp32, 3),
+                                  "note": "reference-algorithm operations; tiers split by FP32 quartet share"}
         h.set_option("precision", 0)
         ok = [s for s in sweep if s["dE_vs_fp64"] <= 1e-6]
         best = max(ok, key=lambda s: s["speedup_vs_fp64"]) if ok else None
-        mixed = {"reference_path": "plain FP64 GPU build (parity-tested against the oracle to 1e-10)",
-                 "best_within_dE_1e-6": best, "sweep": sweep}
+        conf = [s for s in ok if 1e-8 <= s["fp32_cut"] <= 1e-5]
+        best_conf = max(conf, key=lambda s: s["speedup_vs_fp64"]) if conf else None
+        mixed = {"reference_path": "plain FP64 GPU build (parity-tested against the oracle: max|dF| 3e-12, "
+                                   "|dE| < 1e-11 on this workload)",
+                 "fp32_prim": h.get_option("fp32_prim"),
+                 "best_in_configured_sweep_1e-5_1e-8": best_conf, "best_within_dE_1e-6": best,
+                 "roofline_fp32_fp64": mixed_roofline, "sweep": sweep}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -404,7 +441,11 @@ def run_ours(args):
         batched = {"fp64": run_batched(dev, stream, 0), "mixed": run_batched(dev, stream, 1)}
     serve = None
     if world == 1 and not args.no_serve:
-        serve = run_serve(local, args.serve_rate, args.serve_sessions)
+        curve = [run_serve(local, float(r), args.serve_sessions) for r in args.serve_rates.split(",") if r]
+        serve = {"curve": curve,
+                 "summary": [{k: c[k] for k in ("rate_req_per_s", "builds_per_s", "latency_ms_p50", "latency_ms_p99",
+                                                 "peak_device_bytes_measured", "peak_concurrent_sessions")}
+                             for c in curve]}
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
@@ -417,8 +458,6 @@ def run_ours(args):
                 "gpu_launches": launched * args.steps, "roofline": roofline, "cpu_baseline": cpu,
                 "mixed": mixed, "batched": batched, "serve": serve,
                 "quartets": int(st0["quartets"].sum()), "prim_quartets": int(st0["prim_quartets"].sum())}
-        if args.per_class:
-            line["per_class_ms"] = {liberi.KERNELS[k]: round(float(cls_ms[k]), 3) for k in range(21)}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -524,6 +563,9 @@ def run_batched(dev, stream, precision=0):
                       "(all molecules' data fits in L2 as it would across SCF iterations)"}
 
 
+_SERVE_POOL = None
+
+
 def run_serve(local, rate, nsessions):
     """Serving loop: SCF sessions (15 Fock builds each, D perturbed by 1e-3
     seeded noise between builds) of molecules drawn from a seeded pool of
@@ -535,13 +577,17 @@ def run_serve(local, rate, nsessions):
     from gms_liberi_b200 import molecules as M
     from gms_liberi_b200.serve import FockServer, LiberiEngine, poisson_sessions
 
-    rng = np.random.default_rng(77)
-    pool = []
-    for i, n in enumerate(rng.integers(10, 201, 8)):
-        b = M.random_molecule(int(n), seed=500 + i)
-        b["schwrz"] = liberi.schwarz(b)
-        pool.append(b)
-    dens = [M.density(b["num_bas"], M.nocc_of(b), seed=900 + k) for k, b in enumerate(pool)]
+    global _SERVE_POOL
+    if _SERVE_POOL is None:  # the same seeded pool for every rate of the curve
+        rng = np.random.default_rng(77)
+        pool = []
+        for i, n in enumerate(rng.integers(10, 201, 8)):
+            b = M.random_molecule(int(n), seed=500 + i)
+            b["schwrz"] = liberi.schwarz(b)
+            pool.append(b)
+        dens = [M.density(b["num_bas"], M.nocc_of(b), seed=900 + k) for k, b in enumerate(pool)]
+        _SERVE_POOL = (pool, dens)
+    pool, dens = _SERVE_POOL
     sessions = poisson_sessions(pool, rate, nsessions, niter=15, seed=5, densities=dens)
     free0, total = torch.cuda.mem_get_info(local)
     peak = [0]

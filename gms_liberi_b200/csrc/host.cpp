@@ -127,6 +127,8 @@ struct liberi_handle_s {
     double fp32_cut = 1.0e-7;
     // FP32 tier: primitive quartets with bound * max|D| below fp32_prim * fp32_cut are skipped
     double fp32_prim = 1.0e-8;
+    // device bytes a setup may take (0: no limit); checked on the host before any device work
+    double max_device_bytes = 0.0;
     int precision = 0;
     int device = 0;
     uint32_t class_mask = (1u << NKERN) - 1;
@@ -1250,6 +1252,20 @@ int liberi_c_setup(liberi_handle h, int32_t nsh, int32_t natoms, int32_t num_bas
     if (rc) return rc;
     rc = validate_basis(b);
     if (rc) return rc;
+    if (h->max_device_bytes > 0.0) {
+        // the caller's device-memory limit, from the host half of setup (the
+        // same dry run as liberi_c_setup_bytes, with this handle's plan options)
+        PairsHost pr;
+        std::vector<double4> sx;
+        build_pairs(b, pr, sx);
+        size_t need = basis_device_bytes(b, pr);
+        std::vector<PlanHost> plans(NKERN);
+        build_plans(pr, h->schwarz_cut, h->chunk, h->rank_split, my_rank, num_procs, plans.data());
+        for (int k = 0; k < NKERN; k++) need += plan_device_bytes(plans[k]);
+        if ((double)need > h->max_device_bytes)
+            return fail(LIBERI_E_NOMEM, "liberi_setup: needs %zu device bytes, above max_device_bytes = %.0f", need,
+                        h->max_device_bytes);
+    }
     DeviceGuard dev_guard(h->device);
     CUDA_TRY(dev_guard.err);
     cudaDeviceProp prop;
@@ -1666,6 +1682,9 @@ int liberi_c_set_option(liberi_handle h, const char *name, double value) {
     } else if (n == "fp32_cut") {
         if (!(value >= 0)) return fail(LIBERI_E_ARG, "fp32_cut must be >= 0");
         h->fp32_cut = value;
+    } else if (n == "max_device_bytes") {
+        if (!(value >= 0)) return fail(LIBERI_E_ARG, "max_device_bytes must be >= 0");
+        h->max_device_bytes = value;
     } else if (n == "fp32_prim") {
         if (!(value >= 0 && value <= 1)) return fail(LIBERI_E_ARG, "fp32_prim must be in [0, 1]");
         h->fp32_prim = value;
@@ -1704,6 +1723,7 @@ int liberi_c_get_option(liberi_handle h, const char *name, double *value) {
     else if (n == "eri_cut") *value = h->eri_cut;
     else if (n == "fp32_cut") *value = h->fp32_cut;
     else if (n == "fp32_prim") *value = h->fp32_prim;
+    else if (n == "max_device_bytes") *value = h->max_device_bytes;
     else if (n == "precision") *value = h->precision;
     else if (n == "device") *value = h->device;
     else if (n == "class_mask") *value = h->class_mask;

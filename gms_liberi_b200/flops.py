@@ -1,25 +1,51 @@
-"""Algorithmic FP64 operation counts of the engine's quartet kernels.
+"""Algorithmic operation counts of the Fock build, the roofline numerator.
 
-The roofline numerator of a class kernel is
+For a class kernel
     FLOPs = N_prim * c_prim(class) + N_shell * c_shell(class)
 where N_prim / N_shell are the exact primitive / shell quartet counts of the
-plan (liberi_c_get_stats) and the per-unit costs below count the arithmetic
-the algorithm needs (add, mul and FMA as 2, one op each for sqrt and
-division), mirroring the loop structure of csrc/quartet.cuh:
-  per primitive quartet: pair geometry and T, Rys roots and weights
-  (2n polynomials of degree 7), per root the recurrence coefficients, the
-  2D vertical recurrence, the horizontal transfer on both sides and the
-  assembly of the Cartesian block (two multiplies and one add per integral);
-  per shell quartet: DIRFCK digestion, 6 multiply-adds per integral plus the
-  normalisation and the cut test.
+plan (liberi_c_get_stats).  Two sets of per-unit costs:
+
+  * reference algorithm (the primary figure): c_prim and c_shell frozen in
+    flop_constants.json beside this file, counted by the oracle's op-counting
+    build on the C60 benchmark workload (oracle/make_flop_constants.py): the
+    operations of the restated reference algorithm -- Boys-moment Rys rules
+    for the rotated-axis classes, the 35-point Stieltjes procedure and
+    Golub-Welsch step per primitive quartet for the Rys classes, recurrences,
+    assembly and DIRFCK digestion; one operation each for add, subtract,
+    multiply, divide, exp, sqrt, acos and cos.  Redundant work in the engine
+    therefore cannot raise this figure.
+  * engine count (secondary): the arithmetic of the engine's own loops
+    (csrc/quartet.cuh), add, mul and FMA as 2: per primitive quartet the pair
+    geometry and T, the Rys roots and weights (2n polynomials of degree 7), per
+    root the recurrence coefficients, the 2D vertical recurrence, the
+    horizontal transfer and the assembly; per shell quartet the digestion.
 """
+import json
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+KERNELS = ["int0000", "int0001", "int0011", "int0111", "int0101", "int1111",
+           "int0002", "int0012", "int0102", "int0112", "int0022", "int0122",
+           "int1102", "int0202", "int2211", "int2121", "int2120", "int2111",
+           "int2220", "int2221", "int2222"]
+_REF = None
+
+
+def reference_constants():
+    """{class name: (c_prim, c_shell)} of the reference algorithm."""
+    global _REF
+    if _REF is None:
+        with open(os.path.join(_HERE, "flop_constants.json")) as f:
+            d = json.load(f)
+        _REF = {k: (v["c_prim"], v["c_shell"]) for k, v in d["classes"].items()}
+    return _REF
 
 
 def ncart(l):
     return (l + 1) * (l + 2) // 2
 
 
-def class_costs(la, lb, lc, ld):
+def engine_costs(la, lb, lc, ld):
     lab, lcd = la + lb, lc + ld
     n = (lab + lcd) // 2 + 1
     nc = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
@@ -51,9 +77,20 @@ CLASS_L = [(0, 0, 0, 0), (0, 0, 1, 0), (0, 0, 1, 1), (1, 0, 1, 1), (1, 0, 1, 0),
 
 
 def class_flops(k, n_prim, n_shell):
-    c_prim, c_shell = class_costs(*CLASS_L[k])
+    """Reference-algorithm operations of class k (driver order)."""
+    c_prim, c_shell = reference_constants()[KERNELS[k]]
+    return n_prim * c_prim + n_shell * c_shell
+
+
+def engine_class_flops(k, n_prim, n_shell):
+    """The engine's own arithmetic for class k."""
+    c_prim, c_shell = engine_costs(*CLASS_L[k])
     return n_prim * c_prim + n_shell * c_shell
 
 
 def build_flops(stats):
     return sum(class_flops(k, int(stats["prim_quartets"][k]), int(stats["quartets"][k])) for k in range(21))
+
+
+def engine_build_flops(stats):
+    return sum(engine_class_flops(k, int(stats["prim_quartets"][k]), int(stats["quartets"][k])) for k in range(21))

@@ -15,7 +15,12 @@ updated between builds.  Sessions arrive over time; the server
     batching: new sessions join while others are in flight);
   * records, per build, the latency from its request (session arrival for the
     first build, completion of the previous build afterwards) to the moment
-    its F is complete.
+    its F is complete;
+  * cancels sessions on request (`cancel(sid)` from any thread, or a
+    session's scripted `cancel_at` time): a queued session leaves the queue
+    without being set up; an admitted one finishes the build it has on the
+    GPU (device work is not aborted), launches no more and releases its
+    memory.
 
 The scheduling logic is independent of the engine (`Engine` below), so it is
 tested on the CPU with a fake engine; `LiberiEngine` drives the CUDA library.
@@ -46,6 +51,9 @@ class Session:
     admitted_at: float = -1.0
     ready_at: float = -1.0      # setup finished
     waited: bool = False        # found the slots or the HBM budget full on arrival
+    waited_bytes: bool = False  # held back by the HBM budget while a slot was free
+    cancel_at: float = -1.0     # scripted cancellation time (s from the start), < 0: none
+    cancelled: bool = False
     latencies: list = field(default_factory=list)
     results: list = field(default_factory=list)
 
@@ -82,6 +90,20 @@ class FockServer:
         self.max_slots = int(max_slots)
         self.capture = capture
         self.poll_s = poll_s
+        self._cancel = set()
+        self._cancel_lock = threading.Lock()
+
+    def cancel(self, sid):
+        """Request cancellation of session `sid` (thread-safe; takes effect at
+        the loop's next pass)."""
+        with self._cancel_lock:
+            self._cancel.add(int(sid))
+
+    def _cancelled(self, s, t):
+        if s.cancel_at >= 0 and t >= s.cancel_at:
+            return True
+        with self._cancel_lock:
+            return s.sid in self._cancel
 
     def run(self, arrivals, clock=time.perf_counter):
         """Serve `arrivals` (Sessions with arrival times in seconds from the
@@ -94,7 +116,7 @@ class FockServer:
             if s.nbytes > self.budget:
                 raise ValueError("session %d needs %d bytes, above the HBM budget %d" % (s.sid, s.nbytes, self.budget))
         waiting = collections.deque()
-        active, finished = [], []
+        active, finished, cancelled = [], [], []
         reserved = peak_reserved = 0
         peak_active = 0
         in_setup = 0                       # admitted, handed to the worker, not back yet
@@ -129,11 +151,20 @@ class FockServer:
                 t = now()
                 while pending and pending[0].arrival <= t:
                     waiting.append(pending.popleft())
+                # cancelled before admission: leave the queue, never set up
+                for q in (pending, waiting):
+                    for s in [x for x in q if self._cancelled(x, t)]:
+                        q.remove(s)
+                        s.cancelled = True
+                        cancelled.append(s)
                 # admission: FIFO, by free slots and HBM bytes
                 while waiting:
                     s = waiting[0]
-                    if len(active) + in_setup >= self.max_slots or reserved + s.nbytes > self.budget:
+                    slots_full = len(active) + in_setup >= self.max_slots
+                    if slots_full or reserved + s.nbytes > self.budget:
                         s.waited = True
+                        if not slots_full:
+                            s.waited_bytes = True
                         break
                     waiting.popleft()
                     reserved += s.nbytes
@@ -153,8 +184,17 @@ class FockServer:
                 # launch every ready build; collect completions
                 progressed = False
                 for s in list(active):
+                    stop_now = self._cancelled(s, now())
                     if s.token is None:
-                        s.token = self.engine.launch(s)
+                        if stop_now:  # nothing on the GPU: release at once
+                            self.engine.close(s)
+                            s.state = None
+                            reserved -= s.nbytes
+                            active.remove(s)
+                            s.cancelled = True
+                            cancelled.append(s)
+                        else:
+                            s.token = self.engine.launch(s)
                         progressed = True
                     elif self.engine.done(s.token):
                         tdone = now()
@@ -164,7 +204,14 @@ class FockServer:
                         s.it += 1
                         s.token = None
                         progressed = True
-                        if s.it >= s.niter:
+                        if stop_now and s.it < s.niter:  # the build in flight has finished
+                            self.engine.close(s)
+                            s.state = None
+                            reserved -= s.nbytes
+                            active.remove(s)
+                            s.cancelled = True
+                            cancelled.append(s)
+                        elif s.it >= s.niter:
                             self.engine.close(s)
                             s.state = None
                             reserved -= s.nbytes
@@ -193,6 +240,8 @@ class FockServer:
             "latency_ms_mean": round(float(lat.mean()), 3) if nb else None,
             "peak_reserved_bytes": int(peak_reserved), "hbm_budget_bytes": self.budget,
             "peak_concurrent_sessions": int(peak_active), "sessions_that_waited": int(sum(s.waited for s in finished)),
+            "sessions_waited_for_bytes": int(sum(s.waited_bytes for s in finished + cancelled)),
+            "cancelled": len(cancelled),
             "setup_ms_mean": round(1e3 * float(np.mean([s.ready_at - s.admitted_at for s in finished])), 3)
             if finished else None,
         }

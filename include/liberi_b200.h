@@ -123,6 +123,9 @@ int liberi_c_last_error(char *buf, int32_t len);
  *                   set 0 where many handles build at once and already fill
  *                   the GPU, as the serving loop does)
  *   "timing"       (1 = record per-class device times for liberi_c_get_stats)
+ *   "max_device_bytes" (0 = no limit; otherwise liberi_c_setup fails with
+ *                   LIBERI_E_NOMEM, before any device work, when the basis
+ *                   and plans would need more device bytes than this)
  * Options set before liberi_c_setup apply to it; cut options may also be
  * changed between builds (the quartet plan is rebuilt on the next build). */
 int liberi_c_set_option(liberi_handle handle, const char *name, double value);

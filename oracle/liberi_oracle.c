@@ -59,6 +59,21 @@
 #include <omp.h>
 #endif
 
+/* Scalar types of the quartet arithmetic (roots, recurrences, assembly,
+ * digestion): double and long double in this build.  The op-counting build
+ * (oracle/opcount.cpp) compiles this file as C++ with a counting type in
+ * their place, to measure the floating-point operations per primitive and
+ * per shell quartet of this restatement of the reference algorithm. */
+#ifndef ORACLE_REAL
+#define ORACLE_REAL double
+#define ORACLE_REALL long double
+#define ORACLE_OPS() 0
+#define ORACLE_MARK()
+#define ORACLE_MARKED() 0
+#endif
+typedef ORACLE_REAL real_t;
+typedef ORACLE_REALL reall_t;
+
 #define PI_D 3.14159265358979323846
 #define NGRID 35
 #define MAXROOT 5
@@ -112,6 +127,7 @@ typedef struct {
     double t_eval[21];
     int32_t nthreads;
     uint64_t fp[21][2];
+    uint64_t ops[21][2];  /* op-counting build only: ops in primitive-quartet work, in shell-quartet work */
 } oracle_counts;
 
 /* ---- pair classes ---------------------------------------------------------- */
@@ -268,30 +284,30 @@ static void boys_table_init(void) {
 }
 
 /* double-precision Rys rule for 1 and 2 roots (well conditioned) */
-static void rys_small_d(int n, double T, double *u, double *w) {
+static void rys_small_d(int n, real_t T, real_t *u, real_t *w) {
     const int mmax = 2 * n - 1;
-    const int k = (int)(T / (double)BOYS_STEP + 0.5);
-    const double d = T - k * (double)BOYS_STEP;
-    double F[4], s = 0.0, f = 1.0;
+    const int k = (int)((double)T / (double)BOYS_STEP + 0.5);
+    const real_t d = T - k * (double)BOYS_STEP;
+    real_t F[4], sm = 0.0, f = 1.0;
     for (int j = 0; j < BOYS_TERMS; j++) {
-        s += BOYS_D[k][mmax + j] * f;
-        f *= -d / (j + 1);
+        sm += BOYS_D[k][mmax + j] * f;
+        f *= -d / (double)(j + 1);
     }
-    F[mmax] = s;
-    const double e = exp(-T);
-    for (int m = mmax; m > 0; m--) F[m - 1] = (2.0 * T * F[m] + e) / (2 * m - 1);
+    F[mmax] = sm;
+    const real_t e = exp(-T);
+    for (int m = mmax; m > 0; m--) F[m - 1] = (2.0 * T * F[m] + e) / (double)(2 * m - 1);
     if (n == 1) {
         u[0] = F[1] / F[0];
         w[0] = F[0];
         return;
     }
     /* monic recurrence from the moments, then the 2x2 Jacobi matrix */
-    const double a0 = F[1] / F[0];
-    const double s1 = F[2] - a0 * F[1], s2 = F[3] - a0 * F[2];  /* sigma_{1,1}, sigma_{1,2} */
-    const double b1 = s1 / F[0];
-    const double a1 = s2 / s1 - a0;
-    const double m = 0.5 * (a0 + a1), h = 0.5 * (a1 - a0), r = sqrt(h * h + b1);
-    const double x0 = m - r, x1 = m + r;
+    const real_t a0 = F[1] / F[0];
+    const real_t s1 = F[2] - a0 * F[1], s2 = F[3] - a0 * F[2];  /* sigma_{1,1}, sigma_{1,2} */
+    const real_t b1 = s1 / F[0];
+    const real_t a1 = s2 / s1 - a0;
+    const real_t m = 0.5 * (a0 + a1), h = 0.5 * (a1 - a0), r = sqrt(h * h + b1);
+    const real_t x0 = m - r, x1 = m + r;
     u[0] = x0;
     u[1] = x1;
     w[0] = F[0] / (1.0 + (x0 - a0) * (x0 - a0) / b1);
@@ -299,25 +315,27 @@ static void rys_small_d(int n, double T, double *u, double *w) {
 }
 
 /* F_0..F_mmax(T), T <= 25 */
-static void boys_eval(int mmax, double T, long double *F) {
-    int k = (int)((long double)T / BOYS_STEP + 0.5L);
-    long double d = (long double)T - k * BOYS_STEP;
-    long double s = 0.0L, f = 1.0L;
+static void boys_eval(int mmax, real_t T, reall_t *F) {
+    int k = (int)((long double)(double)T / BOYS_STEP + 0.5L);
+    reall_t d = (reall_t)T - k * BOYS_STEP;
+    reall_t sm = 0.0L, f = 1.0L;
     for (int j = 0; j < BOYS_TERMS; j++) {
-        s += BOYS[k][mmax + j] * f;
-        f *= -d / (j + 1);
+        sm += BOYS[k][mmax + j] * f;
+        f *= -d / (long double)(j + 1);
     }
-    F[mmax] = s;
-    long double e = expl(-(long double)T);
-    for (int m = mmax; m > 0; m--) F[m - 1] = (2.0L * T * F[m] + e) / (2 * m - 1);
+    F[mmax] = sm;
+    reall_t e = expl(-(reall_t)T);
+    for (int m = mmax; m > 0; m--) F[m - 1] = (2.0L * (reall_t)T * F[m] + e) / (long double)(2 * m - 1);
 }
 
 /* Gauss rule (n <= 3) of the Rys weight from its moments F_0..F_{2n-1} */
-static void rys_from_moments(int n, double T, double *u, double *w) {
-    long double F[2 * MAXROOT + 1];
+static void rys_from_moments(int n, real_t T, real_t *u, real_t *w) {
+    reall_t F[2 * MAXROOT + 1];
     boys_eval(2 * n - 1, T, F);
-    long double a[MAXROOT] = {0}, b[MAXROOT] = {0};
-    long double sp[2 * MAXROOT] = {0}, sc[2 * MAXROOT], sn[2 * MAXROOT];
+    reall_t a[MAXROOT], b[MAXROOT];
+    reall_t sp[2 * MAXROOT], sc[2 * MAXROOT], sn[2 * MAXROOT];
+    for (int l = 0; l < MAXROOT; l++) { a[l] = 0.0L; b[l] = 0.0L; }
+    for (int l = 0; l < 2 * MAXROOT; l++) { sp[l] = 0.0L; sn[l] = 0.0L; }
     for (int l = 0; l < 2 * n; l++) sc[l] = F[l];
     a[0] = F[1] / F[0];
     b[0] = F[0];
@@ -327,51 +345,111 @@ static void rys_from_moments(int n, double T, double *u, double *w) {
         b[k] = sn[k] / sc[k - 1];
         for (int l = 0; l < 2 * n; l++) { sp[l] = sc[l]; sc[l] = sn[l]; }
     }
-    long double x[MAXROOT];
+    reall_t x[MAXROOT];
     if (n == 1) {
         x[0] = a[0];
     } else if (n == 2) {
-        long double m = 0.5L * (a[0] + a[1]), h = 0.5L * (a[1] - a[0]);
-        long double r = sqrtl(h * h + b[1]);
+        reall_t m = 0.5L * (a[0] + a[1]), h = 0.5L * (a[1] - a[0]);
+        reall_t r = sqrtl(h * h + b[1]);
         x[0] = m - r;
         x[1] = m + r;
     } else {
         /* characteristic polynomial of the 3x3 Jacobi matrix, trigonometric
          * roots, two Newton polishing steps each */
-        long double c2 = -(a[0] + a[1] + a[2]);
-        long double c1 = a[0] * a[1] + a[0] * a[2] + a[1] * a[2] - b[1] - b[2];
-        long double c0 = -(a[0] * a[1] * a[2]) + a[0] * b[2] + a[2] * b[1];
-        long double p = c1 - c2 * c2 / 3.0L, q = 2.0L * c2 * c2 * c2 / 27.0L - c2 * c1 / 3.0L + c0;
-        long double rr = sqrtl(-p / 3.0L);
-        long double arg = 3.0L * q / (2.0L * p * rr);
+        reall_t c2 = -(a[0] + a[1] + a[2]);
+        reall_t c1 = a[0] * a[1] + a[0] * a[2] + a[1] * a[2] - b[1] - b[2];
+        reall_t c0 = -(a[0] * a[1] * a[2]) + a[0] * b[2] + a[2] * b[1];
+        reall_t p = c1 - c2 * c2 / 3.0L, q = 2.0L * c2 * c2 * c2 / 27.0L - c2 * c1 / 3.0L + c0;
+        reall_t rr = sqrtl(-p / 3.0L);
+        reall_t arg = 3.0L * q / (2.0L * p * rr);
         if (arg > 1.0L) arg = 1.0L;
         if (arg < -1.0L) arg = -1.0L;
-        long double th = acosl(arg) / 3.0L;
+        reall_t th = acosl(arg) / 3.0L;
         const long double PI_L = 3.141592653589793238462643383279502884L;
         for (int i = 0; i < 3; i++) x[i] = 2.0L * rr * cosl(th - 2.0L * PI_L * i / 3.0L) - c2 / 3.0L;
         for (int i = 0; i < 3; i++)
             for (int it = 0; it < 2; it++) {
-                long double v = ((x[i] + c2) * x[i] + c1) * x[i] + c0;
-                long double dv = (3.0L * x[i] + 2.0L * c2) * x[i] + c1;
+                reall_t v = ((x[i] + c2) * x[i] + c1) * x[i] + c0;
+                reall_t dv = (3.0L * x[i] + 2.0L * c2) * x[i] + c1;
                 if (dv != 0.0L) x[i] -= v / dv;
             }
         for (int i = 0; i < 3; i++)
             for (int j = i + 1; j < 3; j++)
-                if (x[j] < x[i]) { long double t = x[i]; x[i] = x[j]; x[j] = t; }
+                if (x[j] < x[i]) { reall_t t = x[i]; x[i] = x[j]; x[j] = t; }
     }
     for (int i = 0; i < n; i++) {
         /* Christoffel number: b0 / sum_k p_k(x)^2 / (b1..bk), monic p_k */
-        long double p0 = 1.0L, p1 = 0.0L, nrm = 1.0L, s = 1.0L;
+        reall_t p0 = 1.0L, p1 = 0.0L, nrm = 1.0L, sm = 1.0L;
         for (int k = 0; k + 1 < n; k++) {
-            long double pn = (x[i] - a[k]) * p0 - (k > 0 ? b[k] * p1 : 0.0L);
+            reall_t pn = (x[i] - a[k]) * p0 - (k > 0 ? b[k] * p1 : (reall_t)0.0L);
             p1 = p0;
             p0 = pn;
             nrm *= b[k + 1];
-            s += p0 * p0 / nrm;
+            sm += p0 * p0 / nrm;
         }
-        u[i] = (double)x[i];
-        w[i] = (double)(b[0] / s);
+        u[i] = (real_t)x[i];
+        w[i] = (real_t)(b[0] / sm);
     }
+}
+
+/* Golub-Welsch step of the Rys classes (the reference's RYSGW): eigenvalues
+ * of the symmetric tridiagonal Jacobi matrix (diagonal a[0..n-1], squared
+ * off-diagonals b2[1..n-1]) by implicit QL iterations with Wilkinson shifts
+ * (Golub and Welsch, Math. Comp. 23 (1969) 221), carrying the first row of
+ * the eigenvector matrix, whose squares times the total mass beta0 are the
+ * weights.  Roots ascending. */
+static void rys_gw(int n, const real_t *a, const real_t *b2, real_t beta0, real_t *x, real_t *w) {
+    real_t d[MAXROOT], e[MAXROOT], z[MAXROOT];
+    for (int i = 0; i < n; i++) {
+        d[i] = a[i];
+        e[i] = i + 1 < n ? sqrt(b2[i + 1]) : (real_t)0.0;
+        z[i] = i == 0 ? 1.0 : 0.0;
+    }
+    for (int l = 0; l < n; l++) {
+        for (int iter = 0; iter < 60; iter++) {
+            int m = l;
+            while (m < n - 1 && !(fabs(e[m]) <= 1e-17 * (fabs(d[m]) + fabs(d[m + 1])))) m++;
+            if (m == l) break;
+            /* Wilkinson shift from the leading 2x2 block, then a chase of
+             * plane rotations from row m-1 up to row l */
+            real_t g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            real_t r = sqrt(g * g + 1.0);
+            g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
+            real_t sn = 1.0, cs = 1.0, p = 0.0;
+            int i = m - 1;
+            for (; i >= l; i--) {
+                real_t f = sn * e[i], bb = cs * e[i];
+                r = sqrt(f * f + g * g);
+                e[i + 1] = r;
+                if (r == 0.0) {  /* exact deflation */
+                    d[i + 1] -= p;
+                    e[m] = 0.0;
+                    break;
+                }
+                sn = f / r;
+                cs = g / r;
+                g = d[i + 1] - p;
+                r = (d[i] - g) * sn + 2.0 * cs * bb;
+                p = sn * r;
+                d[i + 1] = g + p;
+                g = cs * r - bb;
+                const real_t zt = z[i + 1];
+                z[i + 1] = sn * z[i] + cs * zt;
+                z[i] = cs * z[i] - sn * zt;
+            }
+            if (i >= l) continue;
+            d[l] -= p;
+            e[l] = g;
+            e[m] = 0.0;
+        }
+    }
+    for (int i = 0; i < n; i++) { x[i] = d[i]; w[i] = beta0 * z[i] * z[i]; }
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++)
+            if (x[j] < x[i]) {
+                real_t t = x[i]; x[i] = x[j]; x[j] = t;
+                t = w[i]; w[i] = w[j]; w[j] = t;
+            }
 }
 
 static void init_tables(void) {
@@ -402,10 +480,10 @@ static void init_tables(void) {
 
 /* Rys roots u_i = t_i^2 in (0,1) and weights w_i (sum w_i = F_0(T)).
  * asym_strict: 1 -> asymptotic when T > thr (rot-axis), 0 -> T >= thr (Rys) */
-static void rys_roots(int n, double T, double thr, int rot, double *u, double *w) {
+static void rys_roots(int n, real_t T, double thr, int rot, real_t *u, real_t *w) {
     int asym = rot ? (T > thr) : (T >= thr);
     if (asym) {
-        double it = 1.0 / T, sq = sqrt(it);
+        real_t it = 1.0 / T, sq = sqrt(it);
         for (int i = 0; i < n; i++) { u[i] = HR[n][i] * it; w[i] = HW[n][i] * sq; }
         return;
     }
@@ -418,9 +496,9 @@ static void rys_roots(int n, double T, double thr, int rot, double *u, double *w
         return;
     }
     /* RYSDS: Stieltjes on the discrete measure {GRID_U, GRID_W*exp(-T u)} */
-    double W[NGRID], p0[NGRID], p1[NGRID];
-    double a[MAXROOT], b2[MAXROOT];
-    double s0 = 0.0, s1 = 0.0;
+    real_t W[NGRID], p0[NGRID], p1[NGRID];
+    real_t a[MAXROOT], b2[MAXROOT];
+    real_t s0 = 0.0, s1 = 0.0;
     for (int j = 0; j < NGRID; j++) {
         W[j] = GRID_W[j] * exp(-T * GRID_U[j]);
         p0[j] = 1.0;
@@ -428,13 +506,14 @@ static void rys_roots(int n, double T, double thr, int rot, double *u, double *w
         s0 += W[j];
         s1 += W[j] * GRID_U[j];
     }
-    double beta0 = s0, nprev = s0;
+    real_t beta0 = s0, nprev = s0;
     a[0] = s1 / s0;
     b2[0] = 0.0;
     for (int k = 1; k < n; k++) {
-        double sa = 0.0, sb = 0.0;
+        real_t sa = 0.0, sb = 0.0;
         for (int j = 0; j < NGRID; j++) {
-            double pn = (GRID_U[j] - a[k - 1]) * p0[j] - (k > 1 ? b2[k - 1] * p1[j] : 0.0);
+            real_t pn = (GRID_U[j] - a[k - 1]) * p0[j];
+            if (k > 1) pn -= b2[k - 1] * p1[j];
             p1[j] = p0[j];
             p0[j] = pn;
             sa += W[j] * pn * pn;
@@ -444,7 +523,7 @@ static void rys_roots(int n, double T, double thr, int rot, double *u, double *w
         b2[k] = sa / nprev;
         nprev = sa;
     }
-    jacobi_gauss(n, a, b2, beta0, 0.0, 1.0, u, w);
+    rys_gw(n, a, b2, beta0, u, w);  /* RYSGW */
 }
 
 /* ============================ setup ========================================= */
@@ -467,12 +546,12 @@ static void build_ctx(ctx_t *c, const oracle_basis *b) {
     memset(c, 0, sizeof(*c));
     c->b = b;
     c->coef[0] = b->coef_s; c->coef[1] = b->coef_p; c->coef[2] = b->coef_d;
-    c->csh = malloc(sizeof(double[3]) * (b->nsh > 0 ? b->nsh : 1));
+    c->csh = (double(*)[3])malloc(sizeof(double[3]) * (b->nsh > 0 ? b->nsh : 1));
     for (int s = 0; s < b->nsh; s++)
         for (int x = 0; x < 3; x++) c->csh[s][x] = b->coords[3 * (b->atom_num[s] - 1) + x];
     /* ascending per-L lists (classify_shells final sort, :301-344) */
     for (int l = 0; l < 3; l++) {
-        c->lst[l] = malloc(sizeof(int32_t) * (b->nsh > 0 ? b->nsh : 1));
+        c->lst[l] = (int32_t *)malloc(sizeof(int32_t) * (b->nsh > 0 ? b->nsh : 1));
         c->nl[l] = 0;
     }
     for (int s = 0; s < b->nsh; s++) {
@@ -486,10 +565,10 @@ static void build_ctx(ctx_t *c, const oracle_basis *b) {
         pairs_t *p = &c->pc[k];
         p->n = same ? n1 * (n1 + 1) / 2 : n1 * n2;
         int64_t nn = p->n > 0 ? p->n : 1;
-        p->ish = malloc(sizeof(int32_t) * nn);
-        p->jsh = malloc(sizeof(int32_t) * nn);
-        p->xint = malloc(sizeof(double) * nn);
-        p->loc = malloc(sizeof(int64_t) * (nn + 1));
+        p->ish = (int32_t *)malloc(sizeof(int32_t) * nn);
+        p->jsh = (int32_t *)malloc(sizeof(int32_t) * nn);
+        p->xint = (double *)malloc(sizeof(double) * nn);
+        p->loc = (int64_t *)malloc(sizeof(int64_t) * (nn + 1));
         int64_t q = 0;
         p->loc[0] = 0;
         for (int64_t ii = 0; ii < n1; ii++) {
@@ -505,10 +584,10 @@ static void build_ctx(ctx_t *c, const oracle_basis *b) {
         }
         int64_t np = p->loc[p->n];
         int64_t npp = np > 0 ? np : 1;
-        p->ea = malloc(sizeof(double) * npp);
-        p->eb = malloc(sizeof(double) * npp);
-        p->cc = malloc(sizeof(double) * npp);
-        p->ismlp = malloc(sizeof(int32_t) * npp);
+        p->ea = (double *)malloc(sizeof(double) * npp);
+        p->eb = (double *)malloc(sizeof(double) * npp);
+        p->cc = (double *)malloc(sizeof(double) * npp);
+        p->ismlp = (int32_t *)malloc(sizeof(int32_t) * npp);
         for (int64_t e = 0; e < p->n; e++) {
             int is = p->ish[e], js = p->jsh[e];
             double r2 = 0.0;
@@ -540,14 +619,14 @@ static void build_ctx(ctx_t *c, const oracle_basis *b) {
 /* out[((i*nb + j)*nc + k)*nd + l] contracted Cartesian integrals */
 static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
                            const pairs_t *pb, int64_t eb_, const pairs_t *pk, int64_t ek_,
-                           const kdesc_t *kd, double *out) {
+                           const kdesc_t *kd, real_t *out) {
     const oracle_basis *b = c->b;
     int la = b->ang_mom[A] - 1, lb = b->ang_mom[B] - 1, lc = b->ang_mom[C] - 1, ld = b->ang_mom[D] - 1;
     int na = NCART[la], nb = NCART[lb], nc = NCART[lc], nd = NCART[ld];
     int n = (la + lb + lc + ld) / 2 + 1;
     int nij = la + lb, nkl = lc + ld;
     const double *Ar = c->csh[A], *Br = c->csh[B], *Cr = c->csh[C], *Dr = c->csh[D];
-    double AB[3], CD[3], rab2 = 0, rcd2 = 0;
+    real_t AB[3], CD[3], rab2 = 0.0, rcd2 = 0.0;
     for (int x = 0; x < 3; x++) {
         AB[x] = Ar[x] - Br[x]; CD[x] = Cr[x] - Dr[x];
         rab2 += AB[x] * AB[x]; rcd2 += CD[x] * CD[x];
@@ -557,50 +636,52 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
     int64_t nprim = 0;
     const double twopi52 = 2.0 * PI_D * PI_D * sqrt(PI_D);
     for (int64_t kq = pk->loc[ek_]; kq < pk->loc[ek_ + 1]; kq++) {
-        double gc = pk->ea[kq], gd = pk->eb[kq], q = gc + gd;
-        double Q[3];
+        real_t gc = pk->ea[kq], gd = pk->eb[kq], q = gc + gd;
+        real_t Q[3];
         for (int x = 0; x < 3; x++) Q[x] = (gc * Cr[x] + gd * Dr[x]) / q;
-        double ecd = exp(-gc * gd / q * rcd2);
+        real_t ecd = exp(-gc * gd / q * rcd2);
         for (int64_t bq = pb->loc[eb_]; bq < pb->loc[eb_ + 1]; bq++) {
             if (!kd->rys && (pb->ismlp[bq] + pk->ismlp[kq] >= 2)) continue;
-            double ga = pb->ea[bq], gb = pb->eb[bq], p = ga + gb;
-            double P[3], PQ2 = 0.0;
+            real_t ga = pb->ea[bq], gb = pb->eb[bq], p = ga + gb;
+            real_t P[3], PQ2 = 0.0;
             for (int x = 0; x < 3; x++) {
                 P[x] = (ga * Ar[x] + gb * Br[x]) / p;
                 PQ2 += (P[x] - Q[x]) * (P[x] - Q[x]);
             }
-            double eab = exp(-ga * gb / p * rab2);
-            double rho = p * q / (p + q);
-            double T = rho * PQ2;
-            double u[MAXROOT], w[MAXROOT];
+            real_t eab = exp(-ga * gb / p * rab2);
+            real_t rho = p * q / (p + q);
+            real_t T = rho * PQ2;
+            real_t u[MAXROOT], w[MAXROOT];
             rys_roots(n, T, kd->asym, !kd->rys, u, w);
-            double pref = twopi52 * (pb->cc[bq] / p) * (pk->cc[kq] / q) * eab * ecd / sqrt(p + q);
+            real_t pref = twopi52 * (pb->cc[bq] / p) * (pk->cc[kq] / q) * eab * ecd / sqrt(p + q);
             nprim++;
             /* 2D integrals per root and dimension: vertical recurrence, then
              * horizontal transfer to I[a][b][c][d] by recurrences */
-            double I2[MAXROOT][3][3][3][3][3];
-            const double ipq = 1.0 / (p + q);
+            real_t I2[MAXROOT][3][3][3][3][3];
+            const real_t ipq = 1.0 / (p + q);
             for (int r = 0; r < n; r++) {
-                double ur = u[r];
-                double B00 = 0.5 * ur * ipq;
-                double B10 = 0.5 / p * (1.0 - q * ur * ipq);
-                double B01 = 0.5 / q * (1.0 - p * ur * ipq);
+                real_t ur = u[r];
+                real_t B00 = 0.5 * ur * ipq;
+                real_t B10 = 0.5 / p * (1.0 - q * ur * ipq);
+                real_t B01 = 0.5 / q * (1.0 - p * ur * ipq);
                 for (int x = 0; x < 3; x++) {
-                    double C00 = (P[x] - Ar[x]) - q * ur * ipq * (P[x] - Q[x]);
-                    double Cp00 = (Q[x] - Cr[x]) + p * ur * ipq * (P[x] - Q[x]);
-                    double g[5][5];
+                    real_t C00 = (P[x] - Ar[x]) - q * ur * ipq * (P[x] - Q[x]);
+                    real_t Cp00 = (Q[x] - Cr[x]) + p * ur * ipq * (P[x] - Q[x]);
+                    real_t g[5][5];
                     g[0][0] = 1.0;
-                    for (int i = 0; i < nij; i++)
-                        g[i + 1][0] = C00 * g[i][0] + (i > 0 ? i * B10 * g[i - 1][0] : 0.0);
+                    for (int i = 0; i < nij; i++) {
+                        g[i + 1][0] = C00 * g[i][0];
+                        if (i > 0) g[i + 1][0] += (double)i * B10 * g[i - 1][0];
+                    }
                     for (int k = 0; k < nkl; k++) {
                         for (int i = 0; i <= nij; i++) {
-                            double v = Cp00 * g[i][k];
-                            if (k > 0) v += k * B01 * g[i][k - 1];
-                            if (i > 0) v += i * B00 * g[i - 1][k];
+                            real_t v = Cp00 * g[i][k];
+                            if (k > 0) v += (double)k * B01 * g[i][k - 1];
+                            if (i > 0) v += (double)i * B00 * g[i - 1][k];
                             g[i][k + 1] = v;
                         }
                     }
-                    double h[5][3][5];
+                    real_t h[5][3][5];
                     for (int e = 0; e <= nij; e++)
                         for (int f = 0; f <= nkl; f++) h[e][0][f] = g[e][f];
                     for (int bb = 1; bb <= lb; bb++)
@@ -608,7 +689,7 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
                             for (int f = 0; f <= nkl; f++) h[a2][bb][f] = h[a2 + 1][bb - 1][f] + AB[x] * h[a2][bb - 1][f];
                     for (int a2 = 0; a2 <= la; a2++)
                         for (int bb = 0; bb <= lb; bb++) {
-                            double k2[5][3];
+                            real_t k2[5][3];
                             for (int f = 0; f <= nkl; f++) k2[f][0] = h[a2][bb][f];
                             for (int dd = 1; dd <= ld; dd++)
                                 for (int cc = 0; cc <= nkl - dd; cc++) k2[cc][dd] = k2[cc + 1][dd - 1] + CD[x] * k2[cc][dd - 1];
@@ -626,13 +707,14 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
                 const int bx = CX[lb][ib], by = CY[lb][ib], bz = CZ[lb][ib];
                 const int cx = CX[lc][ic], cy = CY[lc][ic], cz = CZ[lc][ic];
                 const int dx = CX[ld][id], dy = CY[ld][id], dz = CZ[ld][id];
-                double acc = 0.0;
+                real_t acc = 0.0;
                 for (int r = 0; r < n; r++)
                     acc += w[r] * I2[r][0][ax][bx][cx][dx] * I2[r][1][ay][by][cy][dy] * I2[r][2][az][bz][cz][dz];
                 out[((ia * nb + ib) * nc + ic) * nd + id] += pref * acc;
             }
         }
     }
+    ORACLE_MARK();  /* op-counting build: end of the primitive-quartet work */
     /* component normalisation (sqrt3 on xy,xz,yz of d) */
     for (int ia = 0; ia < na; ia++)
     for (int ib = 0; ib < nb; ib++)
@@ -644,7 +726,7 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
 }
 
 /* =============================== DIRFCK ===================================== */
-static int64_t dirfck(const ctx_t *c, int A, int B, int C, int D, const double *v,
+static int64_t dirfck(const ctx_t *c, int A, int B, int C, int D, const real_t *v,
                       double cut, const double *Dm, double *F) {
     const oracle_basis *b = c->b;
     int na = NCART[b->ang_mom[A] - 1], nb = NCART[b->ang_mom[B] - 1];
@@ -669,7 +751,7 @@ static int64_t dirfck(const ctx_t *c, int A, int B, int C, int D, const double *
                     nkl -= itmp;
                 }
                 for (int l = 0; l < maxl2; l++) {
-                    double val = v[((i * nb + j) * nc + k) * nd + l];
+                    real_t val = v[((i * nb + j) * nc + k) * nd + l];
                     if (fabs(val) < cut) continue;
                     ndig++;
                     int64_t i1 = i + 1 + loci, j1 = j + 1 + locj, k1 = k + 1 + lock, l1 = l + 1 + locl;
@@ -684,13 +766,13 @@ static int64_t dirfck(const ctx_t *c, int A, int B, int C, int D, const double *
                     if (ii == jj) val *= 0.5;
                     if (kk == ll) val *= 0.5;
                     if (ii == kk && jj == ll) val *= 0.5;
-                    double v4 = 4.0 * val;
-                    F[ij - 1] += v4 * Dm[kl - 1];
-                    F[kl - 1] += v4 * Dm[ij - 1];
-                    F[ik - 1] -= val * Dm[jl - 1];
-                    F[jl - 1] -= val * Dm[ik - 1];
-                    F[il - 1] -= val * Dm[jk - 1];
-                    F[jk - 1] -= val * Dm[il - 1];
+                    real_t v4 = 4.0 * val;
+                    F[ij - 1] = (double)(F[ij - 1] + v4 * Dm[kl - 1]);
+                    F[kl - 1] = (double)(F[kl - 1] + v4 * Dm[ij - 1]);
+                    F[ik - 1] = (double)(F[ik - 1] - val * Dm[jl - 1]);
+                    F[jl - 1] = (double)(F[jl - 1] - val * Dm[ik - 1]);
+                    F[il - 1] = (double)(F[il - 1] - val * Dm[jk - 1]);
+                    F[jk - 1] = (double)(F[jk - 1] - val * Dm[il - 1]);
                 }
             }
         }
@@ -768,7 +850,7 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
 #ifdef _OPENMP
     nth = o->nthreads > 0 ? o->nthreads : omp_get_max_threads();
 #endif
-    double *Fp = calloc((size_t)nth * ntri, sizeof(double));
+    double *Fp = (double *)calloc((size_t)nth * ntri, sizeof(double));
     for (int kk = 0; kk < 21; kk++) {
         const kdesc_t *kd = &KD[kk];
         if (o->only_kernel >= 0 && o->only_kernel != kk) continue;
@@ -782,7 +864,7 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
          * own-class maxima for same-class and Rys kernels */
         double sb = o->schwarz_cut / maxval(kd->cross ? pk : pb);
         double sk = o->schwarz_cut / maxval(kd->cross ? pb : pk);
-        int64_t *lb = malloc(sizeof(int64_t) * pb->n), *lk = malloc(sizeof(int64_t) * pk->n);
+        int64_t *lb = (int64_t *)malloc(sizeof(int64_t) * pb->n), *lk = (int64_t *)malloc(sizeof(int64_t) * pk->n);
         int64_t nbl = 0, nkl = 0;
         for (int64_t i = 0; i < pb->n; i++) if (pb->xint[i] >= sb) lb[nbl++] = i;
         if (kd->tri) { memcpy(lk, lb, sizeof(int64_t) * nbl); nkl = nbl; }
@@ -791,16 +873,16 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
         double dcut = kd->digest_schwarz ? o->schwarz_cut : o->eri_cut;
         int64_t niter = kd->tri ? nbl : nbl * nkl;
         int64_t c_scr = 0, c_prim = 0, c_dig = 0, c_eval = 0;
-        uint64_t fp_sum = 0, fp_xor = 0;
+        uint64_t fp_sum = 0, fp_xor = 0, ops_prim = 0, ops_shell = 0;
         double t_eval = 0.0, t_k0 = now_s();
-#pragma omp parallel num_threads(nth) reduction(+ : c_scr, c_prim, c_dig, c_eval, t_eval, fp_sum) reduction(^ : fp_xor)
+#pragma omp parallel num_threads(nth) reduction(+ : c_scr, c_prim, c_dig, c_eval, t_eval, fp_sum, ops_prim, ops_shell) reduction(^ : fp_xor)
         {
             int tid = 0;
 #ifdef _OPENMP
             tid = omp_get_thread_num();
 #endif
             double *Ft = Fp + (size_t)tid * ntri;
-            double vbuf[1296];
+            real_t vbuf[1296];
 #pragma omp for schedule(dynamic, 16)
             for (int64_t it = 1; it <= niter; it++) {
                 if (o->num_procs > 1 && !oracle_rank_owns(kd->tile, niter, it, o->my_rank, o->num_procs)) continue;
@@ -830,8 +912,14 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
                     c_eval++;
                     double tq = o->sample_mod > 1 ? now_s() : 0.0;
                     int A = pb->ish[bi], B = pb->jsh[bi], C = pk->ish[ki], D = pk->jsh[ki];
+                    const uint64_t o0 = ORACLE_OPS();
                     c_prim += eri_quartet(&c, A, B, C, D, pb, bi, pk, ki, kd, vbuf);
+                    const uint64_t o1 = ORACLE_OPS();
                     c_dig += dirfck(&c, A, B, C, D, vbuf, dcut, Dm, Ft);
+                    /* primitive work up to eri_quartet's mark; its normalisation
+                     * and the digestion are shell-quartet work */
+                    ops_prim += ORACLE_MARKED() - o0;
+                    ops_shell += (o1 - ORACLE_MARKED()) + (ORACLE_OPS() - o1);
                     if (o->sample_mod > 1) t_eval += now_s() - tq;
                 }
             }
@@ -844,6 +932,8 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
             cnt->nthreads = nth;
             cnt->fp[kk][0] = fp_sum;
             cnt->fp[kk][1] = fp_xor;
+            cnt->ops[kk][0] = ops_prim;
+            cnt->ops[kk][1] = ops_shell;
         }
         free(lb); free(lk);
     }
@@ -865,7 +955,7 @@ int oracle_schwarz(const oracle_basis *b, double *schwrz_out) {
     kdesc_t kd = {"schwarz", 0, 0, 0, 1, 0, OP_NONE, TILE_NONE, 0, 0, 60.0};
     oracle_basis bb = *b;
     int64_t ntri = (int64_t)b->nsh * (b->nsh + 1) / 2;
-    double *dummy = malloc(sizeof(double) * (ntri > 0 ? ntri : 1));
+    double *dummy = (double *)malloc(sizeof(double) * (ntri > 0 ? ntri : 1));
     for (int64_t i = 0; i < ntri; i++) dummy[i] = 1.0;
     bb.schwrz = dummy;
     ctx_t c;
@@ -875,14 +965,14 @@ int oracle_schwarz(const oracle_basis *b, double *schwrz_out) {
         const pairs_t *p = &c.pc[k];
 #pragma omp parallel for schedule(dynamic, 4)
         for (int64_t e = 0; e < p->n; e++) {
-            double v[1296];
+            real_t v[1296];
             int A = p->ish[e], B = p->jsh[e];
             eri_quartet(&c, A, B, A, B, p, e, p, e, &kd, v);
             int na = NCART[b->ang_mom[A] - 1], nb = NCART[b->ang_mom[B] - 1];
             double m = 0.0;
             for (int i = 0; i < na; i++)
                 for (int j = 0; j < nb; j++) {
-                    double x = fabs(v[((i * nb + j) * na + i) * nb + j]);
+                    double x = (double)fabs(v[((i * nb + j) * na + i) * nb + j]);
                     if (x > m) m = x;
                 }
             schwrz_out[tri_idx(A + 1, B + 1) - 1] = sqrt(m);
@@ -896,7 +986,9 @@ int oracle_schwarz(const oracle_basis *b, double *schwrz_out) {
 /* Exposes the Rys root routine for the table-accuracy tests. */
 void oracle_rys_roots(int n, double T, double thr, int rot, double *u, double *w) {
     init_tables();
-    rys_roots(n, T, thr, rot, u, w);
+    real_t ur[MAXROOT], wr[MAXROOT];
+    rys_roots(n, T, thr, rot, ur, wr);
+    for (int i = 0; i < n; i++) { u[i] = (double)ur[i]; w[i] = (double)wr[i]; }
 }
 
 int oracle_num_kernels(void) { return 21; }

@@ -45,10 +45,12 @@ class _Opts(ctypes.Structure):
 class _Counts(ctypes.Structure):
     _fields_ = [("c", (ctypes.c_int64 * 4) * 21), ("t_wall", ctypes.c_double * 21),
                 ("t_eval", ctypes.c_double * 21), ("nthreads", ctypes.c_int32),
-                ("fp", (ctypes.c_uint64 * 2) * 21)]
+                ("fp", (ctypes.c_uint64 * 2) * 21), ("ops", (ctypes.c_uint64 * 2) * 21)]
 
 
 _lib = None
+_oplib = None
+_OPCOUNT_PATH = os.path.join(_HERE, "_build", "liberi_opcount.so")
 
 
 def build():
@@ -128,6 +130,36 @@ def fock_build(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, my_rank=0,
     if return_counts:
         return f, counts
     return f
+
+
+def count_ops(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, sample_mod=1, sample_seed=0,
+              nthreads=0):
+    """Floating-point operations of this restatement of the reference
+    algorithm, per class, from the op-counting build (oracle/opcount.cpp) on
+    a hashed 1/sample_mod sample of the screened quartets: a (21, 4) array of
+    [operations in primitive-quartet work, operations in shell-quartet work,
+    primitive quartets evaluated, shell quartets evaluated]."""
+    global _oplib
+    if _oplib is None:
+        if not os.path.exists(_OPCOUNT_PATH):
+            build()
+        _oplib = ctypes.CDLL(_OPCOUNT_PATH)
+        _oplib.oracle_fock_build.argtypes = lib().oracle_fock_build.argtypes
+        _oplib.oracle_fock_build.restype = ctypes.c_int
+    keep = []
+    bs = _basis_struct(basis, keep)
+    n = int(basis["num_bas"])
+    d = np.ascontiguousarray(density, dtype=np.float64)
+    assert d.shape == (n * (n + 1) // 2,)
+    f = np.zeros_like(d)
+    opts = _Opts(schwarz_cut, eri_cut, 0, 1, sample_mod, sample_seed, nthreads, -1)
+    cnt = _Counts()
+    rc = _oplib.oracle_fock_build(ctypes.byref(bs), ctypes.byref(opts), d.ctypes.data_as(_F64P),
+                                  f.ctypes.data_as(_F64P), ctypes.byref(cnt))
+    if rc != 0:
+        raise RuntimeError("oracle op count failed: %d" % rc)
+    return np.array([[cnt.ops[k][0], cnt.ops[k][1], cnt.c[k][1], cnt.c[k][3]] for k in range(21)],
+                    dtype=np.float64)
 
 
 def schwarz(basis):

@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from gms_liberi_b200 import liberi
+from gms_liberi_b200 import molecules as M
 from conftest import ROOT
 
 
@@ -52,7 +53,12 @@ def test_options_validate():
     assert h.get_option("eri_cut") == pytest.approx(5e-11)
     h.set_option("precision", 1)
     assert h.get_option("precision") == 1
-    for name, val in [("nope", 1.0), ("precision", 2), ("schwarz_cut", -1.0)]:
+    # FP32-tier primitive screening: default 1e-8 of the cut, 0 disables
+    assert h.get_option("fp32_prim") == pytest.approx(1e-8)
+    h.set_option("fp32_prim", 0.0)
+    assert h.get_option("fp32_prim") == 0.0
+    for name, val in [("nope", 1.0), ("precision", 2), ("schwarz_cut", -1.0), ("fp32_prim", -1.0),
+                      ("fp32_prim", 2.0)]:
         with pytest.raises(liberi.LiberiError) as e:
             h.set_option(name, val)
         assert e.value.code == -1
@@ -162,3 +168,32 @@ def test_fortran_shim_matches_the_c_abi():
         n_f = 0 if not args.strip() else len(args.split(","))
         assert n_f == n_c, (cname, n_f, n_c)
         assert hasattr(lib, cname), cname
+
+
+def test_device_memory_limit_fails_setup_before_device_work():
+    # an allocation failure made on the host: the handle's byte limit is
+    # checked by the host half of setup, before any CUDA call, so this runs
+    # without a GPU and leaves the handle usable
+    b = M.ethane()
+    b["schwrz"] = np.ones(b["nsh"] * (b["nsh"] + 1) // 2)
+    h = liberi.liberi_create()
+    h.set_option("max_device_bytes", 1000.0)
+    assert h.get_option("max_device_bytes") == 1000.0
+    with pytest.raises(liberi.LiberiError) as e:
+        liberi.setup_from_basis(h, b)
+    assert e.value.code == -5 and "max_device_bytes" in str(e.value)
+    need = liberi.setup_bytes(b, 5e-11)
+    assert need > 1000
+    with pytest.raises(liberi.LiberiError) as e:
+        h.set_option("max_device_bytes", -1.0)
+    assert e.value.code == -1
+    liberi.liberi_destroy(h)
+
+
+def test_double_cleanup_and_destroy():
+    # liberi_cleanup on a handle that is not set up is a no-op
+    # (liberi_interface.F90:236), also twice in a row; destroy after cleanup
+    h = liberi.liberi_create()
+    liberi.liberi_cleanup(h)
+    liberi.liberi_cleanup(h)
+    liberi.liberi_destroy(h)

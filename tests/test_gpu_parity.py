@@ -207,6 +207,22 @@ def test_mixed_precision_error_bound(mol):
         assert np.abs(Fm - Fo).max() <= 1e-5
 
 
+def test_fp32_primitive_screening_error_bound():
+    # skipping FP32-tier primitive quartets below fp32_prim * fp32_cut stays
+    # within the tier's error bound and leaves the quartet set unchanged
+    b, nocc = _molecule("random_9")
+    D = M.density(b["num_bas"], nocc, seed=6)
+    Fo = oracle.fock_build(b, D, schwarz_cut=1e-10)
+    full, st0 = gpu_fock(b, D, schwarz_cut=1e-10, precision=1, fp32_cut=1e-3, fp32_prim=0.0)
+    for prim in (1e-8, 1e-6):
+        Fm, st = gpu_fock(b, D, schwarz_cut=1e-10, precision=1, fp32_cut=1e-3, fp32_prim=prim)
+        assert (st["fingerprint"] == st0["fingerprint"]).all()
+        assert abs(energy(D, Fm) - energy(D, Fo)) <= 1e-6, prim
+        # each skipped primitive quartet moves an F element by at most
+        # 6 * prim * cut; far fewer than 1e4 of them reach any one element
+        assert np.abs(Fm - full).max() <= 1e4 * 6 * prim * 1e-3, prim
+
+
 @pytest.mark.parametrize("nsize", [2, 3, 7])
 def test_balanced_rank_split(nsize):
     # cost-balanced contiguous slices: the same total F, even per-rank work

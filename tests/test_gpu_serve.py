@@ -54,3 +54,38 @@ def test_admission_bytes_equal_setup_allocation():
         liberi.fock(h, M.density(b["num_bas"], M.nocc_of(b)))
         assert liberi.setup_bytes(b, 1e-7) == h.stats()["device_bytes"]
         liberi.liberi_destroy(h)
+
+
+def test_hbm_budget_holds_sessions_back_on_the_device():
+    # slots are plentiful; the byte budget (room for the largest session and a
+    # little more) is what makes sessions wait
+    pool = _pool()
+    eng = LiberiEngine(precision=1, fp32_cut=1e-7, schwarz_cut=1e-10)
+    sizes = [eng.bytes_needed(b) for b in pool]
+    budget = max(sizes) + min(sizes) // 2
+    sessions = [Session(sid=i, basis=dict(pool[(i + 1) % len(pool)]), niter=2, seed=70 + i, arrival=0.0)
+                for i in range(6)]
+    srv = FockServer(eng, hbm_budget=budget, max_slots=64)
+    rep, done = srv.run(sessions)
+    assert rep["sessions"] == 6 and rep["builds"] == 12
+    assert rep["sessions_waited_for_bytes"] >= 1
+    assert rep["peak_reserved_bytes"] <= budget
+
+
+def test_cancelled_session_releases_and_others_are_unaffected():
+    pool = _pool()
+    eng = LiberiEngine(precision=1, fp32_cut=1e-7, schwarz_cut=1e-10)
+    sessions = [Session(sid=i, basis=dict(pool[i % len(pool)]), niter=4, seed=90 + i, arrival=0.0)
+                for i in range(3)]
+    srv = FockServer(eng, hbm_budget=8 << 30, max_slots=3, capture=True)
+    srv.cancel(1)  # before its first build: never launches, releases at once
+    rep, done = srv.run(sessions)
+    assert rep["cancelled"] == 1 and rep["sessions"] == 2
+    for s in done:
+        h = liberi.liberi_create()
+        for k, v in (("schwarz_cut", 1e-10), ("precision", 1), ("fp32_cut", 1e-7)):
+            h.set_option(k, v)
+        liberi.setup_from_basis(h, s.basis)
+        for it, D in enumerate(eng.density_sequence(s)):
+            assert np.abs(s.results[it] - liberi.fock(h, D)).max() <= TOL_SAME
+        liberi.liberi_destroy(h)

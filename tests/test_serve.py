@@ -131,3 +131,49 @@ def test_setup_bytes_dry_run():
         bad = dict(b)
         bad["ang_mom"] = [9] * b["nsh"]
         liberi.setup_bytes(bad)
+
+
+def test_waits_for_hbm_bytes_not_slots():
+    # plenty of slots: the second session is held back by the byte budget
+    eng = FakeEngine(dur=0.005)
+    srv = FockServer(eng, hbm_budget=1000, max_slots=64)
+    rep, _ = srv.run(_sessions([700, 600, 100], [0.0, 0.0, 0.0]))
+    assert rep["sessions"] == 3
+    assert rep["sessions_waited_for_bytes"] >= 1
+    assert eng.peak_resident <= 1000
+
+
+def test_cancel_queued_session_is_never_set_up():
+    eng = FakeEngine(dur=0.01)
+    srv = FockServer(eng, hbm_budget=1000, max_slots=1)
+    ss = _sessions([100, 100, 100], [0.0, 0.0, 0.0], niter=4)
+    ss[2].cancel_at = 0.005  # still queued behind the single slot
+    rep, done = srv.run(ss)
+    assert rep["cancelled"] == 1 and rep["sessions"] == 2
+    assert 2 not in eng.open_order
+    assert eng.resident == 0 and eng.live == 0
+
+
+def test_cancel_in_flight_session_finishes_its_build_and_releases():
+    eng = FakeEngine(dur=0.02)
+    srv = FockServer(eng, hbm_budget=1000, max_slots=4, capture=True)
+    ss = _sessions([300, 300], [0.0, 0.0], niter=10)
+    ss[0].cancel_at = 0.03  # during its second build
+    rep, done = srv.run(ss)
+    assert rep["cancelled"] == 1 and rep["sessions"] == 1
+    assert done[0].sid == 1 and len(done[0].latencies) == 10
+    # the cancelled session stopped after the build it had on the device
+    assert 1 <= ss[0].it < 10 and ss[0].state is None
+    assert eng.resident == 0 and eng.live == 0 and eng.inflight == 0
+
+
+def test_cancel_from_another_thread():
+    eng = FakeEngine(dur=0.01)
+    srv = FockServer(eng, hbm_budget=1000, max_slots=2)
+    ss = _sessions([100, 100, 100], [0.0, 0.0, 0.0], niter=20)
+    t = threading.Timer(0.05, srv.cancel, args=(1,))
+    t.start()
+    rep, done = srv.run(ss)
+    t.join()
+    assert rep["cancelled"] == 1 and {s.sid for s in done} == {0, 2}
+    assert eng.resident == 0
