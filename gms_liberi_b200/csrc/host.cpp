@@ -119,6 +119,14 @@ struct DeviceGuard {
     }
 };
 
+// A non-blocking stream at the device's greatest priority.
+static cudaError_t high_priority_stream(cudaStream_t *st) {
+    int least = 0, greatest = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e != cudaSuccess) return e;
+    return cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, greatest);
+}
+
 // ---- handle ------------------------------------------------------------------------
 struct liberi_handle_s {
     // options (defaults reproduce the reference constants)
@@ -1276,7 +1284,11 @@ int liberi_c_setup(liberi_handle h, int32_t nsh, int32_t natoms, int32_t num_bas
     h->num_procs = num_procs;
     std::vector<double4> shell_xyz;
     build_pairs(h->basis, h->pairs, shell_xyz);
-    CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    // the handle's own stream at the highest priority: setup's kernels (the
+    // primitive bounds) and copies then overtake the queued CTAs of builds
+    // already running on the GPU (a serving loop sets sessions up while
+    // others compute); builds through liberi_c_fock_build share it
+    CUDA_TRY(high_priority_stream(&h->stream));
     rc = upload_basis(h, shell_xyz);
     if (!rc) rc = replan(h);
     if (rc) {
@@ -1817,7 +1829,7 @@ int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgto
     CUDA_TRY(cudaGetDevice(&tmp.device));  // the caller's current device
     std::vector<double4> shell_xyz;
     build_pairs(tmp.basis, tmp.pairs, shell_xyz);
-    CUDA_TRY(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking));
+    CUDA_TRY(high_priority_stream(&tmp.stream));
     rc = upload_basis(&tmp, shell_xyz);
     double *d_out = nullptr;
     const int npairs = tmp.pairs.class_off[NPC];
