@@ -24,8 +24,9 @@ updated between builds.  Sessions arrive over time; the server
 
 The scheduling logic is independent of the engine (`Engine` below), so it is
 tested on the CPU with a fake engine; `LiberiEngine` drives the CUDA library.
-Session setup (host planning, Schwarz table) runs on one worker thread so the
-dispatch loop keeps launching builds meanwhile.
+Session setup (host planning, device upload) runs on a small pool of worker
+threads (`setup_workers`), so the dispatch loop keeps launching builds and
+sessions admitted together are set up side by side.
 """
 import collections
 import threading
@@ -84,8 +85,9 @@ class Engine:
 
 
 class FockServer:
-    def __init__(self, engine, hbm_budget, max_slots=64, capture=False, poll_s=2e-4):
+    def __init__(self, engine, hbm_budget, max_slots=64, capture=False, poll_s=2e-4, setup_workers=4):
         self.engine = engine
+        self.setup_workers = max(1, int(setup_workers))
         self.budget = int(hbm_budget)
         self.max_slots = int(max_slots)
         self.capture = capture
@@ -142,8 +144,9 @@ class FockServer:
                 with lock:
                     setup_done.append(s)
 
-        th = threading.Thread(target=worker, daemon=True)
-        th.start()
+        ths = [threading.Thread(target=worker, daemon=True) for _ in range(self.setup_workers)]
+        for th in ths:
+            th.start()
         try:
             while pending or waiting or active or in_setup:
                 if errors:
@@ -227,7 +230,8 @@ class FockServer:
             with lock:
                 stop[0] = True
                 lock.notify_all()
-            th.join()
+            for th in ths:
+                th.join()
         wall = now()
         lat = np.array([x for s in finished for x in s.latencies]) * 1e3
         nb = int(lat.size)
