@@ -182,6 +182,10 @@ struct DeviceBuffers {
     double *D = nullptr, *F = nullptr;
     double *Dsq = nullptr;  // the build's D as a full n x n matrix (class kernels read it)
     float *Df = nullptr;    // FP32 tier: the same in single precision
+    // open-shell builds (made at the first one): the Coulomb and exchange
+    // densities as two consecutive full n x n matrices, and their float copies
+    double *uhf_sq = nullptr;
+    float *uhf_sqf = nullptr;
     long long *scratch_total = nullptr;  // device counters (mixed split)
     size_t bytes = 0;
 };
@@ -210,6 +214,8 @@ struct LaunchCtx {
     // and the primitive screening cut (fp32_prim * fp32_cut; 0 = off)
     const unsigned long long *maxd = nullptr;
     double prim_cut = 0.0;
+    // open-shell builds: the exchange terms read a second full matrix at D + k_offset (0 = D itself)
+    size_t k_offset = 0;
 };
 
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
@@ -234,6 +240,9 @@ cudaError_t launch_split_batch(int nitems, const int4 *items, const ClassView *d
                                int4 *tasks32, int *counts, cudaStream_t stream);
 // full n x n copy of a packed density, and its float copy when sqf is non-null
 cudaError_t launch_unpack(const double *packed, int n, double *sq, float *sqf, cudaStream_t st);
+// open-shell builds: sq = ca * A + cb * B from two packed matrices (full n x n, float copy when sqf)
+cudaError_t launch_unpack_combo(const double *pa, const double *pb, double ca, double cb, int n, double *sq,
+                                float *sqf, cudaStream_t st);
 cudaError_t launch_maxabs(const double *x, long long n, unsigned long long *out,
                           cudaStream_t stream);
 cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_x, const double *ket_x,

@@ -825,7 +825,12 @@ static DevPlan dev_plan_of(liberi_handle h, int k) {
     return dp;
 }
 
-static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaStream_t st) {
+// One Fock build on device buffers.  Closed shell (dDb null): F = J(D) - K(D)
+// in the reference's DIRFCK units.  Open shell (dDb non-null, spin 0 or 1):
+// F_spin = J(D + Db) - K(2 D_spin), D the alpha density: the kernels read the
+// Coulomb density and, k_offset further on, the exchange density.
+static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaStream_t st,
+                           const double *dDb = nullptr, int spin = 0) {
     if (h->plan_dirty) {
         int rc = replan(h);
         if (rc) return rc;
@@ -848,9 +853,28 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     ctx.Df = h->dev.Df;
     ctx.maxd = mixed ? h->d_maxd : nullptr;
     ctx.prim_cut = mixed ? h->fp32_prim * h->fp32_cut : 0.0;
-    // the class kernels read D as a full matrix (and in float for the FP32 tier)
-    CUDA_TRY(launch_unpack(dD, b.num_bas, h->dev.Dsq, mixed ? h->dev.Df : nullptr, st));
-    if (mixed) CUDA_TRY(launch_maxabs(dD, ntri, h->d_maxd, st));
+    if (!dDb) {
+        // the class kernels read D as a full matrix (and in float for the FP32 tier)
+        CUDA_TRY(launch_unpack(dD, b.num_bas, h->dev.Dsq, mixed ? h->dev.Df : nullptr, st));
+        if (mixed) CUDA_TRY(launch_maxabs(dD, ntri, h->d_maxd, st));
+    } else {
+        const size_t nsq = (size_t)b.num_bas * b.num_bas;
+        if (!h->dev.uhf_sq) {  // first open-shell build of this handle
+            CUDA_TRY(cudaMallocAsync((void **)&h->dev.uhf_sq, 2 * nsq * sizeof(double), h->stream));
+            h->allocs.push_back(h->dev.uhf_sq);
+            CUDA_TRY(cudaMallocAsync((void **)&h->dev.uhf_sqf, 2 * nsq * sizeof(float), h->stream));
+            h->allocs.push_back(h->dev.uhf_sqf);
+            CUDA_TRY(cudaStreamSynchronize(h->stream));
+        }
+        CUDA_TRY(launch_unpack_combo(dD, dDb, 1.0, 1.0, b.num_bas, h->dev.uhf_sq, mixed ? h->dev.uhf_sqf : nullptr, st));
+        CUDA_TRY(launch_unpack_combo(dD, dDb, spin == 0 ? 2.0 : 0.0, spin == 0 ? 0.0 : 2.0, b.num_bas,
+                                     h->dev.uhf_sq + nsq, mixed ? h->dev.uhf_sqf + nsq : nullptr, st));
+        // the mixed tier's bound uses the largest element of both densities
+        if (mixed) CUDA_TRY(launch_maxabs(h->dev.uhf_sq, (long long)(2 * nsq), h->d_maxd, st));
+        ctx.D = h->dev.uhf_sq;
+        ctx.Df = h->dev.uhf_sqf;
+        ctx.k_offset = nsq;
+    }
     for (int k = 0; k < NKERN; k++) h->ev_recorded[k] = false;
     // mixed precision: every class's FP64 task list (the few quartets above
     // fp32_cut, the costliest ones, in small low-occupancy launches) runs on
@@ -1310,6 +1334,55 @@ int liberi_c_fock_build_device(liberi_handle h, const double *d_density, double 
     int rc = build_on_device(h, d_density, d_fock, st);
     if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
+    return LIBERI_OK;
+}
+
+int liberi_c_fock_build_uhf_device(liberi_handle h, const double *d_density_a, const double *d_density_b,
+                                   double *d_fock_a, double *d_fock_b, void *stream) {
+    if (!h) return fail(LIBERI_E_ARG, "liberi_fock_build_uhf: null handle");
+    if (!h->initialized) return fail(LIBERI_E_STATE, "liberi_fock_build_uhf called before liberi_setup");
+    if (!d_density_a || !d_density_b || !d_fock_a || !d_fock_b)
+        return fail(LIBERI_E_ARG, "liberi_fock_build_uhf: null device buffer");
+    DeviceGuard dev_guard(h->device);
+    CUDA_TRY(dev_guard.err);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    int rc = build_on_device(h, d_density_a, d_fock_a, st, d_density_b, 0);
+    if (!rc) rc = build_on_device(h, d_density_a, d_fock_b, st, d_density_b, 1);
+    if (rc) return rc;
+    CUDA_TRY(cudaGetLastError());
+    return LIBERI_OK;
+}
+
+int liberi_c_fock_build_uhf(liberi_handle h, const double *density_a, const double *density_b, double *fock_a,
+                            double *fock_b, int32_t matrix_size) {
+    if (!h) return fail(LIBERI_E_ARG, "liberi_fock_build_uhf: null handle");
+    if (!h->initialized) return fail(LIBERI_E_STATE, "liberi_fock_build_uhf called before liberi_setup");
+    const long long n = h->basis.num_bas;
+    if ((long long)matrix_size != n * (n + 1) / 2)
+        return fail(LIBERI_E_SIZE, "liberi_fock_build_uhf: matrix_size %d != num_bas(num_bas+1)/2 = %lld",
+                    matrix_size, n * (n + 1) / 2);
+    if (!density_a || !density_b || !fock_a || !fock_b) return fail(LIBERI_E_ARG, "liberi_fock_build_uhf: null buffer");
+    DeviceGuard dev_guard(h->device);
+    CUDA_TRY(dev_guard.err);
+    cudaStream_t st = h->stream;
+    const size_t bytes = (size_t)matrix_size * sizeof(double);
+    // the beta density and Fock matrix in a stream-ordered scratch pair beside the handle's own D and F
+    double *db = nullptr, *fb = nullptr;
+    CUDA_TRY(cudaMallocAsync((void **)&db, 2 * bytes, st));
+    fb = db + matrix_size;
+    cudaError_t e = cudaMemcpyAsync(h->dev.D, density_a, bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, density_b, bytes, cudaMemcpyHostToDevice, st);
+    int rc = LIBERI_OK;
+    if (e == cudaSuccess) {
+        rc = build_on_device(h, h->dev.D, h->dev.F, st, db, 0);
+        if (!rc) rc = build_on_device(h, h->dev.D, fb, st, db, 1);
+    }
+    if (e == cudaSuccess && !rc) e = cudaMemcpyAsync(fock_a, h->dev.F, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && !rc) e = cudaMemcpyAsync(fock_b, fb, bytes, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(db, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (rc) return rc;
+    CUDA_TRY(e);
     return LIBERI_OK;
 }
 

@@ -215,6 +215,7 @@ static ClassArgs single_args(int k, const LaunchCtx &ctx, const DevPlan &plan, c
     a.cviews = nullptr;
     a.maxd = ctx.maxd;
     a.prim_cut = ctx.prim_cut;
+    a.k_offset = ctx.k_offset;
     return a;
 }
 
@@ -247,6 +248,7 @@ cudaError_t launch_class_batch(int k, const LaunchCtx &ctx, const int4 *tasks, i
     a.cviews = d_cviews;
     a.maxd = ctx.maxd;
     a.prim_cut = ctx.prim_cut;
+    a.k_offset = ctx.k_offset;
 #define LIBERI_CASE(kk, A, B, C, D) \
     case kk: return launch_t<A, B, C, D>(a, precision, 0, ctx.stream);
     switch (k) { LIBERI_CLASSES(LIBERI_CASE) }
@@ -264,6 +266,30 @@ __global__ void unpack_kernel(const double *__restrict__ packed, unsigned n, dou
         sq[i] = d;
         if (sqf) sqf[i] = (float)d;
     }
+}
+
+// Open-shell builds: sq = ca * A + cb * B as a full n x n matrix (and its float copy)
+__global__ void unpack_combo_kernel(const double *__restrict__ pa, const double *__restrict__ pb, double ca,
+                                    double cb, unsigned n, double *__restrict__ sq, float *__restrict__ sqf) {
+    const long long total = (long long)n * n;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+        const unsigned i = (unsigned)g, r = i / n, c = i - r * n;
+        const unsigned t = tri0(r, c);
+        const double d = ca * pa[t] + cb * pb[t];
+        sq[i] = d;
+        if (sqf) sqf[i] = (float)d;
+    }
+}
+
+cudaError_t launch_unpack_combo(const double *pa, const double *pb, double ca, double cb, int n, double *sq,
+                                float *sqf, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int threads = 256;
+    const long long want = ((long long)n * n + threads - 1) / threads;
+    const int blocks = (int)(want < 148LL * 8 ? want : 148LL * 8);
+    unpack_combo_kernel<<<blocks, threads, 0, st>>>(pa, pb, ca, cb, (unsigned)n, sq, sqf);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_unpack(const double *packed, int n, double *sq, float *sqf, cudaStream_t st) {

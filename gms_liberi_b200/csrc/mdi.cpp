@@ -13,6 +13,7 @@
 // NCCL), as the reference's caller-side reduction.
 #include <cstring>
 #include <new>
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -33,6 +34,7 @@ struct liberi_mdi_s {
     std::vector<int32_t> ang_mom, contr_num, sh_loc, atom_num, atom_loc, start_bas, end_bas;
     std::vector<double> exponents, coef_s, coef_p, coef_d, coef_f, coords, schwrz;
     std::vector<double> density, density_b;
+    std::vector<double> fock_b;  // beta partial F of the last open-shell '<FOCK'
 };
 
 namespace {
@@ -191,10 +193,23 @@ int liberi_c_mdi_execute(liberi_mdi s, const char *command, void *buffer, int64_
             if (!s->handle) return set_error(LIBERI_E_STATE, "MDI <FOCK before >SCHWZ_INT set the handle up");
             if ((int64_t)s->density.size() != want)
                 return set_error(LIBERI_E_STATE, "MDI <FOCK before >AO_DENS delivered the density");
-            return liberi_c_fock_build(s->handle, s->density.data(), (double *)buffer, (int32_t)want);
+            s->fock_b.clear();
+            if ((int64_t)s->density_b.size() != want)  // closed shell
+                return liberi_c_fock_build(s->handle, s->density.data(), (double *)buffer, (int32_t)want);
+            // open shell ('>AO_DENS_B' delivered the beta density): alpha F now,
+            // beta F kept for '<FOCK_B' (the reference registers both commands,
+            // liberi_mdi_api.F90:395-421, but builds closed-shell F only)
+            s->fock_b.assign((size_t)want, 0.0);
+            const int rc = liberi_c_fock_build_uhf(s->handle, s->density.data(), s->density_b.data(), (double *)buffer,
+                                                   s->fock_b.data(), (int32_t)want);
+            if (rc) s->fock_b.clear();
+            return rc;
         }
         case K_FOCK_B:
-            return set_error(LIBERI_E_UNSUPPORTED, "MDI <FOCK_B: open-shell (UHF/ROHF) builds are not provided");
+            if ((int64_t)s->fock_b.size() != want)
+                return set_error(LIBERI_E_STATE, "MDI <FOCK_B needs an open-shell <FOCK first (>AO_DENS_B, then <FOCK)");
+            std::copy(s->fock_b.begin(), s->fock_b.end(), (double *)buffer);
+            return LIBERI_OK;
         default:
             return set_error(LIBERI_E_ARG, "MDI command not recognized");
     }

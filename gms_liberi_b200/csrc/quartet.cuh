@@ -698,8 +698,10 @@ struct QuartetCtx {
     int bfA, bfB, bfC, bfD;
     bool iandj, kandl, same;
     T cut;
-    const T *__restrict__ Dm;  // the build's density as a full n x n matrix
-    unsigned ld;               // n
+    const T *__restrict__ Dm;   // the build's density as a full n x n matrix (the Coulomb terms)
+    const T *__restrict__ DmK;  // the density of the exchange terms: Dm itself, or (open-shell builds)
+                                // a second n x n matrix
+    unsigned ld;                // n
 };
 
 // D(i, j) from the full matrix: the row is the CTA's bra shell (A or B) or
@@ -967,9 +969,9 @@ __device__ __forceinline__ void digest_row_distinct(const R (&a)[ncart(LB)][ncar
 #pragma unroll
     for (int ib = 0; ib < NB; ib++) dAB[ib] = R(4) * dget(Dm, qc.ld, mu, qc.bfB + ib);
 #pragma unroll
-    for (int ic = 0; ic < NC; ic++) dAC[ic] = dget(Dm, qc.ld, mu, qc.bfC + ic);
+    for (int ic = 0; ic < NC; ic++) dAC[ic] = dget(qc.DmK, qc.ld, mu, qc.bfC + ic);
 #pragma unroll
-    for (int id = 0; id < ND; id++) dAD[id] = dget(Dm, qc.ld, mu, qc.bfD + id);
+    for (int id = 0; id < ND; id++) dAD[id] = dget(qc.DmK, qc.ld, mu, qc.bfD + id);
     R kac[NC], kad[ND];
 #pragma unroll
     for (int ib = 0; ib < NB; ib++) jab[ib] = R(0);
@@ -1041,10 +1043,10 @@ __device__ __forceinline__ void digest_row_general(const R (&a)[ncart(LB)][ncart
                 if ((mu == la && nu == si) || (mu == si && nu == la)) v *= R(0.5);
                 jab[ib] += R(4) * v * dget(qc.Dm, qc.ld, la, si);
                 kb.cd(ic, id) += R(4) * v * dmn;
-                kac[ic] += v * dget(qc.Dm, qc.ld, nu, si);
-                kad[id] += v * dget(qc.Dm, qc.ld, nu, la);
-                kb.bc(ib, ic) += v * dget(qc.Dm, qc.ld, mu, si);
-                kb.bd(ib, id) += v * dget(qc.Dm, qc.ld, mu, la);
+                kac[ic] += v * dget(qc.DmK, qc.ld, nu, si);
+                kad[id] += v * dget(qc.DmK, qc.ld, nu, la);
+                kb.bc(ib, ic) += v * dget(qc.DmK, qc.ld, mu, si);
+                kb.bd(ib, id) += v * dget(qc.DmK, qc.ld, mu, la);
             }
         }
     }
@@ -1098,9 +1100,9 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
 #pragma unroll
             for (int ib = 0; ib < NB; ib++) {
 #pragma unroll
-                for (int id = 0; id < ND; id++) dBD[ib][id] = dget(qc.Dm, qc.ld, qc.bfB + ib, qc.bfD + id);
+                for (int id = 0; id < ND; id++) dBD[ib][id] = dget(qc.DmK, qc.ld, qc.bfB + ib, qc.bfD + id);
 #pragma unroll
-                for (int ic = 0; ic < NC; ic++) dBC[ib][ic] = dget(qc.Dm, qc.ld, qc.bfB + ib, qc.bfC + ic);
+                for (int ic = 0; ic < NC; ic++) dBC[ib][ic] = dget(qc.DmK, qc.ld, qc.bfB + ib, qc.bfC + ic);
             }
         }
 #pragma unroll
@@ -1177,6 +1179,7 @@ struct ClassArgs {
     const MolView *mols;     // batched launch: per-molecule data (task.w), else null
     const ClassView *cviews; // batched launch: per-molecule lists of this class
     const unsigned long long *maxd;  // FP32 tier: max|D| bits (per molecule for batches)
+    size_t k_offset;                 // exchange density at D + k_offset (0: D itself; n*n for open-shell builds)
     double prim_cut;                 // FP32 tier: primitive screening cut (0 = off)
 };
 
@@ -1288,6 +1291,7 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
         // shells have distinct first functions: same shells <=> same first functions
         qc.iandj = sab.x == sab.y; qc.kandl = qc.bfC == qc.bfD; qc.same = bfA == qc.bfC && bfB == qc.bfD;
         qc.cut = R(a.cut); qc.Dm = LIBERI_D; qc.ld = (unsigned)LIBERI_NBF;
+        qc.DmK = LIBERI_D + a.k_offset;  // open-shell builds: the exchange density follows D
         constexpr bool SM = PassShape<LA, LB, LC, LD, R, V>::NPASS > 1;
         KBuf<NB, NC, ND, SM, R> kb;
         kb.s = slots + threadIdx.x;

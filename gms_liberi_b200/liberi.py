@@ -37,7 +37,7 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_autotune", "liberi_c_rys_eval_f32", "liberi_c_setup_bytes",
            "liberi_c_set_class_variant", "liberi_c_get_class_variant", "liberi_c_mdi_create",
            "liberi_c_mdi_payload", "liberi_c_mdi_execute", "liberi_c_mdi_destroy",
-           "liberi_c_quartet_fingerprint"]
+           "liberi_c_quartet_fingerprint", "liberi_c_fock_build_uhf", "liberi_c_fock_build_uhf_device"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -91,6 +91,9 @@ def lib():
                                        _F64P, _F64P, _F64P, _F64P, _F64P, _F64P]
         L.liberi_c_get_stats.argtypes = [H, ctypes.POINTER(Stats)]
         L.liberi_c_quartet_fingerprint.argtypes = [H, ctypes.POINTER(ctypes.c_uint64)]
+        L.liberi_c_fock_build_uhf.argtypes = [H, _F64P, _F64P, _F64P, _F64P, ctypes.c_int32]
+        L.liberi_c_fock_build_uhf_device.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                     ctypes.c_void_p, ctypes.c_void_p]
         L.liberi_c_setup_bytes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                            _I32P, _I32P, _I32P, _I32P, _I32P,
                                            _F64P, _F64P, _F64P, _F64P, _F64P, _F64P, ctypes.c_double,
@@ -291,6 +294,21 @@ def fock(handle, density):
     out = np.zeros(ntri)
     liberi_fock_build(handle, density, out, ntri)
     return out
+
+
+def fock_uhf(handle, density_a, density_b):
+    """Open-shell partials (F_alpha, F_beta) = (J(Da+Db) - K(2 Da), J(Da+Db) - K(2 Db)) for packed
+    alpha and beta densities (liberi_c_fock_build_uhf); Da = Db = D/2 gives the closed-shell F."""
+    n = handle.num_bas
+    ntri = n * (n + 1) // 2
+    da = np.ascontiguousarray(density_a, dtype=np.float64)
+    db = np.ascontiguousarray(density_b, dtype=np.float64)
+    if da.shape != (ntri,) or db.shape != (ntri,):
+        raise ValueError("densities must be packed of length %d" % ntri)
+    fa, fb = np.zeros(ntri), np.zeros(ntri)
+    _check(lib().liberi_c_fock_build_uhf(handle._h, da.ctypes.data_as(_F64P), db.ctypes.data_as(_F64P),
+                                         fa.ctypes.data_as(_F64P), fb.ctypes.data_as(_F64P), ntri))
+    return fa, fb
 
 
 def microbench(kind):

@@ -140,6 +140,23 @@ int liberi_c_get_option(liberi_handle handle, const char *name, double *value);
 int liberi_c_fock_build_device(liberi_handle handle, const double *d_density, double *d_fock,
                                void *stream);
 
+/* Open-shell (UHF) Fock build.  No counterpart in the reference: its MDI
+ * plugin registers ">AO_DENS_B" and "<FOCK_B" (liberi_mdi_api.F90:395-421)
+ * but libERI builds closed-shell F only.  With the alpha and beta densities
+ * (packed like D) it returns, this rank's partials in the units of
+ * liberi_c_fock_build,
+ *     F_alpha = J(D_alpha + D_beta) - K(2 D_alpha),
+ *     F_beta  = J(D_alpha + D_beta) - K(2 D_beta),
+ * where J and K are the Coulomb and exchange updates of DIRFCK
+ * (int0000.F90:241-311), so that D_alpha = D_beta = D/2 gives the RHF F.
+ * Two builds over the same screened quartets; mixed precision splits at the
+ * largest element of both densities.  The host variant keeps D_alpha/F_alpha
+ * in the handle's buffers and the beta pair in a scratch allocation. */
+int liberi_c_fock_build_uhf(liberi_handle handle, const double *density_a, const double *density_b,
+                            double *fock_a, double *fock_b, int32_t matrix_size);
+int liberi_c_fock_build_uhf_device(liberi_handle handle, const double *d_density_a, const double *d_density_b,
+                                   double *d_fock_a, double *d_fock_b, void *stream);
+
 /* Schwarz table generator: schwrz_out[ia(max)+min] = sqrt(max_components
  * |(ab|ab)|) over shell pairs, computed on the device (GAMESS supplies this
  * table to the reference, liberi_interface.F90:128-129). */
@@ -279,9 +296,11 @@ const char *liberi_c_kernel_name(int32_t k);
  * writes this rank's partial F; the shim sums the ranks' partials (MPI_Reduce
  * in the reference, an NCCL reduction on GPUs) before sending.  'EXIT' sets
  * *terminate and keeps the state for the next launch; 'EXIT_CONVERGED' also
- * releases the handle.  Open-shell commands ('<FOCK_B') return
- * LIBERI_E_UNSUPPORTED; commands the reference registers without handling
- * ('<COORDS', '>FOCK', '>FOCK_B') and unknown ones return LIBERI_E_ARG.
+ * releases the handle.  Open shell: after '>AO_DENS_B' (the beta density),
+ * '<FOCK' returns the alpha F of liberi_c_fock_build_uhf and '<FOCK_B' the
+ * beta F of the same build (LIBERI_E_STATE without one); commands the
+ * reference registers without handling ('<COORDS', '>FOCK', '>FOCK_B') and
+ * unknown ones return LIBERI_E_ARG.
  * '>RANK_ID' / '>NUM_PROCS' (registered, not handled by the reference) set the
  * rank split used at setup; liberi_c_mdi_create takes the same from the
  * shim's communicator. */

@@ -726,8 +726,10 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
 }
 
 /* =============================== DIRFCK ===================================== */
+/* Dm: the density of the Coulomb updates (F(ij) += 4 v D(kl)); Dk: that of the
+ * exchange updates (F(ik) -= v D(jl) ...), Dm itself for a closed-shell build */
 static int64_t dirfck(const ctx_t *c, int A, int B, int C, int D, const real_t *v,
-                      double cut, const double *Dm, double *F) {
+                      double cut, const double *Dm, const double *Dk, double *F) {
     const oracle_basis *b = c->b;
     int na = NCART[b->ang_mom[A] - 1], nb = NCART[b->ang_mom[B] - 1];
     int nc = NCART[b->ang_mom[C] - 1], nd = NCART[b->ang_mom[D] - 1];
@@ -769,10 +771,10 @@ static int64_t dirfck(const ctx_t *c, int A, int B, int C, int D, const real_t *
                     real_t v4 = 4.0 * val;
                     F[ij - 1] = (double)(F[ij - 1] + v4 * Dm[kl - 1]);
                     F[kl - 1] = (double)(F[kl - 1] + v4 * Dm[ij - 1]);
-                    F[ik - 1] = (double)(F[ik - 1] - val * Dm[jl - 1]);
-                    F[jl - 1] = (double)(F[jl - 1] - val * Dm[ik - 1]);
-                    F[il - 1] = (double)(F[il - 1] - val * Dm[jk - 1]);
-                    F[jk - 1] = (double)(F[jk - 1] - val * Dm[il - 1]);
+                    F[ik - 1] = (double)(F[ik - 1] - val * Dk[jl - 1]);
+                    F[jl - 1] = (double)(F[jl - 1] - val * Dk[ik - 1]);
+                    F[il - 1] = (double)(F[il - 1] - val * Dk[jk - 1]);
+                    F[jk - 1] = (double)(F[jk - 1] - val * Dk[il - 1]);
                 }
             }
         }
@@ -838,8 +840,20 @@ static uint64_t quartet_fp(int A, int B, int C, int D) {
 }
 
 /* ============================== driver ====================================== */
+int oracle_fock_build_jk(const oracle_basis *b, const oracle_opts *o, const double *Dm, const double *Dk,
+                         double *F, oracle_counts *cnt);
+
+/* Closed-shell build (liberi_fock_build): one density for every update. */
 int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double *Dm,
                       double *F, oracle_counts *cnt) {
+    return oracle_fock_build_jk(b, o, Dm, Dm, F, cnt);
+}
+
+/* Build with separate Coulomb (Dm) and exchange (Dk) densities: the open-shell
+ * form F_spin = J(D_alpha + D_beta) - K(2 D_spin) is Dm = D_alpha + D_beta,
+ * Dk = 2 D_spin (libERI itself is closed-shell only). */
+int oracle_fock_build_jk(const oracle_basis *b, const oracle_opts *o, const double *Dm, const double *Dk,
+                         double *F, oracle_counts *cnt) {
     init_tables();
     int64_t nbf = b->num_bas, ntri = nbf * (nbf + 1) / 2;
     for (int64_t i = 0; i < ntri; i++) F[i] = 0.0; /* liberi_driver.F90:64 */
@@ -915,7 +929,7 @@ int oracle_fock_build(const oracle_basis *b, const oracle_opts *o, const double 
                     const uint64_t o0 = ORACLE_OPS();
                     c_prim += eri_quartet(&c, A, B, C, D, pb, bi, pk, ki, kd, vbuf);
                     const uint64_t o1 = ORACLE_OPS();
-                    c_dig += dirfck(&c, A, B, C, D, vbuf, dcut, Dm, Ft);
+                    c_dig += dirfck(&c, A, B, C, D, vbuf, dcut, Dm, Dk, Ft);
                     /* primitive work up to eri_quartet's mark; its normalisation
                      * and the digestion are shell-quartet work */
                     ops_prim += ORACLE_MARKED() - o0;

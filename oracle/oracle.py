@@ -67,6 +67,9 @@ def lib():
         _lib.oracle_fock_build.argtypes = [ctypes.POINTER(_Basis), ctypes.POINTER(_Opts),
                                            _F64P, _F64P, ctypes.POINTER(_Counts)]
         _lib.oracle_fock_build.restype = ctypes.c_int
+        _lib.oracle_fock_build_jk.argtypes = [ctypes.POINTER(_Basis), ctypes.POINTER(_Opts),
+                                              _F64P, _F64P, _F64P, ctypes.POINTER(_Counts)]
+        _lib.oracle_fock_build_jk.restype = ctypes.c_int
         _lib.oracle_schwarz.argtypes = [ctypes.POINTER(_Basis), _F64P]
         _lib.oracle_schwarz.restype = ctypes.c_int
         _lib.oracle_rys_roots.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
@@ -160,6 +163,32 @@ def count_ops(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, sample_mod=1,
         raise RuntimeError("oracle op count failed: %d" % rc)
     return np.array([[cnt.ops[k][0], cnt.ops[k][1], cnt.c[k][1], cnt.c[k][3]] for k in range(21)],
                     dtype=np.float64)
+
+
+def fock_build_uhf(basis, density_a, density_b, **kw):
+    """Open-shell partials (F_alpha, F_beta) = (J(Da + Db) - K(2 Da), J(Da + Db) - K(2 Db)) in the
+    units of fock_build; keyword options as fock_build (no counts)."""
+    out = []
+    for ds in (density_a, density_b):
+        out.append(_build_jk(basis, np.asarray(density_a) + np.asarray(density_b), 2.0 * np.asarray(ds), **kw))
+    return out[0], out[1]
+
+
+def _build_jk(basis, dj, dk, *, schwarz_cut=5e-11, eri_cut=5e-11, my_rank=0, num_procs=1, nthreads=0):
+    keep = []
+    bs = _basis_struct(basis, keep)
+    n = int(basis["num_bas"])
+    dj = np.ascontiguousarray(dj, dtype=np.float64)
+    dk = np.ascontiguousarray(dk, dtype=np.float64)
+    assert dj.shape == dk.shape == (n * (n + 1) // 2,)
+    f = np.zeros_like(dj)
+    opts = _Opts(schwarz_cut, eri_cut, my_rank, num_procs, 1, 0, nthreads, -1)
+    cnt = _Counts()
+    rc = lib().oracle_fock_build_jk(ctypes.byref(bs), ctypes.byref(opts), dj.ctypes.data_as(_F64P),
+                                    dk.ctypes.data_as(_F64P), f.ctypes.data_as(_F64P), ctypes.byref(cnt))
+    if rc != 0:
+        raise RuntimeError("oracle_fock_build_jk failed: %d" % rc)
+    return f
 
 
 def schwarz(basis):

@@ -37,9 +37,9 @@ def test_errors():
     with pytest.raises(liberi.LiberiError) as e:  # before >SCHWZ_INT
         m.recv("<FOCK")
     assert e.value.code == -2
-    with pytest.raises(liberi.LiberiError) as e:
+    with pytest.raises(liberi.LiberiError) as e:  # no open-shell <FOCK yet
         m.recv("<FOCK_B")
-    assert e.value.code == -6
+    assert e.value.code == -2
     with pytest.raises(liberi.LiberiError) as e:  # wrong payload length
         m._run(">AO_DENS", np.zeros(3), 3)
     assert e.value.code == -3
