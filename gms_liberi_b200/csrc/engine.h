@@ -262,5 +262,7 @@ int schwarz_host_inputs(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mx
                         const double *contr_coef_p, const double *contr_coef_d, const double *coords,
                         BasisHost &basis, PairsHost &pairs, std::vector<double4> &shell_xyz);
 int set_error(int code, const char *msg);
+// the CUDA device of an NCCL communicator (comm.cpp), -1 for none
+int comm_device(struct liberi_comm_s *comm);
 
 }  // namespace liberi

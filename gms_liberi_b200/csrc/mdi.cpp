@@ -35,6 +35,7 @@ struct liberi_mdi_s {
     std::vector<double> exponents, coef_s, coef_p, coef_d, coef_f, coords, schwrz;
     std::vector<double> density, density_b;
     std::vector<double> fock_b;  // beta partial F of the last open-shell '<FOCK'
+    liberi_comm comm = nullptr;  // NCCL sum of the ranks' partials, or none (the shim sums)
 };
 
 namespace {
@@ -177,6 +178,8 @@ int liberi_c_mdi_execute(liberi_mdi s, const char *command, void *buffer, int64_
                 int rc = liberi_c_create(&s->handle);
                 if (rc) return rc;
             }
+            // with an NCCL communicator, each rank builds on its communicator's device
+            if (s->comm) liberi_c_set_option(s->handle, "device", (double)liberi::comm_device(s->comm));
             int rc = liberi_c_setup(s->handle, s->nsh, s->natoms, s->num_bas, s->mxgtot, or_null(s->ang_mom),
                                     or_null(s->contr_num), or_null(s->sh_loc), or_null(s->atom_num),
                                     or_null(s->atom_loc), or_null(s->start_bas), or_null(s->end_bas),
@@ -194,14 +197,19 @@ int liberi_c_mdi_execute(liberi_mdi s, const char *command, void *buffer, int64_
             if ((int64_t)s->density.size() != want)
                 return set_error(LIBERI_E_STATE, "MDI <FOCK before >AO_DENS delivered the density");
             s->fock_b.clear();
-            if ((int64_t)s->density_b.size() != want)  // closed shell
-                return liberi_c_fock_build(s->handle, s->density.data(), (double *)buffer, (int32_t)want);
+            if ((int64_t)s->density_b.size() != want) {  // closed shell
+                int rc = liberi_c_fock_build(s->handle, s->density.data(), (double *)buffer, (int32_t)want);
+                if (!rc && s->comm) rc = liberi_c_comm_reduce_host(s->comm, (double *)buffer, (double *)buffer, want);
+                return rc;
+            }
             // open shell ('>AO_DENS_B' delivered the beta density): alpha F now,
             // beta F kept for '<FOCK_B' (the reference registers both commands,
             // liberi_mdi_api.F90:395-421, but builds closed-shell F only)
             s->fock_b.assign((size_t)want, 0.0);
-            const int rc = liberi_c_fock_build_uhf(s->handle, s->density.data(), s->density_b.data(), (double *)buffer,
-                                                   s->fock_b.data(), (int32_t)want);
+            int rc = liberi_c_fock_build_uhf(s->handle, s->density.data(), s->density_b.data(), (double *)buffer,
+                                             s->fock_b.data(), (int32_t)want);
+            if (!rc && s->comm) rc = liberi_c_comm_reduce_host(s->comm, (double *)buffer, (double *)buffer, want);
+            if (!rc && s->comm) rc = liberi_c_comm_reduce_host(s->comm, s->fock_b.data(), s->fock_b.data(), want);
             if (rc) s->fock_b.clear();
             return rc;
         }
@@ -213,6 +221,12 @@ int liberi_c_mdi_execute(liberi_mdi s, const char *command, void *buffer, int64_
         default:
             return set_error(LIBERI_E_ARG, "MDI command not recognized");
     }
+}
+
+int liberi_c_mdi_set_comm(liberi_mdi s, liberi_comm comm) {
+    if (!s) return set_error(LIBERI_E_ARG, "liberi_mdi_set_comm: null state");
+    s->comm = comm;
+    return LIBERI_OK;
 }
 
 int liberi_c_mdi_destroy(liberi_mdi s) {

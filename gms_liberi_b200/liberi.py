@@ -37,7 +37,9 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_autotune", "liberi_c_rys_eval_f32", "liberi_c_setup_bytes",
            "liberi_c_set_class_variant", "liberi_c_get_class_variant", "liberi_c_mdi_create",
            "liberi_c_mdi_payload", "liberi_c_mdi_execute", "liberi_c_mdi_destroy",
-           "liberi_c_quartet_fingerprint", "liberi_c_fock_build_uhf", "liberi_c_fock_build_uhf_device"]
+           "liberi_c_quartet_fingerprint", "liberi_c_fock_build_uhf", "liberi_c_fock_build_uhf_device",
+           "liberi_c_mdi_set_comm", "liberi_c_comm_unique_id", "liberi_c_comm_create", "liberi_c_comm_allreduce",
+           "liberi_c_comm_reduce_host", "liberi_c_comm_destroy"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -92,6 +94,13 @@ def lib():
         L.liberi_c_get_stats.argtypes = [H, ctypes.POINTER(Stats)]
         L.liberi_c_quartet_fingerprint.argtypes = [H, ctypes.POINTER(ctypes.c_uint64)]
         L.liberi_c_fock_build_uhf.argtypes = [H, _F64P, _F64P, _F64P, _F64P, ctypes.c_int32]
+        L.liberi_c_mdi_set_comm.argtypes = [H, H]
+        L.liberi_c_comm_unique_id.argtypes = [ctypes.POINTER(ctypes.c_uint8)]
+        L.liberi_c_comm_create.argtypes = [ctypes.POINTER(H), ctypes.POINTER(ctypes.c_uint8), ctypes.c_int32,
+                                           ctypes.c_int32, ctypes.c_int32]
+        L.liberi_c_comm_allreduce.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+        L.liberi_c_comm_reduce_host.argtypes = [H, _F64P, _F64P, ctypes.c_int64]
+        L.liberi_c_comm_destroy.argtypes = [H]
         L.liberi_c_fock_build_uhf_device.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                      ctypes.c_void_p, ctypes.c_void_p]
         L.liberi_c_setup_bytes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
@@ -412,10 +421,47 @@ class MDIEngine:
     def command(self, cmd):
         self._run(cmd, None, 0)
 
+    def set_comm(self, comm):
+        """Sum the ranks' partial F over `comm` (a Comm, or None) inside '<FOCK'."""
+        _check(lib().liberi_c_mdi_set_comm(self._s, comm._c if comm is not None else None))
+
     def destroy(self):
         if self._s:
             _check(lib().liberi_c_mdi_destroy(self._s))
             self._s = ctypes.c_void_p()
+
+
+class Comm:
+    """NCCL communicator for the sum of the ranks' partial F (liberi_c_comm_*).
+    Rank 0 calls `unique_id()`, the caller broadcasts the bytes, every rank
+    constructs `Comm(uid, rank, nranks, device)` (waits for all ranks)."""
+
+    ID_BYTES = 128
+
+    @staticmethod
+    def unique_id():
+        buf = (ctypes.c_uint8 * Comm.ID_BYTES)()
+        _check(lib().liberi_c_comm_unique_id(buf))
+        return bytes(buf)
+
+    def __init__(self, uid, rank=0, nranks=1, device=-1):
+        self._c = ctypes.c_void_p()
+        buf = (ctypes.c_uint8 * Comm.ID_BYTES).from_buffer_copy(uid)
+        _check(lib().liberi_c_comm_create(ctypes.byref(self._c), buf, int(rank), int(nranks), int(device)))
+
+    def allreduce_device(self, d_send, d_recv, count, stream=None):
+        _check(lib().liberi_c_comm_allreduce(self._c, d_send, d_recv, int(count), stream))
+
+    def reduce_host(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.empty_like(x)
+        _check(lib().liberi_c_comm_reduce_host(self._c, x.ctypes.data_as(_F64P), out.ctypes.data_as(_F64P), x.size))
+        return out
+
+    def destroy(self):
+        if self._c:
+            _check(lib().liberi_c_comm_destroy(self._c))
+            self._c = ctypes.c_void_p()
 
 
 def rys_eval(n, T, thr=60.0, strict=False):

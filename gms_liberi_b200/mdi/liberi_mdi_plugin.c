@@ -3,10 +3,15 @@
  * Replaces the reference's src/interface/liberi_mdi_api.F90 (MDI_Plugin_init_ERI,
  * MDI_Plugin_open_ERI, MDI_Plugin_close_ERI): registers the same commands on
  * node @DEFAULT, then answers the driver.  The command state machine is the
- * library's liberi_c_mdi_* object; this file only moves payloads with MDI and
- * sums the ranks' partial Fock matrices before '<FOCK' is sent (MPI_Reduce
- * to rank 0, as the reference does).  Build it against the MDI library and an
- * MPI C compiler, and link with -lliberi_b200:
+ * library's liberi_c_mdi_* object; this file only moves payloads with MDI.
+ * The ranks' partial Fock matrices are summed on the GPUs: rank 0 makes an
+ * NCCL id (liberi_c_comm_unique_id), MPI_Bcast hands it to every rank, each
+ * rank creates its communicator on its own device and attaches it to the
+ * state (liberi_c_mdi_set_comm), so '<FOCK' / '<FOCK_B' come back summed and
+ * rank 0 sends them (the reference sums with MPI_Reduce to rank 0,
+ * liberi_mdi_api.F90:411-414; that path remains if NCCL cannot be set up).
+ * Build it against the MDI library and an MPI C compiler, and link with
+ * -lliberi_b200:
  *
  *     mpicc -shared -fPIC -I<mdi>/include -I<repo>/include liberi_mdi_plugin.c \
  *           -L<repo>/gms_liberi_b200/_build -lliberi_b200 -lmdi -o libliberi_mdi.so
@@ -22,6 +27,7 @@
 #include "liberi_b200.h"
 
 static liberi_mdi g_state = NULL;
+static liberi_comm g_nccl = NULL; /* NCCL sum of the partial F, or NULL (MPI_Reduce) */
 static MDI_Comm g_comm;
 static MPI_Comm g_world;
 
@@ -62,11 +68,15 @@ static int execute(const char *command, int *terminate) {
     rc = liberi_c_mdi_execute(g_state, command, buf, count, &term);
     if (rc) report(command, rc);
     if (command[0] == '<' && count > 0 && rc == 0) {
-        void *sum = rank == 0 ? malloc((size_t)count * elem_size(type)) : NULL;
-        MPI_Reduce(buf, sum, (int)count, mpi_type(type), MPI_SUM, 0, g_world);
-        if (rank == 0) {
-            MDI_Send(sum, (int)count, mdi_type(type), g_comm);
-            free(sum);
+        if (g_nccl) {  /* the library summed the partials over NCCL */
+            if (rank == 0) MDI_Send(buf, (int)count, mdi_type(type), g_comm);
+        } else {
+            void *sum = rank == 0 ? malloc((size_t)count * elem_size(type)) : NULL;
+            MPI_Reduce(buf, sum, (int)count, mpi_type(type), MPI_SUM, 0, g_world);
+            if (rank == 0) {
+                MDI_Send(sum, (int)count, mdi_type(type), g_comm);
+                free(sum);
+            }
         }
     }
     free(buf);
@@ -81,7 +91,24 @@ static int launch(void *plugin_state) {
     MDI_MPI_get_world_comm(&g_world);
     MPI_Comm_rank(g_world, &rank);
     MPI_Comm_size(g_world, &size);
-    if (!g_state && liberi_c_mdi_create(&g_state, rank, size) != LIBERI_OK) return 1;
+    if (!g_state) {
+        if (liberi_c_mdi_create(&g_state, rank, size) != LIBERI_OK) return 1;
+        /* NCCL communicator over the ranks' devices (one rank per device) */
+        uint8_t id[LIBERI_COMM_ID_BYTES];
+        int ok = rank == 0 ? liberi_c_comm_unique_id(id) == LIBERI_OK : 1, all = 0;
+        MPI_Bcast(&ok, 1, MPI_INT, 0, g_world);
+        if (ok) {
+            MPI_Bcast(id, LIBERI_COMM_ID_BYTES, MPI_BYTE, 0, g_world);
+            ok = liberi_c_comm_create(&g_nccl, id, rank, size, -1) == LIBERI_OK;
+        }
+        MPI_Allreduce(&ok, &all, 1, MPI_INT, MPI_MIN, g_world);
+        if (all && g_nccl) {
+            liberi_c_mdi_set_comm(g_state, g_nccl);
+        } else {  /* some rank could not join: sum with MPI as the reference does */
+            if (g_nccl) liberi_c_comm_destroy(g_nccl);
+            g_nccl = NULL;
+        }
+    }
     MDI_Get_role(&role);
     if (role != MDI_ENGINE) fprintf(stderr, "libERI MDI: must run as an ENGINE\n");
     MDI_Register_node("@DEFAULT");

@@ -305,11 +305,33 @@ const char *liberi_c_kernel_name(int32_t k);
  * rank split used at setup; liberi_c_mdi_create takes the same from the
  * shim's communicator. */
 typedef struct liberi_mdi_s *liberi_mdi;
+typedef struct liberi_comm_s *liberi_comm;
 enum { LIBERI_MDI_NONE = 0, LIBERI_MDI_INT = 1, LIBERI_MDI_DOUBLE = 2, LIBERI_MDI_CHAR = 3 };
 int liberi_c_mdi_create(liberi_mdi *state, int32_t my_rank, int32_t num_procs);
 int liberi_c_mdi_payload(liberi_mdi state, const char *command, int32_t *type, int64_t *count);
 int liberi_c_mdi_execute(liberi_mdi state, const char *command, void *buffer, int64_t count, int32_t *terminate);
 int liberi_c_mdi_destroy(liberi_mdi state);
+/* Sum the ranks' partial F over an NCCL communicator inside '<FOCK' (and
+ * '<FOCK_B'): every rank's buffer then holds the total, which the shim sends
+ * from rank 0 without its own MPI_Reduce.  NULL restores the partial. */
+int liberi_c_mdi_set_comm(liberi_mdi state, liberi_comm comm);
+
+/* ---- the sum of the ranks' partial Fock matrices over NCCL ----------------
+ * libERI leaves the sum to its caller (MPI_Reduce in the MDI plugin,
+ * liberi_mdi_api.F90:411-414).  Here it runs on the devices: rank 0 makes a
+ * unique id (LIBERI_COMM_ID_BYTES bytes), the caller broadcasts it (MPI_Bcast
+ * in the shim), every rank creates its communicator on its device (this call
+ * waits for all ranks), and liberi_c_comm_allreduce sums packed F in device
+ * memory (NVLink / NVSwitch) on `stream` (NULL: the communicator's own).
+ * liberi_c_comm_reduce_host sums host buffers through a device copy.
+ * NCCL (libnccl.so.2) is loaded on first use; without it these calls return
+ * LIBERI_E_UNSUPPORTED.  No counterpart in the reference. */
+#define LIBERI_COMM_ID_BYTES 128
+int liberi_c_comm_unique_id(uint8_t *id_out);
+int liberi_c_comm_create(liberi_comm *comm, const uint8_t *id, int32_t rank, int32_t nranks, int32_t device);
+int liberi_c_comm_allreduce(liberi_comm comm, const double *d_send, double *d_recv, int64_t count, void *stream);
+int liberi_c_comm_reduce_host(liberi_comm comm, const double *in, double *out, int64_t count);
+int liberi_c_comm_destroy(liberi_comm comm);
 
 #ifdef __cplusplus
 }

@@ -57,3 +57,22 @@ def test_ranks_partials_reduce_to_full_fock():
     m.destroy()
     assert np.abs(parts[0] + parts[1] - full).max() <= 1e-12
     assert np.abs(full - d["fa_ref"]).max() <= d["tol"]
+
+
+def test_nccl_sum_of_partials_single_rank():
+    # the library's NCCL reduction of the partial F (one rank on one GPU: the
+    # plumbing; more ranks need more GPUs than one call has), inside '<FOCK'
+    d = load_kat("h2o_ccpvdz")
+    comm = liberi.Comm(liberi.Comm.unique_id(), 0, 1, 0)
+    x = np.arange(10, dtype=np.float64)
+    assert np.array_equal(comm.reduce_host(x), x)
+    m = liberi.MDIEngine()
+    m.set_comm(comm)
+    _send_basis(m, d)
+    m.send(">AO_DENS", d["density"])
+    fa = m.recv("<FOCK")
+    assert np.abs(fa - d["fa_ref"]).max() <= 1e-10
+    m.set_comm(None)
+    m.command("EXIT_CONVERGED")
+    m.destroy()
+    comm.destroy()

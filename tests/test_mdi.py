@@ -1,10 +1,13 @@
 """MDI plugin command set on the CPU (no device work): payload sizes follow
 the state the driver has sent (liberi_mdi_api.F90:282-354), errors as the
 C ABI states them."""
+import os
+
 import numpy as np
 import pytest
 
 from gms_liberi_b200 import liberi
+from conftest import ROOT
 
 
 def test_payloads_follow_the_state():
@@ -50,3 +53,18 @@ def test_errors():
     m.destroy()
     with pytest.raises(liberi.LiberiError):
         liberi.MDIEngine(rank=1, nprocs=1)
+
+
+def test_plugin_shim_compiles_against_mdi_and_mpi_declarations():
+    # MDI and MPI are not installed here: the shim is compiled (not linked)
+    # against minimal stub declarations of the calls it makes, so its types,
+    # signatures and use of the C ABI are checked
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = os.path.join(ROOT, "gms_liberi_b200", "mdi", "liberi_mdi_plugin.c")
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(ROOT, "tests", "stubs"),
+                        "-I", os.path.join(ROOT, "include"), src], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
