@@ -789,14 +789,14 @@ constexpr int tuned_nmu_f32(int key) {
         case 1010: return 3;
         case 1100: return 3;
         case 1110: return 3;
-        case 1111: return 3;
+        case 1111: return 1;
         case 1120: return 3;
         case 2000: return 6;
         case 2010: return 6;
         case 2020: return 6;
         case 2100: return 6;
         case 2110: return 6;
-        case 2111: return 3;
+        case 2111: return 1;
         case 2120: return 2;
         case 2121: return 1;
         case 2200: return 6;
@@ -816,14 +816,14 @@ constexpr int tuned_minb_f32(int key) {
         case 1010: return 8;
         case 1100: return 8;
         case 1110: return 5;
-        case 1111: return 3;
+        case 1111: return 4;
         case 1120: return 3;
         case 2000: return 6;
         case 2010: return 6;
         case 2020: return 4;
         case 2100: return 5;
         case 2110: return 3;
-        case 2111: return 3;
+        case 2111: return 4;
         case 2120: return 3;
         case 2121: return 2;
         case 2200: return 3;
@@ -848,10 +848,10 @@ constexpr int alt_nmu(int key, bool f32, int v) {
             case 11101: return 3;
             case 11102: return 3;
             case 11111: return 3;
-            case 11112: return 1;
+            case 11112: return 3;
             case 21101: return 6;
             case 21111: return 3;
-            case 21112: return 1;
+            case 21112: return 3;
             case 21211: return 1;
             default: return 0;
         }
@@ -874,10 +874,10 @@ constexpr int alt_minb(int key, bool f32, int v) {
             case 11101: return 6;
             case 11102: return 8;
             case 11111: return 3;
-            case 11112: return 4;
+            case 11112: return 3;
             case 21101: return 4;
             case 21111: return 2;
-            case 21112: return 4;
+            case 21112: return 3;
             case 21211: return 3;
             default: return 0;
         }
@@ -891,6 +891,31 @@ constexpr int alt_minb(int key, bool f32, int v) {
         case 11101: return 3;
         case 21101: return 3;
         default: return 0;
+    }
+}
+
+// Threads per quartet of a shape variant (multi-pass classes): G lanes of a
+// warp share one quartet and take its passes over the A components in turn
+// (lane g: passes g, g+G, ...), so a quartet's passes run side by side
+// instead of one after another; 1 = one thread per quartet.  Variants 1 and
+// 2 of the multi-pass classes that have no other alternative shape.
+// Variant 0 (the default): (dd|dd) in FP64 runs two lanes per quartet (its
+// 1,830 C60 quartets: 0.73 -> 0.45 ms); variant 1 keeps one.
+constexpr int tuned_tpq(int key, bool f32) { return (!f32 && key == 2222) ? 2 : 1; }
+constexpr int alt_tpq(int key, bool f32, int v) {
+    if (v == 0) return tuned_tpq(key, f32);
+    if (!f32 && key == 2222) return v == 1 ? 1 : 4;
+    if (f32) {
+        switch (key * 10 + v) {
+            case 21201: case 21212: case 22101: case 22111: case 22201: case 22211: case 22221: return 2;
+            case 21202: case 22102: case 22112: case 22202: case 22212: case 22222: return 4;
+            default: return 1;
+        }
+    }
+    switch (key) {
+        case 1111: case 2111: case 2120: case 2121: case 2210: case 2211: case 2220: case 2221: case 2222:
+            return v == 1 ? 2 : 4;
+        default: return 1;
     }
 }
 
@@ -908,9 +933,12 @@ struct PassShape {
     static constexpr int NPASS = (NA + NMU - 1) / NMU;
     static constexpr int MINB_V0 = F32 ? tuned_minb_f32(KEY) : tuned_minb(KEY);
     static constexpr int MINB = (V > 0 && alt_minb(KEY, F32, V) > 0) ? alt_minb(KEY, F32, V) : MINB_V0;
+    // threads per quartet (powers of two; only where the class has passes to share)
+    static constexpr int TPQ = NPASS > 1 ? alt_tpq(KEY, F32, V) : 1;
     // a variant is compiled only when it differs from variant 0
     static constexpr bool DISTINCT = V == 0 || NMU != PassShape<LA, LB, LC, LD, R, 0>::NMU ||
-                                     MINB != PassShape<LA, LB, LC, LD, R, 0>::MINB;
+                                     MINB != PassShape<LA, LB, LC, LD, R, 0>::MINB ||
+                                     TPQ != PassShape<LA, LB, LC, LD, R, 0>::TPQ;
 };
 
 constexpr int CLASS_THREADS = 128;
@@ -944,6 +972,20 @@ template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// sum over the lanes that share lane % G (G a power of two)
+template <int G, typename T>
+__device__ __forceinline__ T warp_sum_strided(T v) {
+#pragma unroll
+    for (int o = 16; o >= G; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// sum over the G lanes of one group (lanes that differ in the low bits only)
+template <int G, typename T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
 
@@ -1056,6 +1098,69 @@ __device__ __forceinline__ void digest_row_general(const R (&a)[ncart(LB)][ncart
     for (int id = 0; id < ND; id++) rows.add(ia, mu, qc.bfD + id, -kad[id]);
 }
 
+// Digestion of one pass of M A components (from mu0): the D sub-blocks of a
+// distinct-shell quartet, the digestion of each component, and the row
+// pair's J summed over the lanes that hold the same component (all lanes of
+// the warp for G = 1, every G-th lane otherwise) and added once.  Every lane
+// reaches the reductions (the quartet loop is warp-uniform; idle lanes, and
+// for G > 1 trips past a lane's passes (live false), digest zeros).
+template <int LA, int LB, int LC, int LD, typename R, int M, bool HGP, int G, typename ACC, typename KB>
+__device__ __forceinline__ void digest_pass(const ACC &acc, int mu0, bool live, R abx, R aby, R abz,
+                                            const QuartetCtx<R> &qc, const Rows<R> &rows, KB &kb) {
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    const bool distinct = !qc.iandj && !qc.kandl && !qc.same;
+    R dCD[NC][ND], dBD[NB][ND], dBC[NB][NC];
+    if (distinct) {
+#pragma unroll
+        for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+            for (int id = 0; id < ND; id++) dCD[ic][id] = dget(qc.Dm, qc.ld, qc.bfC + ic, qc.bfD + id);
+#pragma unroll
+        for (int ib = 0; ib < NB; ib++) {
+#pragma unroll
+            for (int id = 0; id < ND; id++) dBD[ib][id] = dget(qc.DmK, qc.ld, qc.bfB + ib, qc.bfD + id);
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++) dBC[ib][ic] = dget(qc.DmK, qc.ld, qc.bfB + ib, qc.bfC + ic);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        const int ia = mu0 + m;
+        if constexpr (G == 1) {
+            if (ia >= NA) break;
+        }
+        const bool comp = G == 1 || (live && ia < NA);
+        R jab[NB];
+        if constexpr (G > 1) {
+#pragma unroll
+            for (int ib = 0; ib < NB; ib++) jab[ib] = R(0);
+        }
+        if (comp) {
+            if constexpr (HGP) {
+                // one pass: the component index is the unrolled m (a compile-time
+                // index into acc; the run-time ia would put acc in local memory)
+                R sl[NB][NC][ND];
+                bra_transfer<LA, LB, LC, R>(acc, m, abx, aby, abz, sl);
+                if (distinct)
+                    digest_row_distinct<LA, LB, LC, LD, R>(sl, ia, qc, dCD, dBD, dBC, rows, kb, jab);
+                else
+                    digest_row_general<LA, LB, LC, LD, R>(sl, ia, qc, rows, kb, jab);
+            } else {
+                if (distinct)
+                    digest_row_distinct<LA, LB, LC, LD, R>(acc[m], ia, qc, dCD, dBD, dBC, rows, kb, jab);
+                else
+                    digest_row_general<LA, LB, LC, LD, R>(acc[m], ia, qc, rows, kb, jab);
+            }
+        }
+#pragma unroll
+        for (int ib = 0; ib < NB; ib++) jab[ib] = warp_sum_strided<G>(jab[ib]);
+        if ((int)(threadIdx.x & 31) < G && comp) {
+#pragma unroll
+            for (int ib = 0; ib < NB; ib++) rows.add(ia, qc.bfA + ia, qc.bfB + ib, jab[ib]);
+        }
+    }
+}
+
 // Runtime loop over passes of NMU A components; digestion of each pass.
 template <int LA, int LB, int LC, int LD, typename R, int V, typename KB>
 __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, int q0, int nq, const double4 &A,
@@ -1077,63 +1182,39 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
     R cache_u[CAP * NR], cache_w[CAP * NR];
     const bool cache_ok = CACHE && np * nq <= CAP;
     constexpr bool HGP = hgp_class<LA, LB, LC, LD>(PS::NPASS);
+    using Acc = typename std::conditional<HGP, R[nrange(LA, LA + LB)][NC], R[M][NB][NC][ND]>::type;
+    // G lanes per quartet (lane g of a group takes passes g, g+G, ...)
+    constexpr int G = PS::TPQ;
+    if constexpr (G == 1) {
 #pragma unroll 1
-    for (int pass = 0; pass < PS::NPASS; pass++) {
-        const int mu0 = pass * M;
-        // (e0|c0) intermediates (HGP) or the (ab|cd) block of this pass's A components
-        using Acc = typename std::conditional<HGP, R[nrange(LA, LA + LB)][NC], R[M][NB][NC][ND]>::type;
-        Acc acc;
-        eval_block<LA, LB, LC, LD, R, M, HGP>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict, tab,
-                                              tabf, mu0, acc, cache_u, cache_w, cache_ok ? (pass == 0 ? 1 : 2) : 0,
-                                              pthr, bpmax);
-        // The J update of the row pair (mu nu) is the same address for every
-        // lane of the warp (one bra per CTA): it is summed over the warp and
-        // added once.  Every lane reaches the reduction (the quartet loop is
-        // warp-uniform; idle lanes carry zero integrals).
-        const bool distinct = !qc.iandj && !qc.kandl && !qc.same;
-        R dCD[NC][ND], dBD[NB][ND], dBC[NB][NC];
-        if (distinct) {
-#pragma unroll
-            for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-                for (int id = 0; id < ND; id++) dCD[ic][id] = dget(qc.Dm, qc.ld, qc.bfC + ic, qc.bfD + id);
-#pragma unroll
-            for (int ib = 0; ib < NB; ib++) {
-#pragma unroll
-                for (int id = 0; id < ND; id++) dBD[ib][id] = dget(qc.DmK, qc.ld, qc.bfB + ib, qc.bfD + id);
-#pragma unroll
-                for (int ic = 0; ic < NC; ic++) dBC[ib][ic] = dget(qc.DmK, qc.ld, qc.bfB + ib, qc.bfC + ic);
-            }
+        for (int pass = 0; pass < PS::NPASS; pass++) {
+            const int mu0 = pass * M;
+            // (e0|c0) intermediates (HGP) or the (ab|cd) block of this pass's A components
+            Acc acc;
+            eval_block<LA, LB, LC, LD, R, M, HGP>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict,
+                                                  tab, tabf, mu0, acc, cache_u, cache_w,
+                                                  cache_ok ? (pass == 0 ? 1 : 2) : 0, pthr, bpmax);
+            digest_pass<LA, LB, LC, LD, R, M, HGP, 1>(acc, mu0, true, abx, aby, abz, qc, rows, kb);
         }
-#pragma unroll
-        for (int m = 0; m < M; m++) {
-            const int ia = mu0 + m;
-            if (ia >= NA) break;
-            R jab[NB];
-            if constexpr (HGP) {
-                // one pass: the component index is the unrolled m (a compile-time
-                // index into acc; the run-time ia would put acc in local memory)
-                R sl[NB][NC][ND];
-                bra_transfer<LA, LB, LC, R>(acc, m, abx, aby, abz, sl);
-                if (distinct)
-                    digest_row_distinct<LA, LB, LC, LD, R>(sl, ia, qc, dCD, dBD, dBC, rows, kb, jab);
-                else
-                    digest_row_general<LA, LB, LC, LD, R>(sl, ia, qc, rows, kb, jab);
-            } else {
-                if (distinct)
-                    digest_row_distinct<LA, LB, LC, LD, R>(acc[m], ia, qc, dCD, dBD, dBC, rows, kb, jab);
-                else
-                    digest_row_general<LA, LB, LC, LD, R>(acc[m], ia, qc, rows, kb, jab);
-            }
-#pragma unroll
-            for (int ib = 0; ib < NB; ib++) jab[ib] = warp_sum(jab[ib]);
-            if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-                for (int ib = 0; ib < NB; ib++) rows.add(ia, qc.bfA + ia, qc.bfB + ib, jab[ib]);
-            }
+    } else {
+        // every lane runs the same number of trips; a trip past a lane's last
+        // pass evaluates and digests nothing, but still joins the warp sums
+        constexpr int NIT = (PS::NPASS + G - 1) / G;
+        const int sub = (int)(threadIdx.x & 31) & (G - 1);
+#pragma unroll 1
+        for (int trip = 0; trip < NIT; trip++) {
+            const int pass = trip * G + sub;
+            const bool live = pass < PS::NPASS;
+            const int mu0 = (live ? pass : 0) * M;
+            Acc acc;
+            eval_block<LA, LB, LC, LD, R, M, HGP>(b, p0, np, q0, live ? nq : 0, A, C, abx, aby, abz, cdx, cdy, cdz,
+                                                  thr, strict, tab, tabf, mu0, acc, cache_u, cache_w,
+                                                  cache_ok ? (trip == 0 ? 1 : 2) : 0, pthr, bpmax);
+            digest_pass<LA, LB, LC, LD, R, M, HGP, G>(acc, mu0, live, abx, aby, abz, qc, rows, kb);
         }
     }
 }
+
 
 // ---- reference rank ownership (int0000.F90:76-91, int0001.F90:89-104) ---------
 __device__ __forceinline__ bool rank_owns(const RankSplit &rs, long long it) {
@@ -1273,9 +1354,12 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     // Warp-uniform loop: every lane of a warp runs the same iterations (the
     // digestion sums the row pair's J over the warp); a lane past the end of
     // the task, or holding a quartet of another rank, evaluates no primitives
-    // and digests zeros.
-    for (int qb = threadIdx.x & ~31; qb < cnt; qb += CLASS_THREADS) {
-        const int qi = qb + (threadIdx.x & 31);
+    // and digests zeros.  With G threads per quartet a warp takes 32/G
+    // quartets per trip, lanes 0..G-1 the first, and so on.
+    constexpr int G = PassShape<LA, LB, LC, LD, R, V>::TPQ;
+    const int gsub = (int)(threadIdx.x & 31) & (G - 1);
+    for (int qb = (int)(threadIdx.x >> 5) * (32 / G); qb < cnt; qb += CLASS_THREADS / G) {
+        const int qi = qb + (int)(threadIdx.x & 31) / G;
         bool act = qi < cnt;
         const int j = k0 + (act ? qi : 0);
         if (act && a.rs.nsize > 1) act = quartet_owned(a, ibra, j);
@@ -1299,20 +1383,28 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
         for (int i = 0; i < KBuf<NB, NC, ND, SM, R>::N; i++) kb.at(i) = R(0);
         run_passes<LA, LB, LC, LD, R, V>(bas, p0, np, (int)(unsigned)kpr, act ? (int)(unsigned)(kpr >> 32) : 0, A, C, abx, aby,
                                       abz, cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb, pthr, bpmax);
+        if constexpr (G > 1) {
+            // the group's lanes hold partial sums over their passes: combine
+            // them, the group's first lane adds them to F
 #pragma unroll
-        for (int ib = 0; ib < NB; ib++) {
-#pragma unroll
-            for (int ic = 0; ic < NC; ic++) rowsB.add(ib, bfB + ib, qc.bfC + ic, -kb.bc(ib, ic));
-#pragma unroll
-            for (int id = 0; id < ND; id++) rowsB.add(ib, bfB + ib, qc.bfD + id, -kb.bd(ib, id));
+            for (int i = 0; i < KBuf<NB, NC, ND, SM, R>::N; i++) kb.at(i) = group_sum<G>(kb.at(i));
         }
+        if (G == 1 || gsub == 0) {
 #pragma unroll
-        for (int ic = 0; ic < NC; ic++)
+            for (int ib = 0; ib < NB; ib++) {
 #pragma unroll
-            for (int id = 0; id < ND; id++) {
-                const R v = kb.cd(ic, id);
-                if (v != R(0)) atomicAdd(LIBERI_F + tri0(qc.bfC + ic, qc.bfD + id), (double)v);
+                for (int ic = 0; ic < NC; ic++) rowsB.add(ib, bfB + ib, qc.bfC + ic, -kb.bc(ib, ic));
+#pragma unroll
+                for (int id = 0; id < ND; id++) rowsB.add(ib, bfB + ib, qc.bfD + id, -kb.bd(ib, id));
             }
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                for (int id = 0; id < ND; id++) {
+                    const R v = kb.cd(ic, id);
+                    if (v != R(0)) atomicAdd(LIBERI_F + tri0(qc.bfC + ic, qc.bfD + id), (double)v);
+                }
+        }
     }
     if (use_tile) {
         __syncthreads();
