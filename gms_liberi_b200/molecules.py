@@ -3,15 +3,18 @@
 No public data set is involved: every input is generated here from a seed.
 The arrays follow the reference's liberi_setup layout
 (src/interface/liberi_interface.F90:72-200): 1-based sh_loc / atom_num /
-atom_loc, ang_mom 1=s 2=p 3=d, per-primitive contraction coefficients that
+atom_loc, ang_mom 1=s 2=p 3=d 4=f, per-primitive contraction coefficients that
 already contain the GAMESS primitive norms, sp shells split into an s and a p
-shell that share exponents, Cartesian d (xx,yy,zz,xy,xz,yz).
+shell that share exponents, Cartesian d (xx,yy,zz,xy,xz,yz) and f (xxx,yyy,zzz,
+xxy,xxz,xyy,yyz,xzz,yzz,xyz), normalised on the axial component.
 
 Workloads:
   * ``h2o_like()``       bent triatomic, STO-3G-shaped, 7 functions.
   * ``ethane()``         staggered C2H6, 6-31G(d)-shaped, 42 functions.
   * ``c60()``            truncated icosahedron, 6-31G(d)-shaped, 900 functions.
   * ``random_molecule()`` C/N/O/H clusters for the batched and serving loops.
+  * ``f_triatomic()``    O/C/H with s, p, d and f shells, 38 functions (f checks).
+  * ``f_cluster()``      C/N/O/H clusters with f shells on the heavy atoms.
 """
 import math
 
@@ -24,6 +27,9 @@ _SHAPE_631GD_HEAVY = [("s", 6), ("sp", 3), ("sp", 1), ("d", 1)]
 _SHAPE_631GD_H = [("s", 3), ("s", 1)]
 _SHAPE_STO3G_HEAVY = [("s", 3), ("sp", 3)]
 _SHAPE_STO3G_H = [("s", 3)]
+# f-bearing shapes: a polarised heavy-atom set with one f shell, H with a p
+_SHAPE_F_HEAVY = [("s", 6), ("sp", 3), ("sp", 1), ("d", 1), ("f", 1)]
+_SHAPE_F_H = [("s", 3), ("s", 1), ("p", 1)]
 
 
 def _prim_norm(l, a):
@@ -32,8 +38,11 @@ def _prim_norm(l, a):
         return base
     if l == 1:
         return 2.0 * math.sqrt(a) * base
-    # d normalised on the xx component; xy/xz/yz carry the extra sqrt(3)
-    return 4.0 * a / math.sqrt(3.0) * base
+    if l == 2:
+        # d normalised on the xx component; xy/xz/yz carry the extra sqrt(3)
+        return 4.0 * a / math.sqrt(3.0) * base
+    # f normalised on xxx: (4a)^(3/2) / sqrt(5!!); the mixed components carry sqrt5 / sqrt15
+    return 8.0 * a ** 1.5 / math.sqrt(15.0) * base
 
 
 def _self_overlap(l, exps, coefs):
@@ -46,6 +55,8 @@ def _self_overlap(l, exps, coefs):
                 f *= 0.5 / p
             elif l == 2:
                 f *= 0.75 / (p * p)
+            elif l == 3:
+                f *= 1.875 / (p * p * p)
             s += ci * cj * f
     return s
 
@@ -67,8 +78,12 @@ def element_basis(elem, shape, lo, hi, seed=0):
         elif kind == "sp":
             shells.append((0, exps, _contracted(0, exps, rng.uniform(0.1, 1.0, K).tolist())))
             shells.append((1, exps, _contracted(1, exps, rng.uniform(0.1, 1.0, K).tolist())))
+        elif kind == "p":
+            shells.append((1, exps, _contracted(1, exps, rng.uniform(0.1, 1.0, K).tolist())))
         elif kind == "d":
             shells.append((2, exps, _contracted(2, exps, rng.uniform(0.1, 1.0, K).tolist())))
+        elif kind == "f":
+            shells.append((3, exps, _contracted(3, exps, rng.uniform(0.1, 1.0, K).tolist())))
     return shells
 
 
@@ -85,25 +100,25 @@ def build_basis(symbols, coords, shells_of):
             anum.append(ia + 1)
             aloc.append(bf)
             sbas.append(bf)
-            nc = (1, 3, 6)[l]
+            nc = (1, 3, 6, 10)[l]
             ebas.append(bf + nc - 1)
             bf += nc
     nsh = len(per_shell)
     mx = max(cnum)
     exps_a = np.zeros(mx * nsh)
-    cs, cp, cd = np.zeros(mx * nsh), np.zeros(mx * nsh), np.zeros(mx * nsh)
+    cs, cp, cd, cf = (np.zeros(mx * nsh) for _ in range(4))
     for s, (l, exps, coefs) in enumerate(per_shell):
         loc = s * mx
         shloc.append(loc + 1)
         exps_a[loc:loc + len(exps)] = exps
-        (cs, cp, cd)[l][loc:loc + len(exps)] = coefs
+        (cs, cp, cd, cf)[l][loc:loc + len(exps)] = coefs
     nbf = bf - 1
     return {
         "nsh": nsh, "natoms": len(symbols), "num_bas": nbf, "mxgtot": mx,
         "ang_mom": ang, "contr_num": cnum, "sh_loc": shloc, "atom_num": anum,
         "atom_loc": aloc, "start_bas": sbas, "end_bas": ebas,
         "exponents": exps_a, "coef_s": cs, "coef_p": cp, "coef_d": cd,
-        "coef_f": np.zeros(mx * nsh),
+        "coef_f": cf,
         "coords": np.asarray(coords, dtype=np.float64).reshape(-1),
         "symbols": list(symbols),
     }
@@ -227,3 +242,33 @@ def nocc_of(basis):
     """Closed-shell occupation from nuclear charges (neutral molecule)."""
     z = sum(_ELEM_Z[s] for s in basis["symbols"])
     return z // 2
+
+
+def _basis_f(seed=0):
+    def shells_of(sym):
+        if sym == "H":
+            return element_basis("H", _SHAPE_F_H, 0.12, 20.0, seed)
+        return element_basis(sym, _SHAPE_F_HEAVY, 0.15, 3000.0, seed)
+    return shells_of
+
+
+def f_triatomic(seed=0):
+    """Three atoms with s, p, d and f shells (38 functions): O with s(3), s(1),
+    p(1), d(1), f(1); C with s(1), s(2), p(2), f(1); H with s(2), s(1)."""
+    shapes = {"O": [("s", 3), ("sp", 1), ("d", 1), ("f", 1)],
+              "C": [("s", 1), ("sp", 2), ("f", 1)],
+              "H": [("s", 2), ("s", 1)]}
+
+    def shells_of(sym):
+        return element_basis(sym, shapes[sym], 0.2, 40.0, seed)
+
+    xyz = np.array([[0.0, 0.0, 0.0], [0.4, 2.1, 1.3], [-1.7, -0.6, 1.1]])
+    return build_basis(["O", "C", "H"], xyz, shells_of)
+
+
+def f_cluster(natoms, seed=0, rho=0.01, dmin=1.9):
+    """C/N/O/H cluster (as random_molecule) with an f shell and a d shell on
+    every heavy atom and a p shell on every H."""
+    b = random_molecule(natoms, seed, rho, dmin)
+    xyz = np.asarray(b["coords"]).reshape(-1, 3)
+    return build_basis(b["symbols"], xyz, _basis_f(seed))

@@ -12,7 +12,12 @@
  *     primitive-pair data and the mu*R^2 > cux=50 "ismlp" flag
  *       (src/liberi_shell_pair.F90:348-1283, e.g. compute_ss_pairs :348-474)
  *   - the 21 s/p/d kernels in the driver's fixed order
- *       (src/liberi_driver.F90:69-102)
+ *       (src/liberi_driver.F90:69-102), then the 34 f kernels of the ENABLE_F
+ *       block in its order (src/liberi_driver.F90:103-160): four f pair
+ *       classes sf, pf, df, ff (src/liberi_shell_pair.F90:1285-1682; lower-L
+ *       shell outer, f inner, ff triangular), GAMESS f order xxx, yyy, zzz,
+ *       xxy, xxz, xyy, yyz, xzz, yzz, xyz with sqrt5 on the six mixed and
+ *       sqrt15 on xyz (int3011_rysgen.F90 ijx/ijy/ijz, d03bra)
  *     with each kernel's own pre-screen (cross-class or own-class maxima),
  *     product test operator (>=, > or none), bra-range / flat-index rank split
  *     with its tile size, and digestion cut
@@ -27,24 +32,29 @@
  * kernels (s/p/d up to L=5) and generated Rys kernels (L>=5 with a d-d pair).
  * Both are exact methods up to ~1e-14; this oracle evaluates every class by Rys
  * quadrature.  Rys classes take the reference's own root algorithm: the
- * 35-point discretised Stieltjes procedure (RYSDS) on Gauss-Legendre nodes
- * u=t^2 followed by a Gauss-Christoffel weight evaluation (the reference's
- * RYSGW, an implicit QL; here Sturm bisection on the same Jacobi matrix),
- * int2222_rysgen.F90:636-877.  Rotated-axis classes work, like the reference's,
+ * discretised Stieltjes procedure (RYSDS) on Gauss-Legendre nodes u=t^2 --
+ * 30 points for up to 4 roots (int2111_rysgen.F90:473-533), 35 for 5
+ * (int2222_rysgen.F90:661-697), 40 for 6 and 7 (int3333_rysgen.F90:1229-1309)
+ * -- followed by the Golub-Welsch step (the reference's RYSGW, below),
+ * int2222_rysgen.F90:636-877.  The ERIC kernels of the f block (int0030,
+ * int0031, int0032, int1030: src/rhf/eric/) work from tabulated Boys
+ * functions like the rotated-axis ones (int0030_ericgen.F90:261-300) and are
+ * restated the same way, without their primitive skip.  Rotated-axis classes work, like the reference's,
  * from tabulated Boys functions (liberi_boys.F90): the Rys rule is formed from
  * the Boys moments F_0..F_{2n-1} in long double.
  * The asymptotic branch follows the reference per class: rotated-axis classes
  * switch to the large-T form for T > t_max = 25 (src/liberi_boys.F90:22,
- * int0000.F90:220-234), Rys classes for xx >= 43 / 49 / 55 (3 / 4 / 5 roots,
- * int2111_rysgen.F90:458, int2211_rysgen.F90:540, int2222_rysgen.F90:642).
+ * int0000.F90:220-234), Rys classes for xx >= 43 / 49 / 55 / 60 / 65 (3 / 4 /
+ * 5 / 6 / 7 roots, int2111_rysgen.F90:458, int2211_rysgen.F90:540,
+ * int2222_rysgen.F90:642, int3322_rysgen.F90, int3333_rysgen.F90:1206).
  * The large-T Boys form sqrt(pi/4t)*(2m-1)!!/(2t)^m is exactly the Gauss-
  * Hermite limit of the Rys roots, so both branches are reproduced.
  *
  * Deliberate deviations (both far below the 1e-10 parity bar):
  *   - d_coeff_alt / sq for primitive pairs with mu*R^2 > 50 are left
  *     uninitialised by the reference (liberi_shell_pair.F90:438-441); here the
- *     Rys classes use the formula value, the rotated-axis classes skip the pair
- *     as the reference does (int0000.F90:208-210).
+ *     Rys and ERIC classes use the formula value, the rotated-axis classes skip
+ *     the pair as the reference does (int0000.F90:208-210).
  *   - the reference decodes triangular pair indices in single precision for
  *     most kernels (int0001.F90:124); here the decode is exact integer math,
  *     which agrees for every pair count below ~2M.
@@ -75,31 +85,35 @@ typedef ORACLE_REAL real_t;
 typedef ORACLE_REALL reall_t;
 
 #define PI_D 3.14159265358979323846
-#define NGRID 35
-#define MAXROOT 5
-#define MAXCART 6
+#define MAXGRID 40
+#define MAXROOT 7
+#define MAXCART 10
+#define MAXL 3
+#define NK 55  /* 21 s/p/d kernels, then the 34 of the f block */
 
 /* ---- reference parameters (src/liberi_parameters.F90) -------------------- */
 static const double CUX = 50.0;                   /* :44 */
 
-/* ---- Cartesian component tables: p = x,y,z ; d = xx,yy,zz,xy,xz,yz ------- */
-static const int NCART[3] = {1, 3, 6};
-static const int CX[3][6] = {{0}, {1, 0, 0}, {2, 0, 0, 1, 1, 0}};
-static const int CY[3][6] = {{0}, {0, 1, 0}, {0, 2, 0, 1, 0, 1}};
-static const int CZ[3][6] = {{0}, {0, 0, 1}, {0, 0, 2, 0, 1, 1}};
-/* off-diagonal d components carry sqrt(3) (int2222_rysgen.F90:599-634) */
-static double CNORM[3][6];
+/* ---- Cartesian component tables: p = x,y,z ; d = xx,yy,zz,xy,xz,yz ;
+ * f = xxx,yyy,zzz,xxy,xxz,xyy,yyz,xzz,yzz,xyz ----------------------------- */
+static const int NCART[4] = {1, 3, 6, 10};
+static const int CX[4][10] = {{0}, {1, 0, 0}, {2, 0, 0, 1, 1, 0}, {3, 0, 0, 2, 2, 1, 0, 1, 0, 1}};
+static const int CY[4][10] = {{0}, {0, 1, 0}, {0, 2, 0, 1, 0, 1}, {0, 3, 0, 1, 0, 2, 2, 0, 1, 1}};
+static const int CZ[4][10] = {{0}, {0, 0, 1}, {0, 0, 2, 0, 1, 1}, {0, 0, 3, 0, 1, 0, 1, 2, 2, 1}};
+/* off-diagonal d components carry sqrt(3) (int2222_rysgen.F90:599-634), the
+ * six mixed f components sqrt(5) and xyz sqrt(15) (int3011_rysgen.F90 d03bra) */
+static double CNORM[4][10];
 
 /* ---- input basis (mirror of basis_t, src/liberi_types.f90:26-67) --------- */
 typedef struct {
     int32_t nsh, natoms, num_bas, mxgtot;
-    const int32_t *ang_mom;   /* 1=s 2=p 3=d */
+    const int32_t *ang_mom;   /* 1=s 2=p 3=d 4=f */
     const int32_t *contr_num;
     const int32_t *sh_loc;    /* 1-based primitive offset */
     const int32_t *atom_num;  /* 1-based */
     const int32_t *atom_loc;  /* 1-based first basis function */
     const double *exponents;
-    const double *coef_s, *coef_p, *coef_d;
+    const double *coef_s, *coef_p, *coef_d, *coef_f;
     const double *coords;     /* 3*natoms */
     const double *schwrz;     /* nsh(nsh+1)/2 packed */
 } oracle_basis;
@@ -111,7 +125,7 @@ typedef struct {
     int32_t sample_mod;  /* >1: evaluate only the quartets of a hashed 1/sample_mod of bra pairs */
     int32_t sample_seed;
     int32_t nthreads;
-    int32_t only_kernel; /* -1: all, else kernel index 0..20 */
+    int32_t only_kernel; /* -1: all, else kernel index 0..NK-1 */
 } oracle_opts;
 
 /* per kernel: [0] screened shell quartets, [1] primitive quartets evaluated,
@@ -122,18 +136,18 @@ typedef struct {
  * quartet_fp() (order independent, so any evaluation order gives the same
  * pair of words; the engine computes the same function over its task lists) */
 typedef struct {
-    int64_t c[21][4];
-    double t_wall[21];
-    double t_eval[21];
+    int64_t c[NK][4];
+    double t_wall[NK];
+    double t_eval[NK];
     int32_t nthreads;
-    uint64_t fp[21][2];
-    uint64_t ops[21][2];  /* op-counting build only: ops in primitive-quartet work, in shell-quartet work */
+    uint64_t fp[NK][2];
+    uint64_t ops[NK][2];  /* op-counting build only: ops in primitive-quartet work, in shell-quartet work */
 } oracle_counts;
 
-/* ---- pair classes ---------------------------------------------------------- */
-enum { SS = 0, SP, PP, SD, PD, DD, NPC };
-static const int PC_L1[NPC] = {0, 0, 1, 0, 1, 2};
-static const int PC_L2[NPC] = {0, 1, 1, 2, 2, 2};
+/* ---- pair classes: the six s/p/d ones, then sf, pf, df, ff ----------------- */
+enum { SS = 0, SP, PP, SD, PD, DD, SF, PF, DF, FF, NPC };
+static const int PC_L1[NPC] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3};
+static const int PC_L2[NPC] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
 
 typedef struct {
     int64_t n;          /* shell pairs */
@@ -147,48 +161,93 @@ typedef struct {
 typedef struct {
     const oracle_basis *b;
     double (*csh)[3];     /* shell coordinates */
-    int32_t *lst[3];      /* ascending shell lists per L */
-    int64_t nl[3];
+    int32_t *lst[MAXL + 1];  /* ascending shell lists per L */
+    int64_t nl[MAXL + 1];
     pairs_t pc[NPC];
-    const double *coef[3];
+    const double *coef[MAXL + 1];
 } ctx_t;
 
-/* ---- kernel descriptors (src/liberi_driver.F90:69-102) -------------------- */
+/* ---- kernel descriptors (src/liberi_driver.F90:69-160) ------------------- */
 enum { OP_GE = 0, OP_GT = 1, OP_NONE = 2 };
 enum { TILE_SQRT = 0, TILE_E9 = 1, TILE_E8 = 2, TILE_NONE = 3 };
+/* rys: Rys root algorithm (discretised Stieltjes on ngrid points), else the
+ * Boys-function rule (rotated-axis and ERIC kernels); skip: primitive pairs
+ * with mu R^2 > 50 skipped (rotated-axis kernels only) */
 typedef struct {
     const char *name;
     int bra, ket, tri, rys, cross, op, tile, ketmajor, digest_schwarz;
     double asym;  /* rot: T > 25 ; rys: xx >= asym */
+    int ngrid, skip;
 } kdesc_t;
 
-static const kdesc_t KD[21] = {
-    /* name      bra ket tri rys cross op      tile       kmaj dsch asym */
-    {"int0000", SS, SS, 1, 0, 0, OP_GE, TILE_SQRT, 0, 1, 25.0},
-    {"int0001", SS, SP, 0, 0, 1, OP_GT, TILE_E9, 0, 1, 25.0},
-    {"int0011", SS, PP, 0, 0, 1, OP_GT, TILE_E9, 0, 1, 25.0},
-    {"int0111", SP, PP, 0, 0, 1, OP_GT, TILE_E9, 0, 0, 25.0},
-    {"int0101", SP, SP, 1, 0, 0, OP_GE, TILE_NONE, 0, 0, 25.0},
-    {"int1111", PP, PP, 1, 0, 0, OP_GE, TILE_NONE, 0, 1, 25.0},
-    {"int0002", SS, SD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0},
-    {"int0012", SS, PD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0},
-    {"int0102", SP, SD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0},
-    {"int0112", SP, PD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0},
-    {"int0022", SS, DD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0},
-    {"int0122", SP, DD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0},
-    {"int1102", PP, SD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0},
-    {"int0202", SD, SD, 1, 0, 0, OP_GT, TILE_NONE, 0, 0, 25.0},
-    {"int2211", DD, PP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0},
-    {"int2121", PD, PD, 1, 1, 0, OP_GT, TILE_NONE, 0, 0, 49.0},
-    {"int2120", PD, SD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 43.0},
-    {"int2111", PD, PP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 43.0},
-    {"int2220", DD, SD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0},
-    {"int2221", DD, PD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0},
-    {"int2222", DD, DD, 1, 1, 0, OP_NONE, TILE_NONE, 0, 0, 55.0},
+static const kdesc_t KD[NK] = {
+    /* name      bra ket tri rys cross op      tile       kmaj dsch asym grid skip */
+    {"int0000", SS, SS, 1, 0, 0, OP_GE, TILE_SQRT, 0, 1, 25.0, 0, 1},
+    {"int0001", SS, SP, 0, 0, 1, OP_GT, TILE_E9, 0, 1, 25.0, 0, 1},
+    {"int0011", SS, PP, 0, 0, 1, OP_GT, TILE_E9, 0, 1, 25.0, 0, 1},
+    {"int0111", SP, PP, 0, 0, 1, OP_GT, TILE_E9, 0, 0, 25.0, 0, 1},
+    {"int0101", SP, SP, 1, 0, 0, OP_GE, TILE_NONE, 0, 0, 25.0, 0, 1},
+    {"int1111", PP, PP, 1, 0, 0, OP_GE, TILE_NONE, 0, 1, 25.0, 0, 1},
+    {"int0002", SS, SD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0, 0, 1},
+    {"int0012", SS, PD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0, 0, 1},
+    {"int0102", SP, SD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0, 0, 1},
+    {"int0112", SP, PD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0, 0, 1},
+    {"int0022", SS, DD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0, 0, 1},
+    {"int0122", SP, DD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0, 0, 1},
+    {"int1102", PP, SD, 0, 0, 1, OP_GT, TILE_E8, 0, 0, 25.0, 0, 1},
+    {"int0202", SD, SD, 1, 0, 0, OP_GT, TILE_NONE, 0, 0, 25.0, 0, 1},
+    {"int2211", DD, PP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int2121", PD, PD, 1, 1, 0, OP_GT, TILE_NONE, 0, 0, 49.0, 30, 0},
+    {"int2120", PD, SD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 43.0, 30, 0},
+    {"int2111", PD, PP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 43.0, 30, 0},
+    {"int2220", DD, SD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int2221", DD, PD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int2222", DD, DD, 1, 1, 0, OP_NONE, TILE_NONE, 0, 0, 55.0, 35, 0},
+    /* f block: own-class pre-screens, ">" product test except int3333 (none),
+     * 3.75e8 tiles for product kernels, bra-fastest flat order in the Rys
+     * product kernels and bra-major in the ERIC ones (int0030_ericgen.F90:
+     * 66-124, int3011_rysgen.F90:213-274, int3333_rysgen.F90:829-867);
+     * digestion at the literal 5e-11 throughout */
+    {"int3333", FF, FF, 1, 1, 0, OP_NONE, TILE_NONE, 0, 0, 65.0, 40, 0},
+    {"int0030", SS, SF, 0, 0, 0, OP_GT, TILE_E8, 0, 0, 25.0, 0, 0},
+    {"int0031", SS, PF, 0, 0, 0, OP_GT, TILE_E8, 0, 0, 25.0, 0, 0},
+    {"int0032", SS, DF, 0, 0, 0, OP_GT, TILE_E8, 0, 0, 25.0, 0, 0},
+    {"int1030", SP, SF, 0, 0, 0, OP_GT, TILE_E8, 0, 0, 25.0, 0, 0},
+    {"int3330", FF, SF, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 55.0, 35, 0},
+    {"int3011", SF, PP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 43.0, 30, 0},
+    {"int3020", SF, SD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 43.0, 30, 0},
+    {"int2130", PD, SF, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int2230", DD, SF, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int3030", SF, SF, 1, 1, 0, OP_GT, TILE_NONE, 0, 0, 49.0, 30, 0},
+    {"int3110", PF, SP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 43.0, 30, 0},
+    {"int3111", PF, PP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int3120", PF, SD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int3121", PF, PD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int2231", DD, PF, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 55.0, 35, 0},
+    {"int3130", PF, SF, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int3131", PF, PF, 1, 1, 0, OP_GT, TILE_NONE, 0, 0, 55.0, 35, 0},
+    {"int3210", DF, SP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int3331", FF, PF, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 60.0, 40, 0},
+    {"int3211", DF, PP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int3220", DF, SD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int3221", DF, PD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 55.0, 35, 0},
+    {"int3222", DF, DD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 55.0, 35, 0},
+    {"int3230", DF, SF, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 55.0, 35, 0},
+    {"int3231", DF, PF, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 55.0, 35, 0},
+    {"int3232", DF, DF, 1, 1, 0, OP_GT, TILE_NONE, 0, 0, 60.0, 40, 0},
+    {"int3300", FF, SS, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int3310", FF, SP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 49.0, 30, 0},
+    {"int3311", FF, PP, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 55.0, 35, 0},
+    {"int3320", FF, SD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 55.0, 35, 0},
+    {"int3321", FF, PD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 55.0, 35, 0},
+    {"int3322", FF, DD, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 60.0, 40, 0},
+    {"int3332", FF, DF, 0, 1, 0, OP_GT, TILE_E8, 1, 0, 60.0, 40, 0},
 };
 
 /* ======================= Rys roots and weights ============================= */
-static double GRID_U[NGRID], GRID_W[NGRID];
+/* Gauss-Legendre grids of the RYSDS procedure: 30, 35 and 40 points */
+static double GRID_U[3][MAXGRID], GRID_W[3][MAXGRID];
+static int grid_slot(int ngrid) { return ngrid <= 30 ? 0 : (ngrid <= 35 ? 1 : 2); }
 /* asymptotic: u_i = HR[n][i]/T, w_i = HW[n][i]/sqrt(T) (Gauss-Hermite, 2n pts) */
 static double HR[MAXROOT + 1][MAXROOT], HW[MAXROOT + 1][MAXROOT];
 static int g_init = 0;
@@ -455,12 +514,15 @@ static void rys_gw(int n, const real_t *a, const real_t *b2, real_t beta0, real_
 static void init_tables(void) {
     if (g_init) return;
     boys_table_init();
-    double gx[NGRID], gw[NGRID];
-    gauss_legendre(NGRID, gx, gw);
-    for (int i = 0; i < NGRID; i++) {
-        double t = 0.5 * (gx[i] + 1.0);
-        GRID_U[i] = t * t;
-        GRID_W[i] = 0.5 * gw[i];
+    for (int gs = 0; gs < 3; gs++) {
+        const int ng = 30 + 5 * gs;
+        double gx[MAXGRID], gw[MAXGRID];
+        gauss_legendre(ng, gx, gw);
+        for (int i = 0; i < ng; i++) {
+            double t = 0.5 * (gx[i] + 1.0);
+            GRID_U[gs][i] = t * t;
+            GRID_W[gs][i] = 0.5 * gw[i];
+        }
     }
     for (int n = 1; n <= MAXROOT; n++) {
         int m = 2 * n;
@@ -472,15 +534,18 @@ static void init_tables(void) {
             HW[n][i] = w[n + i];
         }
     }
-    for (int l = 0; l < 3; l++)
-        for (int c = 0; c < 6; c++) CNORM[l][c] = 1.0;
+    for (int l = 0; l <= MAXL; l++)
+        for (int c = 0; c < MAXCART; c++) CNORM[l][c] = 1.0;
     CNORM[2][3] = CNORM[2][4] = CNORM[2][5] = sqrt(3.0);
+    for (int c = 3; c < 9; c++) CNORM[3][c] = sqrt(5.0);
+    CNORM[3][9] = sqrt(5.0) * sqrt(3.0);
     g_init = 1;
 }
 
 /* Rys roots u_i = t_i^2 in (0,1) and weights w_i (sum w_i = F_0(T)).
- * asym_strict: 1 -> asymptotic when T > thr (rot-axis), 0 -> T >= thr (Rys) */
-static void rys_roots(int n, real_t T, double thr, int rot, real_t *u, real_t *w) {
+ * rot: 1 -> Boys-function rule, asymptotic when T > thr (rotated-axis and
+ * ERIC kernels), 0 -> RYSDS on an ngrid-point grid, asymptotic for T >= thr */
+static void rys_roots(int n, real_t T, double thr, int rot, int ngrid, real_t *u, real_t *w) {
     int asym = rot ? (T > thr) : (T >= thr);
     if (asym) {
         real_t it = 1.0 / T, sq = sqrt(it);
@@ -496,15 +561,17 @@ static void rys_roots(int n, real_t T, double thr, int rot, real_t *u, real_t *w
         return;
     }
     /* RYSDS: Stieltjes on the discrete measure {GRID_U, GRID_W*exp(-T u)} */
-    real_t W[NGRID], p0[NGRID], p1[NGRID];
+    const int NGRID = ngrid, gs = grid_slot(ngrid);
+    const double *GU = GRID_U[gs], *GW = GRID_W[gs];
+    real_t W[MAXGRID], p0[MAXGRID], p1[MAXGRID];
     real_t a[MAXROOT], b2[MAXROOT];
     real_t s0 = 0.0, s1 = 0.0;
     for (int j = 0; j < NGRID; j++) {
-        W[j] = GRID_W[j] * exp(-T * GRID_U[j]);
+        W[j] = GW[j] * exp(-T * GU[j]);
         p0[j] = 1.0;
         p1[j] = 0.0;
         s0 += W[j];
-        s1 += W[j] * GRID_U[j];
+        s1 += W[j] * GU[j];
     }
     real_t beta0 = s0, nprev = s0;
     a[0] = s1 / s0;
@@ -512,12 +579,12 @@ static void rys_roots(int n, real_t T, double thr, int rot, real_t *u, real_t *w
     for (int k = 1; k < n; k++) {
         real_t sa = 0.0, sb = 0.0;
         for (int j = 0; j < NGRID; j++) {
-            real_t pn = (GRID_U[j] - a[k - 1]) * p0[j];
+            real_t pn = (GU[j] - a[k - 1]) * p0[j];
             if (k > 1) pn -= b2[k - 1] * p1[j];
             p1[j] = p0[j];
             p0[j] = pn;
             sa += W[j] * pn * pn;
-            sb += W[j] * GRID_U[j] * pn * pn;
+            sb += W[j] * GU[j] * pn * pn;
         }
         a[k] = sb / sa;
         b2[k] = sa / nprev;
@@ -529,7 +596,7 @@ static void rys_roots(int n, real_t T, double thr, int rot, real_t *u, real_t *w
 /* ============================ setup ========================================= */
 static void free_ctx(ctx_t *c) {
     free(c->csh);
-    for (int l = 0; l < 3; l++) free(c->lst[l]);
+    for (int l = 0; l <= MAXL; l++) free(c->lst[l]);
     for (int k = 0; k < NPC; k++) {
         pairs_t *p = &c->pc[k];
         free(p->ish); free(p->jsh); free(p->xint); free(p->loc);
@@ -545,18 +612,18 @@ static int64_t tri_idx(int64_t i, int64_t j) { /* 1-based ia(max)+min */
 static void build_ctx(ctx_t *c, const oracle_basis *b) {
     memset(c, 0, sizeof(*c));
     c->b = b;
-    c->coef[0] = b->coef_s; c->coef[1] = b->coef_p; c->coef[2] = b->coef_d;
+    c->coef[0] = b->coef_s; c->coef[1] = b->coef_p; c->coef[2] = b->coef_d; c->coef[3] = b->coef_f;
     c->csh = (double(*)[3])malloc(sizeof(double[3]) * (b->nsh > 0 ? b->nsh : 1));
     for (int s = 0; s < b->nsh; s++)
         for (int x = 0; x < 3; x++) c->csh[s][x] = b->coords[3 * (b->atom_num[s] - 1) + x];
     /* ascending per-L lists (classify_shells final sort, :301-344) */
-    for (int l = 0; l < 3; l++) {
+    for (int l = 0; l <= MAXL; l++) {
         c->lst[l] = (int32_t *)malloc(sizeof(int32_t) * (b->nsh > 0 ? b->nsh : 1));
         c->nl[l] = 0;
     }
     for (int s = 0; s < b->nsh; s++) {
         int l = b->ang_mom[s] - 1;
-        if (l >= 0 && l < 3) c->lst[l][c->nl[l]++] = s;
+        if (l >= 0 && l <= MAXL) c->lst[l][c->nl[l]++] = s;
     }
     for (int k = 0; k < NPC; k++) {
         int l1 = PC_L1[k], l2 = PC_L2[k];
@@ -641,7 +708,7 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
         for (int x = 0; x < 3; x++) Q[x] = (gc * Cr[x] + gd * Dr[x]) / q;
         real_t ecd = exp(-gc * gd / q * rcd2);
         for (int64_t bq = pb->loc[eb_]; bq < pb->loc[eb_ + 1]; bq++) {
-            if (!kd->rys && (pb->ismlp[bq] + pk->ismlp[kq] >= 2)) continue;
+            if (kd->skip && (pb->ismlp[bq] + pk->ismlp[kq] >= 2)) continue;
             real_t ga = pb->ea[bq], gb = pb->eb[bq], p = ga + gb;
             real_t P[3], PQ2 = 0.0;
             for (int x = 0; x < 3; x++) {
@@ -652,12 +719,12 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
             real_t rho = p * q / (p + q);
             real_t T = rho * PQ2;
             real_t u[MAXROOT], w[MAXROOT];
-            rys_roots(n, T, kd->asym, !kd->rys, u, w);
+            rys_roots(n, T, kd->asym, !kd->rys, kd->ngrid, u, w);
             real_t pref = twopi52 * (pb->cc[bq] / p) * (pk->cc[kq] / q) * eab * ecd / sqrt(p + q);
             nprim++;
             /* 2D integrals per root and dimension: vertical recurrence, then
              * horizontal transfer to I[a][b][c][d] by recurrences */
-            real_t I2[MAXROOT][3][3][3][3][3];
+            real_t I2[MAXROOT][3][MAXL + 1][MAXL + 1][MAXL + 1][MAXL + 1];
             const real_t ipq = 1.0 / (p + q);
             for (int r = 0; r < n; r++) {
                 real_t ur = u[r];
@@ -667,7 +734,7 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
                 for (int x = 0; x < 3; x++) {
                     real_t C00 = (P[x] - Ar[x]) - q * ur * ipq * (P[x] - Q[x]);
                     real_t Cp00 = (Q[x] - Cr[x]) + p * ur * ipq * (P[x] - Q[x]);
-                    real_t g[5][5];
+                    real_t g[2 * MAXL + 1][2 * MAXL + 1];
                     g[0][0] = 1.0;
                     for (int i = 0; i < nij; i++) {
                         g[i + 1][0] = C00 * g[i][0];
@@ -681,7 +748,7 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
                             g[i][k + 1] = v;
                         }
                     }
-                    real_t h[5][3][5];
+                    real_t h[2 * MAXL + 1][MAXL + 1][2 * MAXL + 1];
                     for (int e = 0; e <= nij; e++)
                         for (int f = 0; f <= nkl; f++) h[e][0][f] = g[e][f];
                     for (int bb = 1; bb <= lb; bb++)
@@ -689,7 +756,7 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
                             for (int f = 0; f <= nkl; f++) h[a2][bb][f] = h[a2 + 1][bb - 1][f] + AB[x] * h[a2][bb - 1][f];
                     for (int a2 = 0; a2 <= la; a2++)
                         for (int bb = 0; bb <= lb; bb++) {
-                            real_t k2[5][3];
+                            real_t k2[2 * MAXL + 1][MAXL + 1];
                             for (int f = 0; f <= nkl; f++) k2[f][0] = h[a2][bb][f];
                             for (int dd = 1; dd <= ld; dd++)
                                 for (int cc = 0; cc <= nkl - dd; cc++) k2[cc][dd] = k2[cc + 1][dd - 1] + CD[x] * k2[cc][dd - 1];
@@ -715,7 +782,7 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
         }
     }
     ORACLE_MARK();  /* op-counting build: end of the primitive-quartet work */
-    /* component normalisation (sqrt3 on xy,xz,yz of d) */
+    /* component normalisation (sqrt3 on xy,xz,yz of d; sqrt5 / sqrt15 on f) */
     for (int ia = 0; ia < na; ia++)
     for (int ib = 0; ib < nb; ib++)
     for (int ic = 0; ic < nc; ic++)
@@ -865,13 +932,14 @@ int oracle_fock_build_jk(const oracle_basis *b, const oracle_opts *o, const doub
     nth = o->nthreads > 0 ? o->nthreads : omp_get_max_threads();
 #endif
     double *Fp = (double *)calloc((size_t)nth * ntri, sizeof(double));
-    for (int kk = 0; kk < 21; kk++) {
+    for (int kk = 0; kk < NK; kk++) {
         const kdesc_t *kd = &KD[kk];
         if (o->only_kernel >= 0 && o->only_kernel != kk) continue;
         /* driver guards (liberi_driver.F90:69-81) */
         if (kk == 0 && c.nl[0] == 0) continue;
         if (kk >= 1 && kk <= 5 && c.nl[1] == 0) continue;
-        if (kk >= 6 && c.nl[2] == 0) continue;
+        if (kk >= 6 && kk < 21 && c.nl[2] == 0) continue;
+        if (kk >= 21 && c.nl[3] == 0) continue;  /* ENABLE_F block (liberi_driver.F90:103-160) */
         const pairs_t *pb = &c.pc[kd->bra], *pk = &c.pc[kd->ket];
         if (pb->n == 0 || pk->n == 0) continue;
         /* pre-screen: cross-class maxima for rotated-axis mixed kernels,
@@ -896,7 +964,7 @@ int oracle_fock_build_jk(const oracle_basis *b, const oracle_opts *o, const doub
             tid = omp_get_thread_num();
 #endif
             double *Ft = Fp + (size_t)tid * ntri;
-            real_t vbuf[1296];
+            real_t vbuf[MAXCART * MAXCART * MAXCART * MAXCART];
 #pragma omp for schedule(dynamic, 16)
             for (int64_t it = 1; it <= niter; it++) {
                 if (o->num_procs > 1 && !oracle_rank_owns(kd->tile, niter, it, o->my_rank, o->num_procs)) continue;
@@ -964,9 +1032,9 @@ int oracle_fock_build_jk(const oracle_basis *b, const oracle_opts *o, const doub
 int oracle_schwarz(const oracle_basis *b, double *schwrz_out) {
     init_tables();
     /* evaluate with a Rys-style descriptor: no primitive skipping, the
-     * 35-point procedure below T = 60 and the large-T form above it (the
-     * 35-point grid integrates the Rys moments to ~1e-15 only up to T ~ 60) */
-    kdesc_t kd = {"schwarz", 0, 0, 0, 1, 0, OP_NONE, TILE_NONE, 0, 0, 60.0};
+     * 40-point procedure below T = 60 and the large-T form above it (the
+     * 40-point grid integrates the moments of up to 7 roots to ~1e-15 there) */
+    kdesc_t kd = {"schwarz", 0, 0, 0, 1, 0, OP_NONE, TILE_NONE, 0, 0, 60.0, 40, 0};
     oracle_basis bb = *b;
     int64_t ntri = (int64_t)b->nsh * (b->nsh + 1) / 2;
     double *dummy = (double *)malloc(sizeof(double) * (ntri > 0 ? ntri : 1));
@@ -979,7 +1047,7 @@ int oracle_schwarz(const oracle_basis *b, double *schwrz_out) {
         const pairs_t *p = &c.pc[k];
 #pragma omp parallel for schedule(dynamic, 4)
         for (int64_t e = 0; e < p->n; e++) {
-            real_t v[1296];
+            real_t v[MAXCART * MAXCART * MAXCART * MAXCART];
             int A = p->ish[e], B = p->jsh[e];
             eri_quartet(&c, A, B, A, B, p, e, p, e, &kd, v);
             int na = NCART[b->ang_mom[A] - 1], nb = NCART[b->ang_mom[B] - 1];
@@ -997,13 +1065,20 @@ int oracle_schwarz(const oracle_basis *b, double *schwrz_out) {
     return 0;
 }
 
-/* Exposes the Rys root routine for the table-accuracy tests. */
-void oracle_rys_roots(int n, double T, double thr, int rot, double *u, double *w) {
+/* Exposes the Rys root routine for the table-accuracy tests: the grid of the
+ * reference's kernels with n roots (30 points up to 4 roots, 35 for 5, 40 for
+ * 6 and 7), or ngrid points. */
+void oracle_rys_roots_grid(int n, double T, double thr, int rot, int ngrid, double *u, double *w) {
     init_tables();
     real_t ur[MAXROOT], wr[MAXROOT];
-    rys_roots(n, T, thr, rot, ur, wr);
+    if (n < 1 || n > MAXROOT) return;
+    rys_roots(n, T, thr, rot, ngrid, ur, wr);
     for (int i = 0; i < n; i++) { u[i] = (double)ur[i]; w[i] = (double)wr[i]; }
 }
 
-int oracle_num_kernels(void) { return 21; }
-const char *oracle_kernel_name(int k) { return (k >= 0 && k < 21) ? KD[k].name : ""; }
+void oracle_rys_roots(int n, double T, double thr, int rot, double *u, double *w) {
+    oracle_rys_roots_grid(n, T, thr, rot, n <= 4 ? 30 : (n == 5 ? 35 : 40), u, w);
+}
+
+int oracle_num_kernels(void) { return NK; }
+const char *oracle_kernel_name(int k) { return (k >= 0 && k < NK) ? KD[k].name : ""; }

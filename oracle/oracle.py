@@ -21,6 +21,13 @@ KERNELS = ["int0000", "int0001", "int0011", "int0111", "int0101", "int1111",
            "int0002", "int0012", "int0102", "int0112", "int0022", "int0122",
            "int1102", "int0202", "int2211", "int2121", "int2120", "int2111",
            "int2220", "int2221", "int2222"]
+# the f block of the driver, in its order (src/liberi_driver.F90:103-160)
+KERNELS_F = ["int3333", "int0030", "int0031", "int0032", "int1030", "int3330", "int3011", "int3020",
+             "int2130", "int2230", "int3030", "int3110", "int3111", "int3120", "int3121", "int2231",
+             "int3130", "int3131", "int3210", "int3331", "int3211", "int3220", "int3221", "int3222",
+             "int3230", "int3231", "int3232", "int3300", "int3310", "int3311", "int3320", "int3321",
+             "int3322", "int3332"]
+NK = len(KERNELS) + len(KERNELS_F)
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -32,7 +39,7 @@ class _Basis(ctypes.Structure):
                 ("ang_mom", _I32P), ("contr_num", _I32P), ("sh_loc", _I32P),
                 ("atom_num", _I32P), ("atom_loc", _I32P),
                 ("exponents", _F64P), ("coef_s", _F64P), ("coef_p", _F64P),
-                ("coef_d", _F64P), ("coords", _F64P), ("schwrz", _F64P)]
+                ("coef_d", _F64P), ("coef_f", _F64P), ("coords", _F64P), ("schwrz", _F64P)]
 
 
 class _Opts(ctypes.Structure):
@@ -43,9 +50,9 @@ class _Opts(ctypes.Structure):
 
 
 class _Counts(ctypes.Structure):
-    _fields_ = [("c", (ctypes.c_int64 * 4) * 21), ("t_wall", ctypes.c_double * 21),
-                ("t_eval", ctypes.c_double * 21), ("nthreads", ctypes.c_int32),
-                ("fp", (ctypes.c_uint64 * 2) * 21), ("ops", (ctypes.c_uint64 * 2) * 21)]
+    _fields_ = [("c", (ctypes.c_int64 * 4) * NK), ("t_wall", ctypes.c_double * NK),
+                ("t_eval", ctypes.c_double * NK), ("nthreads", ctypes.c_int32),
+                ("fp", (ctypes.c_uint64 * 2) * NK), ("ops", (ctypes.c_uint64 * 2) * NK)]
 
 
 _lib = None
@@ -75,6 +82,9 @@ def lib():
         _lib.oracle_rys_roots.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_int, _F64P, _F64P]
         _lib.oracle_rys_roots.restype = None
+        _lib.oracle_rys_roots_grid.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                               ctypes.c_int, ctypes.c_int, _F64P, _F64P]
+        _lib.oracle_rys_roots_grid.restype = None
         _lib.oracle_rank_owns.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int64,
                                           ctypes.c_int, ctypes.c_int]
         _lib.oracle_rank_owns.restype = ctypes.c_int
@@ -88,14 +98,15 @@ def _basis_struct(b, keep):
         return a.ctypes.data_as(_I32P)
 
     def f64(name):
-        a = np.ascontiguousarray(b[name], dtype=np.float64)
+        v = b[name] if name in b else np.zeros(len(b["exponents"]))  # bases without f: no coef_f
+        a = np.ascontiguousarray(v, dtype=np.float64)
         keep.append(a)
         return a.ctypes.data_as(_F64P)
 
     return _Basis(int(b["nsh"]), int(b["natoms"]), int(b["num_bas"]), int(b["mxgtot"]),
                   i32("ang_mom"), i32("contr_num"), i32("sh_loc"), i32("atom_num"),
                   i32("atom_loc"), f64("exponents"), f64("coef_s"), f64("coef_p"),
-                  f64("coef_d"), f64("coords"), f64("schwrz"))
+                  f64("coef_d"), f64("coef_f"), f64("coords"), f64("schwrz"))
 
 
 def fock_build(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, my_rank=0,
@@ -104,9 +115,11 @@ def fock_build(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, my_rank=0,
     """Packed F (this rank's partial) for packed D; optional per-kernel counts
     [screened quartets, primitive quartets, digested integrals, evaluated] and
     times (wall seconds per kernel, evaluation seconds summed over threads,
-    thread count).  return_info: (F, dict) with "counts", "t_wall", "t_eval",
-    "nthreads" and "fingerprint", a (21, 3) uint64 array per kernel of the
-    screened-quartet set [count, sum, xor] (see quartet_fp in the C file)."""
+    thread count), one row per kernel: the 21 s/p/d kernels, then the 34 of
+    the f block (KERNELS + KERNELS_F).  return_info: (F, dict) with "counts",
+    "t_wall", "t_eval", "nthreads" and "fingerprint", an (NK, 3) uint64 array
+    per kernel of the screened-quartet set [count, sum, xor] (see quartet_fp in
+    the C file)."""
     keep = []
     bs = _basis_struct(basis, keep)
     n = int(basis["num_bas"])
@@ -121,10 +134,10 @@ def fock_build(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, my_rank=0,
                                  ctypes.byref(cnt))
     if rc != 0:
         raise RuntimeError("oracle_fock_build failed: %d" % rc)
-    counts = np.array([[cnt.c[k][j] for j in range(4)] for k in range(21)], dtype=np.int64)
+    counts = np.array([[cnt.c[k][j] for j in range(4)] for k in range(NK)], dtype=np.int64)
     if return_info:
-        fp = np.zeros((21, 3), dtype=np.uint64)
-        for k in range(21):
+        fp = np.zeros((NK, 3), dtype=np.uint64)
+        for k in range(NK):
             fp[k] = (np.uint64(counts[k, 0]), np.uint64(cnt.fp[k][0]), np.uint64(cnt.fp[k][1]))
         return f, {"counts": counts, "t_wall": np.array(cnt.t_wall[:]), "t_eval": np.array(cnt.t_eval[:]),
                    "nthreads": int(cnt.nthreads), "fingerprint": fp}
@@ -139,7 +152,7 @@ def count_ops(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, sample_mod=1,
               nthreads=0):
     """Floating-point operations of this restatement of the reference
     algorithm, per class, from the op-counting build (oracle/opcount.cpp) on
-    a hashed 1/sample_mod sample of the screened quartets: a (21, 4) array of
+    a hashed 1/sample_mod sample of the screened quartets: an (NK, 4) array of
     [operations in primitive-quartet work, operations in shell-quartet work,
     primitive quartets evaluated, shell quartets evaluated]."""
     global _oplib
@@ -161,7 +174,7 @@ def count_ops(basis, density, *, schwarz_cut=5e-11, eri_cut=5e-11, sample_mod=1,
                                   f.ctypes.data_as(_F64P), ctypes.byref(cnt))
     if rc != 0:
         raise RuntimeError("oracle op count failed: %d" % rc)
-    return np.array([[cnt.ops[k][0], cnt.ops[k][1], cnt.c[k][1], cnt.c[k][3]] for k in range(21)],
+    return np.array([[cnt.ops[k][0], cnt.ops[k][1], cnt.c[k][1], cnt.c[k][3]] for k in range(NK)],
                     dtype=np.float64)
 
 
@@ -203,10 +216,16 @@ def schwarz(basis):
     return out
 
 
-def rys_roots(n, T, thr=55.0, rot=False):
+def rys_roots(n, T, thr=55.0, rot=False, ngrid=None):
+    """Roots and weights of the oracle's rule: the reference's grid for n roots
+    (30 points up to 4, 35 for 5, 40 for 6 and 7) unless ngrid is given."""
     u = np.zeros(n)
     w = np.zeros(n)
-    lib().oracle_rys_roots(n, T, thr, int(rot), u.ctypes.data_as(_F64P), w.ctypes.data_as(_F64P))
+    if ngrid is None:
+        lib().oracle_rys_roots(n, T, thr, int(rot), u.ctypes.data_as(_F64P), w.ctypes.data_as(_F64P))
+    else:
+        lib().oracle_rys_roots_grid(n, T, thr, int(rot), int(ngrid), u.ctypes.data_as(_F64P),
+                                    w.ctypes.data_as(_F64P))
     return u, w
 
 

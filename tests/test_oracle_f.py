@@ -1,0 +1,120 @@
+"""The oracle's f-shell restatement (the 34 kernels of the reference's ENABLE_F
+block, src/liberi_driver.F90:103-160).
+
+Pins:
+  * the reference's own f known answer (tests/fortran/test_h2o_ccpvtz.F90 with
+    fa_h2o_ccpvtz_reference.dat): that fixture's Fock rows of four oxygen
+    shells -- the third p, both d and the f shell (functions 11-35) -- are
+    exactly zero, i.e. it was produced by a build in which those shells
+    contributed nothing; the oracle reproduces every value at the fixture's
+    1e-10 when the same four shells carry zero coefficients, which pins the
+    rest of that cc-pVTZ basis (H d shells included) but says nothing about f;
+  * f integrals, component order and normalisation against an independent
+    McMurchie-Davidson evaluation (tests/md_eri.py) on a three-atom molecule
+    whose quartets fill all 34 f classes;
+  * the Rys rule for 6 and 7 roots (Gauss exactness on the Boys moments) and
+    the reference rank split for the f kernels.
+"""
+import numpy as np
+import pytest
+from scipy.special import gamma, gammainc
+
+import md_eri
+from conftest import load_kat
+from gms_liberi_b200 import molecules as M
+from oracle import oracle
+
+DROPPED_SHELLS = [6, 7, 8, 9]  # 0-based: O's third p, two d and f shells
+
+
+def test_fixture_rows_of_four_oxygen_shells_are_zero():
+    d = load_kat("h2o_ccpvtz")
+    n = d["num_bas"]
+    F = M.unpack(d["fa_ref"], n)
+    rows = []
+    for s in DROPPED_SHELLS:
+        rows += list(range(d["atom_loc"][s] - 1, d["atom_loc"][s] - 1 + [1, 3, 6, 10][d["ang_mom"][s] - 1]))
+    assert rows == list(range(10, 35))
+    assert np.abs(F[rows]).max() == 0.0
+    others = [i for i in range(n) if i not in rows]
+    assert np.abs(np.diag(F)[others]).min() > 20.0  # every other diagonal element is populated
+
+
+def test_oracle_matches_fixture_without_the_four_shells():
+    d = load_kat("h2o_ccpvtz")
+    e = dict(d)
+    for k in ("coef_s", "coef_p", "coef_d", "coef_f"):
+        e[k] = d[k].copy()
+    for s in DROPPED_SHELLS:
+        lo = d["sh_loc"][s] - 1
+        for k in ("coef_s", "coef_p", "coef_d", "coef_f"):
+            e[k][lo:lo + d["contr_num"][s]] = 0.0
+    f = oracle.fock_build(e, d["density"])
+    assert np.abs(f - d["fa_ref"]).max() <= d["tol"]
+    # with the shells present the result differs (the f kernels run: 34 classes)
+    full, cnt = oracle.fock_build(d, d["density"], return_counts=True)
+    assert np.abs(full - d["fa_ref"]).max() > 1.0
+    assert (cnt[21:, 0] > 0).all()
+
+
+@pytest.fixture(scope="module")
+def f_triatomic():
+    b = M.f_triatomic()
+    b["schwrz"] = np.full(b["nsh"] * (b["nsh"] + 1) // 2, 1e10)  # screening off, as the fixture does
+    return b, md_eri.eri_tensor(b)
+
+
+def test_oracle_f_matches_independent_integrals(f_triatomic):
+    b, G = f_triatomic
+    D = M.density(b["num_bas"], 10, seed=4)
+    F_md = md_eri.fock_from_eri(G, D)
+    F, cnt = oracle.fock_build(b, D, schwarz_cut=0.0, eri_cut=0.0, return_counts=True)
+    assert (cnt[21:, 0] > 0).all(), "every f class has quartets"
+    assert np.abs(F - F_md).max() <= 1e-10, np.abs(F - F_md).max()
+
+
+def test_oracle_f_open_shell_matches_independent_integrals(f_triatomic):
+    # F_spin = J(Da + Db) - K(2 D_spin): Coulomb updates read Da + Db, exchange updates 2 D_spin
+    b, G = f_triatomic
+    n = b["num_bas"]
+    Da, Db = M.density(n, 10, seed=5) * 0.5, M.density(n, 8, seed=6) * 0.5
+    Fa, Fb = oracle.fock_build_uhf(b, Da, Db, schwarz_cut=0.0, eri_cut=0.0)
+    assert np.abs(Fa - md_eri.fock_from_eri(G, Da + Db, 2 * Da)).max() <= 1e-10
+    assert np.abs(Fb - md_eri.fock_from_eri(G, Da + Db, 2 * Db)).max() <= 1e-10
+
+
+def test_oracle_f_schwarz_matches_independent_integrals(f_triatomic):
+    b, _ = f_triatomic
+    S = oracle.schwarz(b)
+    sh = md_eri.shells_of(b)
+    for i in range(len(sh)):
+        for j in range(i + 1):
+            v = md_eri.shell_quartet(sh[i], sh[j], sh[i], sh[j])
+            m = max(abs(v[a, c, a, c]) for a in range(v.shape[0]) for c in range(v.shape[1]))
+            assert abs(np.sqrt(m) - S[i * (i + 1) // 2 + j]) <= 1e-12 * np.sqrt(m)
+
+
+def _boys(m, T):
+    if T < 1e-13:
+        return 1.0 / (2 * m + 1)
+    return gamma(m + 0.5) * gammainc(m + 0.5, T) / (2 * T ** (m + 0.5))
+
+
+@pytest.mark.parametrize("n,thr", [(6, 60.0), (7, 65.0)])
+def test_oracle_rys_moments_six_seven_roots(n, thr):
+    # the reference's 40-point procedure below its thresholds (int3322, int3333)
+    for T in [0.0, 0.4, 3.0, 17.0, 33.0, 47.0, thr - 0.1]:
+        u, w = oracle.rys_roots(n, T, thr=thr, rot=False)
+        for k in range(2 * n):
+            ex = _boys(k, T)
+            assert abs(np.sum(w * u ** k) - ex) <= 1e-13 * ex, (n, T, k)
+
+
+@pytest.mark.parametrize("nsize", [2, 3])
+def test_oracle_f_rank_partials_sum_to_full(nsize):
+    b = M.f_triatomic(seed=1)
+    b["schwrz"] = oracle.schwarz(b)
+    D = M.density(b["num_bas"], 10, seed=2)
+    full = oracle.fock_build(b, D, schwarz_cut=1e-10)
+    parts = sum(oracle.fock_build(b, D, schwarz_cut=1e-10, my_rank=r, num_procs=nsize) for r in range(nsize))
+    assert np.abs(parts - full).max() < 1e-12
