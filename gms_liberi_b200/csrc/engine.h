@@ -3,7 +3,8 @@
 // Host side (host.cpp) builds, once per geometry, the device-resident shell,
 // pair and quartet-plan buffers described here; the device side (kernels.cu)
 // evaluates the 21 s/p/d quartet classes of the reference driver
-// (src/liberi_driver.F90:69-102) with Rys quadrature and digests them into
+// (src/liberi_driver.F90:69-102) and the 34 classes of its f block
+// (src/liberi_driver.F90:103-160) with Rys quadrature and digests them into
 // the packed Fock matrix.
 #pragma once
 
@@ -15,7 +16,9 @@
 
 namespace liberi {
 
-constexpr int NKERN = 21;
+constexpr int NKERN = 21;     // s/p/d classes: per-class kernels, FP32 tier, batching, tuning
+constexpr int NKERN_F = 34;   // f classes: one shared-memory kernel, FP64
+constexpr int NKALL = NKERN + NKERN_F;
 constexpr int NVARIANT = 3;  // kernel shape variants per class and precision
 constexpr int MAXROOT = 5;
 // Rys tables: intervals of width 1/4 in T on [0, RYS_TMAX), degree-7 power
@@ -47,8 +50,22 @@ __host__ __device__ constexpr int rysf_herm_off(int n) {
     return rysf_table_off(MAXROOT + 1) + (n - 1) * 2 * MAXROOT;
 }
 constexpr int RYSF_TABLE_SIZE = rysf_herm_off(MAXROOT + 1);
+// Tables of the f classes: 1..7 roots on [0, RYS7_TMAX) (the 7-root classes
+// switch to the large-T limit at 65), same interval width and degree as above;
+// then per n the large-T limit: MAXROOT7 r_i followed by MAXROOT7 W_i.
+constexpr int MAXROOT7 = 7;
+constexpr double RYS7_TMAX = 65.0;
+constexpr int RYS7_NINT = 65 * RYS_PER_UNIT;
+__host__ __device__ constexpr int rys7_table_off(int n) { return RYS7_NINT * RYS_NCOEF * n * (n - 1); }
+__host__ __device__ constexpr int rys7_herm_off(int n) {
+    return rys7_table_off(MAXROOT7 + 1) + (n - 1) * 2 * MAXROOT7;
+}
+constexpr int RYS7_TABLE_SIZE = rys7_herm_off(MAXROOT7 + 1);
 
-enum PairClass { SS = 0, SP, PP, SD, PD, DD, NPC };
+// the six s/p/d pair classes, then the f ones (lower-L shell first in the
+// reference order, src/liberi_shell_pair.F90:1285-1682)
+enum PairClass { SS = 0, SP, PP, SD, PD, DD, SF, PF, DF, FF, NPC };
+constexpr int NPC_SPD = 6;
 enum Op { OP_GE = 0, OP_GT = 1, OP_NONE = 2 };
 enum Tile { TILE_SQRT = 0, TILE_E9 = 1, TILE_E8 = 2, TILE_NONE = 3 };
 
@@ -67,7 +84,7 @@ struct KernelDesc {
     bool swap;           // engine rows = the reference's ket class (larger block)
     int la, lb, lc, ld;  // engine orientation: rows (A,B), kets (C,D), L_A >= L_B
 };
-extern const KernelDesc KDESC[NKERN];
+extern const KernelDesc KDESC[NKALL];
 
 // Device views ----------------------------------------------------------------
 struct DevBasis {
@@ -156,6 +173,7 @@ struct BasisHost {
     std::vector<int> ang_mom, contr_num, sh_loc, atom_num, atom_loc, start_bas, end_bas;
     std::vector<double> exponents, cs, cp, cd, cf, coords, schwrz;
 };
+constexpr int MAXL = 3;  // f
 
 struct PairsHost {
     // global pair numbering: class offsets
@@ -167,7 +185,7 @@ struct PairsHost {
     std::vector<int> kab;         // contraction-pattern key K_a * K_b
     std::vector<double4> P;
     std::vector<double2> X;
-    int nl[3] = {0, 0, 0};
+    int nl[MAXL + 1] = {0, 0, 0, 0};
 };
 
 struct DeviceBuffers {
@@ -193,6 +211,7 @@ struct DeviceBuffers {
 // Rys root/weight tables (host generated once, uploaded per handle), layout above
 const std::vector<double> &rys_table_host();
 const std::vector<float> &rys_table_f32_host();
+const std::vector<double> &rys_table7_host();  // the f classes' table (1..7 roots)
 
 // Launchers (kernels.cu) ------------------------------------------------------
 // builds of at most FAN_MAX_QUARTETS screened quartets spread their classes
@@ -216,10 +235,14 @@ struct LaunchCtx {
     double prim_cut = 0.0;
     // open-shell builds: the exchange terms read a second full matrix at D + k_offset (0 = D itself)
     size_t k_offset = 0;
+    const double *rys_tab7 = nullptr;  // f classes: the 1..7-root table
 };
 
 cudaError_t launch_class(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,
                          int precision, int nbf, int tile_rows, int variant);  // precision 0: FP64, 1: FP32
+// f class k (NKERN <= k < NKALL), FP64: one CTA per task, the task's
+// quartets in turn, every quartet evaluated and digested by the whole CTA
+cudaError_t launch_fclass(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs, int nbf);
 // adds {count, sum, xor} of the hashes of the quartets a launch of class k over
 // this plan's task list would evaluate to out[0..2] (zeroed by the caller)
 cudaError_t launch_quartet_fp(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs,

@@ -36,7 +36,7 @@ namespace liberi {
 // Engine orientation: the "rows" pair (A,B) is the class with the larger
 // Cartesian block (its rows of F are staged in shared memory), the kets (C,D)
 // the smaller; `swap` marks classes whose rows are the reference's ket list.
-const KernelDesc KDESC[NKERN] = {
+const KernelDesc KDESC[NKALL] = {
     //  name      bra ket  tri    rys    cross  op      tile       kmaj   dsch   asym  swap   la lb lc ld
     {"int0000", SS, SS, true, false, false, OP_GE, TILE_SQRT, false, true, 25.0, false, 0, 0, 0, 0},
     {"int0001", SS, SP, false, false, true, OP_GT, TILE_E9, false, true, 25.0, true, 1, 0, 0, 0},
@@ -59,10 +59,52 @@ const KernelDesc KDESC[NKERN] = {
     {"int2220", DD, SD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 2, 2, 2, 0},
     {"int2221", DD, PD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 2, 2, 2, 1},
     {"int2222", DD, DD, true, true, false, OP_NONE, TILE_NONE, false, false, 55.0, false, 2, 2, 2, 2},
+    // the f block (liberi_driver.F90:103-160): own-class pre-screens, ">"
+    // product test except int3333 (none), 3.75e8 tiles for the product
+    // kernels, bra-fastest flat order in the Rys product kernels and
+    // bra-major in the ERIC ones (int0030_ericgen.F90:66-124,
+    // int3011_rysgen.F90:213-274, int3333_rysgen.F90:829-867); digestion at
+    // 5e-11; the ERIC kernels (rys false) take the Boys-function rule with the
+    // large-T form above t_max = 25, the Rys ones switch at 43/49/55/60/65
+    // for 3..7 roots.  The rows are the reference's bra list (no swap).
+    {"int3333", FF, FF, true, true, false, OP_NONE, TILE_NONE, false, false, 65.0, false, 3, 3, 3, 3},
+    {"int0030", SS, SF, false, false, false, OP_GT, TILE_E8, false, false, 25.0, false, 0, 0, 3, 0},
+    {"int0031", SS, PF, false, false, false, OP_GT, TILE_E8, false, false, 25.0, false, 0, 0, 3, 1},
+    {"int0032", SS, DF, false, false, false, OP_GT, TILE_E8, false, false, 25.0, false, 0, 0, 3, 2},
+    {"int1030", SP, SF, false, false, false, OP_GT, TILE_E8, false, false, 25.0, false, 1, 0, 3, 0},
+    {"int3330", FF, SF, false, true, false, OP_GT, TILE_E8, true, false, 55.0, false, 3, 3, 3, 0},
+    {"int3011", SF, PP, false, true, false, OP_GT, TILE_E8, true, false, 43.0, false, 3, 0, 1, 1},
+    {"int3020", SF, SD, false, true, false, OP_GT, TILE_E8, true, false, 43.0, false, 3, 0, 2, 0},
+    {"int2130", PD, SF, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 2, 1, 3, 0},
+    {"int2230", DD, SF, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 2, 2, 3, 0},
+    {"int3030", SF, SF, true, true, false, OP_GT, TILE_NONE, false, false, 49.0, false, 3, 0, 3, 0},
+    {"int3110", PF, SP, false, true, false, OP_GT, TILE_E8, true, false, 43.0, false, 3, 1, 1, 0},
+    {"int3111", PF, PP, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 3, 1, 1, 1},
+    {"int3120", PF, SD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 3, 1, 2, 0},
+    {"int3121", PF, PD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 3, 1, 2, 1},
+    {"int2231", DD, PF, false, true, false, OP_GT, TILE_E8, true, false, 55.0, false, 2, 2, 3, 1},
+    {"int3130", PF, SF, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 3, 1, 3, 0},
+    {"int3131", PF, PF, true, true, false, OP_GT, TILE_NONE, false, false, 55.0, false, 3, 1, 3, 1},
+    {"int3210", DF, SP, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 3, 2, 1, 0},
+    {"int3331", FF, PF, false, true, false, OP_GT, TILE_E8, true, false, 60.0, false, 3, 3, 3, 1},
+    {"int3211", DF, PP, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 3, 2, 1, 1},
+    {"int3220", DF, SD, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 3, 2, 2, 0},
+    {"int3221", DF, PD, false, true, false, OP_GT, TILE_E8, true, false, 55.0, false, 3, 2, 2, 1},
+    {"int3222", DF, DD, false, true, false, OP_GT, TILE_E8, true, false, 55.0, false, 3, 2, 2, 2},
+    {"int3230", DF, SF, false, true, false, OP_GT, TILE_E8, true, false, 55.0, false, 3, 2, 3, 0},
+    {"int3231", DF, PF, false, true, false, OP_GT, TILE_E8, true, false, 55.0, false, 3, 2, 3, 1},
+    {"int3232", DF, DF, true, true, false, OP_GT, TILE_NONE, false, false, 60.0, false, 3, 2, 3, 2},
+    {"int3300", FF, SS, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 3, 3, 0, 0},
+    {"int3310", FF, SP, false, true, false, OP_GT, TILE_E8, true, false, 49.0, false, 3, 3, 1, 0},
+    {"int3311", FF, PP, false, true, false, OP_GT, TILE_E8, true, false, 55.0, false, 3, 3, 1, 1},
+    {"int3320", FF, SD, false, true, false, OP_GT, TILE_E8, true, false, 55.0, false, 3, 3, 2, 0},
+    {"int3321", FF, PD, false, true, false, OP_GT, TILE_E8, true, false, 55.0, false, 3, 3, 2, 1},
+    {"int3322", FF, DD, false, true, false, OP_GT, TILE_E8, true, false, 60.0, false, 3, 3, 2, 2},
+    {"int3332", FF, DF, false, true, false, OP_GT, TILE_E8, true, false, 60.0, false, 3, 3, 3, 2},
 };
 
-static const int PC_L1[NPC] = {0, 0, 1, 0, 1, 2};  // reference pair order (first, second)
-static const int PC_L2[NPC] = {0, 1, 1, 2, 2, 2};
+static const int PC_L1[NPC] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3};  // reference pair order (first, second)
+static const int PC_L2[NPC] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
 static const double CUX = 50.0;                    // src/liberi_parameters.F90:44
 static const double SQRT_TWOPI52 = 5.9149671727956128778;  // sqrt(2 pi^(5/2))
 static const size_t TILE_MAX_BYTES = 160 * 1024;            // shared-memory F rows per CTA
@@ -71,10 +113,12 @@ static const int TUNE_CHUNKS[] = {128, 256, 512, 1024, 2048};  // kets per CTA t
 
 static int ncart_l(int l) { return (l + 1) * (l + 2) / 2; }
 
-// default kets per CTA task (the autotuner may override per class)
+// default kets per CTA task (the autotuner may override per s/p/d class; an f
+// class CTA evaluates its task's quartets one after another)
 static int default_chunk(int k) {
     const KernelDesc &d = KDESC[k];
     const int nc = ncart_l(d.la) * ncart_l(d.lb) * ncart_l(d.lc) * ncart_l(d.ld);
+    if (k >= NKERN) return nc >= 1000 ? 2 : (nc >= 200 ? 4 : 16);
     const int qpt = nc >= 216 ? 1 : (nc >= 54 ? 2 : 4);
     return CLASS_CTA_THREADS * qpt;
 }
@@ -145,7 +189,7 @@ struct liberi_handle_s {
     // tile's shared memory costs more L1, where tables and spills live, than
     // its atomics save; measured on C60 and the batched molecules)
     uint32_t tile_mask = 0;
-    int chunk[NKERN] = {};  // kets per CTA task per class (0 = default)
+    int chunk[NKALL] = {};  // kets per CTA task per class (0 = default)
     int variant[2][NKERN] = {};  // kernel shape variant per class, FP64 / FP32 tier
     bool timing = false;
     bool last_split_lists = false;  // the last build ran the per-build FP64/FP32 task lists
@@ -157,9 +201,11 @@ struct liberi_handle_s {
     int my_rank = 0, num_procs = 1;
     BasisHost basis;
     PairsHost pairs;
-    PlanHost plan[NKERN];
+    PlanHost plan[NKALL];
+    long long fq[NKERN_F] = {}, fprim[NKERN_F] = {};  // per f class: quartets, primitive quartets
     DeviceBuffers dev;
     double *d_tab = nullptr;
+    double *d_tab7 = nullptr;  // the f classes' 1..7-root table (bases with f shells)
     float *d_tabf = nullptr;
     unsigned long long *d_maxd = nullptr;
     cudaStream_t stream = nullptr;
@@ -266,9 +312,10 @@ static void free_device(liberi_handle h) {
     h->arena = nullptr;
     h->dev = DeviceBuffers();
     h->d_tab = nullptr;
+    h->d_tab7 = nullptr;
     h->d_tabf = nullptr;
     h->d_maxd = nullptr;
-    for (int k = 0; k < NKERN; k++) h->plan[k] = PlanHost();
+    for (int k = 0; k < NKALL; k++) h->plan[k] = PlanHost();
     if (h->stream) {
         cudaStreamDestroy(h->stream);
         h->stream = nullptr;
@@ -294,15 +341,16 @@ static int validate_basis(const BasisHost &b) {
     const long long ncoef = (long long)b.nsh * b.mxgtot;
     for (int s = 0; s < b.nsh; s++) {
         int l = b.ang_mom[s];
-        if (l == 4) return fail(LIBERI_E_UNSUPPORTED, "liberi_setup: shell %d is an f shell; f classes are not built", s + 1);
-        if (l < 1 || l > 3) return fail(LIBERI_E_ARG, "liberi_setup: ang_mom(%d)=%d out of range", s + 1, l);
+        if (l < 1 || l > 4) return fail(LIBERI_E_ARG, "liberi_setup: ang_mom(%d)=%d out of range", s + 1, l);
+        if (l == 4 && b.cf.size() < (size_t)ncoef)
+            return fail(LIBERI_E_ARG, "liberi_setup: shell %d is an f shell but contr_coef_f is null", s + 1);
         if (b.contr_num[s] < 1 || b.contr_num[s] > b.mxgtot)
             return fail(LIBERI_E_ARG, "liberi_setup: contr_num(%d)=%d out of range", s + 1, b.contr_num[s]);
         if (b.sh_loc[s] < 1 || b.sh_loc[s] - 1 + b.contr_num[s] > ncoef)
             return fail(LIBERI_E_ARG, "liberi_setup: sh_loc(%d)=%d out of range", s + 1, b.sh_loc[s]);
         if (b.atom_num[s] < 1 || b.atom_num[s] > b.natoms)
             return fail(LIBERI_E_ARG, "liberi_setup: atom_num(%d)=%d out of range", s + 1, b.atom_num[s]);
-        int nc = (l == 1) ? 1 : (l == 2 ? 3 : 6);
+        int nc = l * (l + 1) / 2;
         if (b.atom_loc[s] < 1 || b.atom_loc[s] - 1 + nc > b.num_bas)
             return fail(LIBERI_E_ARG, "liberi_setup: atom_loc(%d)=%d out of range", s + 1, b.atom_loc[s]);
     }
@@ -322,12 +370,11 @@ static void build_pairs(const BasisHost &b, PairsHost &pr, std::vector<double4> 
         shell_xyz[s] = make_double4(b.coords[3 * a], b.coords[3 * a + 1], b.coords[3 * a + 2], 0.0);
     }
     // ascending per-L lists (classify_shells, liberi_shell_pair.F90:301-344)
-    std::vector<int> lst[3];
+    std::vector<int> lst[MAXL + 1];
     for (int s = 0; s < b.nsh; s++) lst[b.ang_mom[s] - 1].push_back(s);
-    for (int l = 0; l < 3; l++) pr.nl[l] = (int)lst[l].size();
-    const std::vector<double> *coef[3] = {&b.cs, &b.cp, &b.cd};
+    const std::vector<double> *coef[MAXL + 1] = {&b.cs, &b.cp, &b.cd, &b.cf};
     pr = PairsHost{};
-    for (int l = 0; l < 3; l++) pr.nl[l] = (int)lst[l].size();
+    for (int l = 0; l <= MAXL; l++) pr.nl[l] = (int)lst[l].size();
     for (int c = 0; c < NPC; c++) {
         pr.class_off[c] = (int)pr.ish.size();
         const int l1 = PC_L1[c], l2 = PC_L2[c];
@@ -508,7 +555,8 @@ static void balance_items(const PairsHost &pr, int rank, int nsize, PlanHost &ph
 static void build_plans(const PairsHost &pr, double cut, const int *chunk, int rank_split, int rank, int nprocs,
                         PlanHost *plans) {
     auto one = [&](int k) {
-        const bool run = (k == 0 && pr.nl[0] > 0) || (k >= 1 && k <= 5 && pr.nl[1] > 0) || (k >= 6 && pr.nl[2] > 0);
+        const bool run = (k == 0 && pr.nl[0] > 0) || (k >= 1 && k <= 5 && pr.nl[1] > 0) ||
+                         (k >= 6 && k < NKERN && pr.nl[2] > 0) || (k >= NKERN && pr.nl[3] > 0);
         if (!run) {
             plans[k] = PlanHost();
             return;
@@ -518,10 +566,10 @@ static void build_plans(const PairsHost &pr, double cut, const int *chunk, int r
     };
     std::atomic<int> next{0};
     auto worker = [&]() {
-        for (int k = next++; k < NKERN; k = next++) one(k);
+        for (int k = next++; k < NKALL; k = next++) one(k);
     };
     const unsigned hw = std::thread::hardware_concurrency();
-    const int nextra = (int)std::min<unsigned>(NKERN, hw > 1 ? hw : 1) - 1;
+    const int nextra = (int)std::min<unsigned>(pr.nl[3] > 0 ? NKALL : NKERN, hw > 1 ? hw : 1) - 1;
     std::vector<std::thread> pool;
     for (int t = 0; t < nextra; t++) {
         try {
@@ -565,10 +613,10 @@ static size_t plan_device_bytes(const PlanHost &ph);
 
 static int upload_plans(liberi_handle h) {
     size_t total = 0;
-    for (int k = 0; k < NKERN; k++) total += plan_device_bytes(h->plan[k]);
+    for (int k = 0; k < NKALL; k++) total += plan_device_bytes(h->plan[k]);
     CUDA_TRY(arena_open(h, h->arena_plans, total));
     ArenaScope scope{h};
-    for (int k = 0; k < NKERN; k++) {
+    for (int k = 0; k < NKALL; k++) {
         PlanHost &ph = h->plan[k];
         if (ph.nbra == 0) continue;
         {
@@ -611,22 +659,24 @@ static size_t basis_device_bytes(const BasisHost &b, const PairsHost &pr) {
            up_bytes(2 * nprim, sizeof(float4)) + up_bytes(RYS_TABLE_SIZE, sizeof(double)) +
            up_bytes(RYSF_TABLE_SIZE, sizeof(float)) + 2 * al_bytes(ntri, sizeof(double)) +
            al_bytes(nsq, sizeof(double)) + al_bytes(nsq, sizeof(float)) + al_bytes(1, sizeof(unsigned long long)) +
-           al_bytes(nprim, sizeof(float));
+           al_bytes(nprim, sizeof(float)) + (pr.nl[3] > 0 ? up_bytes(RYS7_TABLE_SIZE, sizeof(double)) : 0);
 }
 
 static void compute_stats(liberi_handle h) {
-    for (int k = 0; k < NKERN; k++) {
+    for (int k = 0; k < NKALL; k++) {
         const PlanHost &ph = h->plan[k];
         long long q = 0;
         for (const int4 &it : ph.items) q += it.z;
-        h->stats.quartets[k] = q;  // this rank's share under the balanced split
+        if (k >= NKERN) h->fq[k - NKERN] = q;
+        else h->stats.quartets[k] = q;  // this rank's share under the balanced split
         // primitive quartets: sum_i nprim(bra_i) * sum_{j<n_i} nprim(ket_j)
         std::vector<long long> kp(ph.nket + 1, 0);
         for (int j = 0; j < ph.nket; j++) kp[j + 1] = kp[j] + h->pairs.nprim[ph.ket_ids[j]];
         long long s = 0;
         for (const int4 &it : ph.items)
             s += (long long)h->pairs.nprim[ph.bra_ids[it.x]] * (kp[it.y + it.z] - kp[it.y]);
-        h->stats.prim_quartets[k] = s;
+        if (k >= NKERN) h->fprim[k - NKERN] = s;
+        else h->stats.prim_quartets[k] = s;
     }
 }
 
@@ -684,6 +734,10 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
     CUDA_TRY(dev_upload(h, &h->d_tab, tab.data(), tab.size()));
     const std::vector<float> &tabf = rys_table_f32_host();
     CUDA_TRY(dev_upload(h, &h->d_tabf, tabf.data(), tabf.size()));
+    if (h->pairs.nl[3] > 0) {
+        const std::vector<double> &tab7 = rys_table7_host();
+        CUDA_TRY(dev_upload(h, &h->d_tab7, tab7.data(), tab7.size()));
+    }
     // Bounds of the single primitive pairs (the FP32 tier's primitive
     // screening), computed on the device from the pair data and tables; then
     // every pair's primitives are put in order of decreasing bound, so that
@@ -695,13 +749,16 @@ static int upload_basis(liberi_handle h, const std::vector<double4> &shell_xyz) 
     std::vector<float> bound(nprim);
     if (nprim) {
         DevBasis db = dev_basis(h);
-        for (int c = 0; c < NPC; c++) {
+        for (int c = 0; c < NPC_SPD; c++) {
             const int o = pr.class_off[c], n = pr.class_off[c + 1] - o;
             CUDA_TRY(launch_prim_bound(c, n, o, db, h->d_tab, h->dev.prim_bound, h->stream));
         }
         CUDA_TRY(cudaMemcpyAsync(bound.data(), h->dev.prim_bound, nprim * sizeof(float), cudaMemcpyDeviceToHost,
                                  h->stream));
         CUDA_TRY(cudaStreamSynchronize(h->stream));
+        // f pairs (FP64 only) have no bounds: their primitives keep their order
+        for (int q = pr.class_off[NPC_SPD]; q < pr.class_off[NPC]; q++)
+            for (int k = pr.prim0[q]; k < pr.prim0[q] + pr.nprim[q]; k++) bound[k] = 0.0f;
         std::vector<int> ord;
         std::vector<double4> P2(pr.P.size());
         std::vector<double2> X2(pr.X.size());
@@ -766,11 +823,11 @@ static DevBasis dev_basis(liberi_handle h) {
 // ---- build ------------------------------------------------------------------------
 static int replan(liberi_handle h) {
     bool had_plans = false;
-    for (int k = 0; k < NKERN; k++) had_plans = had_plans || h->plan[k].d_bra != nullptr;
+    for (int k = 0; k < NKALL; k++) had_plans = had_plans || h->plan[k].d_bra != nullptr;
     // builds of the old plans may still run on any stream (re-plans follow an
     // option change, rarely): wait for the device before releasing them
     if (had_plans) CUDA_TRY(cudaDeviceSynchronize());
-    for (int k = 0; k < NKERN; k++) {
+    for (int k = 0; k < NKALL; k++) {
         PlanHost &ph = h->plan[k];
         // pieces of the plan arena are released with it; a task list the
         // tuner uploaded on its own is released here
@@ -995,6 +1052,18 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
             h->ev_recorded[k] = true;
         }
     }
+    // f classes (FP64 in every precision mode), in the driver's order
+    if (h->pairs.nl[3] > 0) {
+        ctx.rys_tab7 = h->d_tab7;
+        for (int k = NKERN; k < NKALL; k++) {
+            PlanHost &ph = h->plan[k];
+            if (ph.total == 0) continue;
+            DevPlan dp = dev_plan_of(h, k);
+            ctx.stream = fan ? h->fan[nfanned++ % FAN_STREAMS] : st;
+            CUDA_TRY(launch_fclass(k, ctx, dp, rank_split_of(h, k), b.num_bas));
+        }
+        ctx.stream = st;
+    }
     if (fan)  // join: the build completes on the caller's stream
         for (int i = 0; i < FAN_STREAMS; i++) {
             CUDA_TRY(cudaEventRecord(h->fan_ev[i], h->fan[i]));
@@ -1015,6 +1084,10 @@ int schwarz_host_inputs(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mx
                         const int32_t *atom_loc, const double *exponents, const double *contr_coef_s,
                         const double *contr_coef_p, const double *contr_coef_d, const double *coords,
                         BasisHost &basis, PairsHost &pairs, std::vector<double4> &shell_xyz) {
+    if (ang_mom)
+        for (int s = 0; s < nsh; s++)
+            if (ang_mom[s] == 4)
+                return fail(LIBERI_E_UNSUPPORTED, "liberi_schwarz: shell %d is an f shell; the generator covers s/p/d", s + 1);
     std::vector<double> ones((size_t)(nsh > 0 ? nsh : 0) * (nsh + 1) / 2, 1.0);
     int rc = copy_basis(basis, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num, atom_loc,
                         nullptr, nullptr, exponents, contr_coef_s, contr_coef_p, contr_coef_d, nullptr, coords,
@@ -1157,7 +1230,7 @@ int liberi_c_last_error(char *buf, int32_t len) {
     return LIBERI_OK;
 }
 
-const char *liberi_c_kernel_name(int32_t k) { return (k >= 0 && k < NKERN) ? KDESC[k].name : nullptr; }
+const char *liberi_c_kernel_name(int32_t k) { return (k >= 0 && k < NKALL) ? KDESC[k].name : nullptr; }
 
 int liberi_c_rys_eval(int32_t n, double T, double thr, int32_t strict, double *u, double *w) {
     if (n < 1 || n > MAXROOT || !u || !w || !(T >= 0.0)) return fail(LIBERI_E_ARG, "liberi_rys_eval: bad argument");
@@ -1182,6 +1255,32 @@ int liberi_c_rys_eval(int32_t n, double T, double thr, int32_t strict, double *u
         const double a2 = std::fma(c[5], x, c[4]), a3 = std::fma(c[7], x, c[6]);
         const double b0 = std::fma(a1, x2, a0), b1 = std::fma(a3, x2, a2);
         const double v = std::fma(b1, x4, b0);
+        if (f < n) u[f] = v; else w[f - n] = v;
+    }
+    return LIBERI_OK;
+}
+
+int liberi_c_rys7_eval(int32_t n, double T, double thr, int32_t strict, double *u, double *w) {
+    if (n < 1 || n > MAXROOT7 || !u || !w || !(T >= 0.0)) return fail(LIBERI_E_ARG, "liberi_rys7_eval: bad argument");
+    const std::vector<double> &tab = rys_table7_host();
+    const bool asym = strict ? (T > thr) : (T >= thr);
+    if (asym || T >= RYS7_TMAX) {
+        const double it = 1.0 / T, sq = std::sqrt(it);
+        for (int i = 0; i < n; i++) {
+            u[i] = tab[rys7_herm_off(n) + i] * it;
+            w[i] = tab[rys7_herm_off(n) + MAXROOT7 + i] * sq;
+        }
+        return LIBERI_OK;
+    }
+    const double t4 = T * (double)RYS_PER_UNIT;
+    const int k = (int)t4;
+    const double x = 2.0 * (t4 - (double)k) - 1.0, x2 = x * x, x4 = x2 * x2;
+    const double *base = tab.data() + rys7_table_off(n) + (size_t)k * 2 * n * RYS_NCOEF;
+    for (int f = 0; f < 2 * n; f++) {  // the f kernel's evaluation (k_f.cu rys7_root)
+        const double *c = base + f * RYS_NCOEF;
+        const double a0 = std::fma(c[1], x, c[0]), a1 = std::fma(c[3], x, c[2]);
+        const double a2 = std::fma(c[5], x, c[4]), a3 = std::fma(c[7], x, c[6]);
+        const double v = std::fma(std::fma(a3, x2, a2), x4, std::fma(a1, x2, a0));
         if (f < n) u[f] = v; else w[f - n] = v;
     }
     return LIBERI_OK;
@@ -1247,12 +1346,13 @@ int liberi_c_destroy(liberi_handle h) {
 int liberi_c_setup_bytes(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot, const int32_t *ang_mom,
                          const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
                          const int32_t *atom_loc, const double *exponents, const double *contr_coef_s,
-                         const double *contr_coef_p, const double *contr_coef_d, const double *coords,
-                         const double *schwrz_int, double schwarz_cut, int64_t *bytes) {
+                         const double *contr_coef_p, const double *contr_coef_d, const double *contr_coef_f,
+                         const double *coords, const double *schwrz_int, double schwarz_cut, int64_t *bytes) {
     if (!bytes) return fail(LIBERI_E_ARG, "liberi_setup_bytes: null result pointer");
     BasisHost b;
     int rc = copy_basis(b, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num, atom_loc, nullptr,
-                        nullptr, exponents, contr_coef_s, contr_coef_p, contr_coef_d, nullptr, coords, schwrz_int);
+                        nullptr, exponents, contr_coef_s, contr_coef_p, contr_coef_d, contr_coef_f, coords,
+                        schwrz_int);
     if (rc) return rc;
     rc = validate_basis(b);
     if (rc) return rc;
@@ -1260,9 +1360,9 @@ int liberi_c_setup_bytes(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t m
     std::vector<double4> shell_xyz;
     build_pairs(b, pr, shell_xyz);
     size_t total = basis_device_bytes(b, pr);
-    std::vector<PlanHost> plans(NKERN);
+    std::vector<PlanHost> plans(NKALL);
     build_plans(pr, schwarz_cut, nullptr, 0, 0, 1, plans.data());
-    for (int k = 0; k < NKERN; k++) total += plan_device_bytes(plans[k]);
+    for (int k = 0; k < NKALL; k++) total += plan_device_bytes(plans[k]);
     *bytes = (int64_t)total;
     return LIBERI_OK;
 }
@@ -1291,9 +1391,9 @@ int liberi_c_setup(liberi_handle h, int32_t nsh, int32_t natoms, int32_t num_bas
         std::vector<double4> sx;
         build_pairs(b, pr, sx);
         size_t need = basis_device_bytes(b, pr);
-        std::vector<PlanHost> plans(NKERN);
+        std::vector<PlanHost> plans(NKALL);
         build_plans(pr, h->schwarz_cut, h->chunk, h->rank_split, my_rank, num_procs, plans.data());
-        for (int k = 0; k < NKERN; k++) need += plan_device_bytes(plans[k]);
+        for (int k = 0; k < NKALL; k++) need += plan_device_bytes(plans[k]);
         if ((double)need > h->max_device_bytes)
             return fail(LIBERI_E_NOMEM, "liberi_setup: needs %zu device bytes, above max_device_bytes = %.0f", need,
                         h->max_device_bytes);
@@ -1434,6 +1534,10 @@ int liberi_c_batch_create(liberi_batch *out, const liberi_handle *handles, int32
             (h->precision == 1 && (h->fp32_cut != handles[0]->fp32_cut || h->fp32_prim != handles[0]->fp32_prim))) {
             delete b;
             return fail(LIBERI_E_ARG, "liberi_batch_create: handle %d differs in device, rank split, precision or cuts", i);
+        }
+        if (h->pairs.nl[3] > 0) {
+            delete b;
+            return fail(LIBERI_E_UNSUPPORTED, "liberi_batch_create: handle %d has f shells; batched builds cover s/p/d", i);
         }
         if (h->plan_dirty) {
             int rc = replan(h);
@@ -1844,7 +1948,15 @@ int liberi_c_get_stats(liberi_handle h, liberi_stats *stats) {
     return LIBERI_OK;
 }
 
-int liberi_c_quartet_fingerprint(liberi_handle h, uint64_t *out) {
+int liberi_c_get_class_stats(liberi_handle h, int32_t k, int64_t *out) {
+    if (!h || !out || k < 0 || k >= NKALL) return fail(LIBERI_E_ARG, "liberi_get_class_stats: bad argument");
+    out[0] = k < NKERN ? h->stats.quartets[k] : h->fq[k - NKERN];
+    out[1] = k < NKERN ? h->stats.prim_quartets[k] : h->fprim[k - NKERN];
+    return LIBERI_OK;
+}
+
+// {count, sum, xor} per class for classes 0..nclass-1 (see the header)
+static int quartet_fingerprint(liberi_handle h, int nclass, uint64_t *out) {
     if (!h || !out) return fail(LIBERI_E_ARG, "liberi_quartet_fingerprint: null argument");
     if (!h->initialized) return fail(LIBERI_E_STATE, "liberi_quartet_fingerprint called before liberi_setup");
     if (h->plan_dirty) return fail(LIBERI_E_STATE, "liberi_quartet_fingerprint: options changed since the last build");
@@ -1852,17 +1964,17 @@ int liberi_c_quartet_fingerprint(liberi_handle h, uint64_t *out) {
     CUDA_TRY(dev_guard.err);
     cudaStream_t st = h->stream;
     unsigned long long *d_out = nullptr;
-    CUDA_TRY(cudaMallocAsync((void **)&d_out, 3 * NKERN * sizeof(unsigned long long), st));
-    cudaError_t e = cudaMemsetAsync(d_out, 0, 3 * NKERN * sizeof(unsigned long long), st);
+    CUDA_TRY(cudaMallocAsync((void **)&d_out, 3 * NKALL * sizeof(unsigned long long), st));
+    cudaError_t e = cudaMemsetAsync(d_out, 0, 3 * NKALL * sizeof(unsigned long long), st);
     LaunchCtx ctx{};
     ctx.basis = dev_basis(h);
     ctx.stream = st;
-    for (int k = 0; k < NKERN && e == cudaSuccess; k++) {
+    for (int k = 0; k < nclass && e == cudaSuccess; k++) {
         const PlanHost &ph = h->plan[k];
-        if (ph.total == 0 || !((h->class_mask >> k) & 1u)) continue;
+        if (ph.total == 0 || (k < NKERN && !((h->class_mask >> k) & 1u))) continue;
         const RankSplit rs = rank_split_of(h, k);
         DevPlan dp = dev_plan_of(h, k);
-        if (!h->last_split_lists) {
+        if (!h->last_split_lists || k >= NKERN) {  // f classes: always the static FP64 list
             e = launch_quartet_fp(k, ctx, dp, rs, d_out + 3 * k);
             continue;
         }
@@ -1876,14 +1988,18 @@ int liberi_c_quartet_fingerprint(liberi_handle h, uint64_t *out) {
         dp.ntasks_dev = ph.d_ntasks + 1;
         e = launch_quartet_fp(k, ctx, dp, rs, d_out + 3 * k);
     }
-    unsigned long long host[3 * NKERN];
+    unsigned long long host[3 * NKALL];
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, d_out, sizeof(host), cudaMemcpyDeviceToHost, st);
     cudaFreeAsync(d_out, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     CUDA_TRY(e);
-    for (int i = 0; i < 3 * NKERN; i++) out[i] = host[i];
+    for (int i = 0; i < 3 * nclass; i++) out[i] = host[i];
     return LIBERI_OK;
 }
+
+int liberi_c_quartet_fingerprint(liberi_handle h, uint64_t *out) { return quartet_fingerprint(h, NKERN, out); }
+
+int liberi_c_quartet_fingerprint_all(liberi_handle h, uint64_t *out) { return quartet_fingerprint(h, NKALL, out); }
 
 int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot, const int32_t *ang_mom,
                      const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
@@ -1891,6 +2007,10 @@ int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgto
                      const double *contr_coef_p, const double *contr_coef_d, const double *coords,
                      double *schwrz_out) {
     if (!schwrz_out) return fail(LIBERI_E_ARG, "liberi_schwarz: null output");
+    if (ang_mom && nsh > 0)
+        for (int s = 0; s < nsh; s++)
+            if (ang_mom[s] == 4)
+                return fail(LIBERI_E_UNSUPPORTED, "liberi_schwarz: shell %d is an f shell; the generator covers s/p/d", s + 1);
     liberi_handle_s tmp;
     std::vector<double> ones((size_t)(nsh > 0 ? nsh : 0) * (nsh + 1) / 2, 1.0);
     int rc = copy_basis(tmp.basis, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num,

@@ -1,4 +1,5 @@
-// rys_table.cpp -- piecewise-polynomial Rys roots and weights for 1..5 roots.
+// rys_table.cpp -- piecewise-polynomial Rys roots and weights for 1..5 roots
+// (s/p/d classes) and 1..7 roots (f classes).
 //
 // The reference computes Rys roots per primitive quartet by a 35-point
 // discretised Stieltjes procedure followed by Golub-Welsch
@@ -18,7 +19,9 @@
 // against the oracle's 35-point procedure).  Above the class threshold the device
 // uses the large-T (Gauss-Hermite) limit, built here as well.  A second,
 // single-precision set (intervals of width 1/8, degree 3) serves the FP32
-// tier of the mixed-precision build.
+// tier of the mixed-precision build.  The f classes' table covers 1..7 roots
+// on [0, 65) in the same form (the reference's 6- and 7-root kernels switch
+// to the large-T limit at 60 and 65, int3322_rysgen.F90, int3333_rysgen.F90:1206).
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -110,7 +113,7 @@ void exact_rys(const Grid &g, int n, double T, double *u, double *w) {
         s0 += W[j];
         s1 += W[j] * g.u[j];
     }
-    double a[MAXROOT], b2[MAXROOT];
+    double a[MAXROOT7], b2[MAXROOT7];
     a[0] = s1 / s0;
     b2[0] = 0.0;
     double prev = s0;
@@ -197,18 +200,22 @@ void build_tables_f32() {
     }
 }
 
-void build_tables() {
+// Double-precision table of 1..nmax roots over nint intervals of width
+// 1/RYS_PER_UNIT: per n and interval, 2n functions (roots, then weights) of
+// RYS_NCOEF power-basis coefficients at tab_off(n); then per n the large-T
+// limit (nmax Gauss-Hermite r_i, then nmax W_i) at herm_off(n).
+template <typename OffT, typename HermT>
+void fill_table(int nmax, int nint, OffT tab_off, HermT herm_off, std::vector<double> &out) {
     Grid g;
-    g_table.assign(RYS_TABLE_SIZE, 0.0);
     const int M = RYS_DEG + 1;  // interpolation nodes / coefficients
     std::vector<double> xs(M);
     for (int m = 0; m < M; m++) xs[m] = std::cos(PI * (m + 0.5) / M);
-    for (int n = 1; n <= MAXROOT; n++) {
-        for (int k = 0; k < RYS_NINT; k++) {
+    for (int n = 1; n <= nmax; n++) {
+        for (int k = 0; k < nint; k++) {
             std::vector<std::vector<double>> f(2 * n, std::vector<double>(M));
             for (int m = 0; m < M; m++) {
                 double T = (k + 0.5 * (xs[m] + 1.0)) / RYS_PER_UNIT;
-                double u[MAXROOT], w[MAXROOT];
+                double u[MAXROOT7], w[MAXROOT7];
                 exact_rys(g, n, T, u, w);
                 for (int i = 0; i < n; i++) {
                     f[i][m] = u[i];
@@ -216,52 +223,40 @@ void build_tables() {
                 }
             }
             for (int fi = 0; fi < 2 * n; fi++) {
-                // Chebyshev interpolation coefficients
-                std::vector<double> c(M, 0.0);
-                for (int j = 0; j < M; j++) {
-                    double s = 0.0;
-                    for (int m = 0; m < M; m++) s += f[fi][m] * std::cos(PI * j * (m + 0.5) / M);
-                    c[j] = 2.0 * s / M;
-                }
-                c[0] *= 0.5;
-                // to power basis in x
-                // T_0 = 1, T_1 = x, T_{j+1} = 2x T_j - T_{j-1}
-                std::vector<double> pw(M, 0.0), tprev(M, 0.0), tcur(M, 0.0);
-                tcur[0] = 1.0;
-                for (int j = 0; j < M; j++) {
-                    if (j == 1) {
-                        tprev = tcur;
-                        std::fill(tcur.begin(), tcur.end(), 0.0);
-                        tcur[1] = 1.0;
-                    } else if (j > 1) {
-                        std::vector<double> tn(M, 0.0);
-                        for (int i = 0; i + 1 < M; i++) tn[i + 1] += 2.0 * tcur[i];
-                        for (int i = 0; i < M; i++) tn[i] -= tprev[i];
-                        tprev = tcur;
-                        tcur = tn;
-                    }
-                    for (int i = 0; i < M; i++) pw[i] += c[j] * tcur[i];
-                }
-                double *dst = &g_table[rys_table_off(n) + ((size_t)k * 2 * n + fi) * RYS_NCOEF];
+                std::vector<double> pw = cheb_to_power(f[fi]);
+                double *dst = &out[tab_off(n) + ((size_t)k * 2 * n + fi) * RYS_NCOEF];
                 for (int i = 0; i < M; i++) dst[i] = pw[i];
                 for (int i = M; i < RYS_NCOEF; i++) dst[i] = 0.0;
             }
         }
     }
     // Gauss-Hermite (2n points) positive half: large-T limit
-    for (int n = 1; n <= MAXROOT; n++) {
+    for (int n = 1; n <= nmax; n++) {
         int m = 2 * n;
-        double a[2 * MAXROOT], b2[2 * MAXROOT], x[2 * MAXROOT], w[2 * MAXROOT];
+        double a[2 * MAXROOT7], b2[2 * MAXROOT7], x[2 * MAXROOT7], w[2 * MAXROOT7];
         for (int i = 0; i < m; i++) {
             a[i] = 0.0;
             b2[i] = 0.5 * i;
         }
         jacobi_rule(m, a, b2, std::sqrt(PI), -(double)m, (double)m, x, w);
         for (int i = 0; i < n; i++) {
-            g_table[rys_herm_off(n) + i] = x[n + i] * x[n + i];
-            g_table[rys_herm_off(n) + MAXROOT + i] = w[n + i];
+            out[herm_off(n) + i] = x[n + i] * x[n + i];
+            out[herm_off(n) + nmax + i] = w[n + i];
         }
     }
+}
+
+void build_tables() {
+    g_table.assign(RYS_TABLE_SIZE, 0.0);
+    fill_table(MAXROOT, RYS_NINT, rys_table_off, rys_herm_off, g_table);
+}
+
+std::vector<double> g_table7;
+std::once_flag g_once7;
+
+void build_tables7() {
+    g_table7.assign(RYS7_TABLE_SIZE, 0.0);
+    fill_table(MAXROOT7, RYS7_NINT, rys7_table_off, rys7_herm_off, g_table7);
 }
 
 }  // namespace
@@ -274,6 +269,11 @@ const std::vector<double> &rys_table_host() {
 const std::vector<float> &rys_table_f32_host() {
     std::call_once(g_once_f, build_tables_f32);
     return g_table_f;
+}
+
+const std::vector<double> &rys_table7_host() {
+    std::call_once(g_once7, build_tables7);
+    return g_table7;
 }
 
 

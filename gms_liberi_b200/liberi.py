@@ -25,6 +25,14 @@ KERNELS = ["int0000", "int0001", "int0011", "int0111", "int0101", "int1111",
            "int0002", "int0012", "int0102", "int0112", "int0022", "int0122",
            "int1102", "int0202", "int2211", "int2121", "int2120", "int2111",
            "int2220", "int2221", "int2222"]
+# the f block of the reference driver, in its order (src/liberi_driver.F90:103-160)
+KERNELS_F = ["int3333", "int0030", "int0031", "int0032", "int1030", "int3330", "int3011", "int3020",
+             "int2130", "int2230", "int3030", "int3110", "int3111", "int3120", "int3121", "int2231",
+             "int3130", "int3131", "int3210", "int3331", "int3211", "int3220", "int3221", "int3222",
+             "int3230", "int3231", "int3232", "int3300", "int3310", "int3311", "int3320", "int3321",
+             "int3322", "int3332"]
+KERNELS_ALL = KERNELS + KERNELS_F
+NCLASS = len(KERNELS_ALL)
 
 EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fock_build",
            "liberi_c_cleanup", "liberi_c_init", "liberi_c_fock", "liberi_c_finalize",
@@ -39,7 +47,8 @@ EXPORTS = ["liberi_c_create", "liberi_c_destroy", "liberi_c_setup", "liberi_c_fo
            "liberi_c_mdi_payload", "liberi_c_mdi_execute", "liberi_c_mdi_destroy",
            "liberi_c_quartet_fingerprint", "liberi_c_fock_build_uhf", "liberi_c_fock_build_uhf_device",
            "liberi_c_mdi_set_comm", "liberi_c_comm_unique_id", "liberi_c_comm_create", "liberi_c_comm_allreduce",
-           "liberi_c_comm_reduce_host", "liberi_c_comm_destroy"]
+           "liberi_c_comm_reduce_host", "liberi_c_comm_destroy", "liberi_c_get_class_stats",
+           "liberi_c_quartet_fingerprint_all", "liberi_c_rys7_eval"]
 
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
@@ -105,8 +114,12 @@ def lib():
                                                      ctypes.c_void_p, ctypes.c_void_p]
         L.liberi_c_setup_bytes.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                            _I32P, _I32P, _I32P, _I32P, _I32P,
-                                           _F64P, _F64P, _F64P, _F64P, _F64P, _F64P, ctypes.c_double,
+                                           _F64P, _F64P, _F64P, _F64P, _F64P, _F64P, _F64P, ctypes.c_double,
                                            ctypes.POINTER(ctypes.c_int64)]
+        L.liberi_c_get_class_stats.argtypes = [H, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
+        L.liberi_c_quartet_fingerprint_all.argtypes = [H, ctypes.POINTER(ctypes.c_uint64)]
+        L.liberi_c_rys7_eval.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                                         _F64P, _F64P]
         L.liberi_c_schwarz_noalloc.argtypes = L.liberi_c_schwarz.argtypes
         L.liberi_c_rys_eval.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                         _F64P, _F64P]
@@ -186,19 +199,28 @@ class LiberiHandle:
         return v.value
 
     def stats(self):
+        """Per-class arrays over all 55 classes (KERNELS_ALL: the 21 s/p/d, then
+        the f block): quartets and prim_quartets of this rank; fp32_quartets and
+        kernel_ms (s/p/d only, zero for the f classes)."""
         s = Stats()
         _check(lib().liberi_c_get_stats(self._h, ctypes.byref(s)))
-        return {"quartets": np.array(s.quartets[:]), "fp32_quartets": np.array(s.fp32_quartets[:]),
-                "prim_quartets": np.array(s.prim_quartets[:]), "kernel_ms": np.array(s.kernel_ms[:]),
+        q, pq = np.zeros(NCLASS, dtype=np.int64), np.zeros(NCLASS, dtype=np.int64)
+        pair = (ctypes.c_int64 * 2)()
+        for k in range(NCLASS):
+            _check(lib().liberi_c_get_class_stats(self._h, k, pair))
+            q[k], pq[k] = pair[0], pair[1]
+        pad = np.zeros(NCLASS - 21)
+        return {"quartets": q, "fp32_quartets": np.concatenate([np.array(s.fp32_quartets[:]), pad.astype(np.int64)]),
+                "prim_quartets": pq, "kernel_ms": np.concatenate([np.array(s.kernel_ms[:]), pad]),
                 "build_ms": s.build_ms, "device_bytes": s.device_bytes}
 
     def quartet_fingerprint(self):
-        """(21, 3) uint64: per class in driver order the number, sum and xor of
-        the 64-bit hashes of the quartets the last build evaluated (on the
+        """(55, 3) uint64: per class (KERNELS_ALL order) the number, sum and xor
+        of the 64-bit hashes of the quartets the last build evaluated (on the
         device, over the same task lists; see liberi_c_quartet_fingerprint)."""
-        out = (ctypes.c_uint64 * 63)()
-        _check(lib().liberi_c_quartet_fingerprint(self._h, out))
-        return np.array(out[:], dtype=np.uint64).reshape(21, 3)
+        out = (ctypes.c_uint64 * (3 * NCLASS))()
+        _check(lib().liberi_c_quartet_fingerprint_all(self._h, out))
+        return np.array(out[:], dtype=np.uint64).reshape(NCLASS, 3)
 
     def destroy(self):
         if self._h:
@@ -472,6 +494,14 @@ def rys_eval(n, T, thr=60.0, strict=False):
     return u, w
 
 
+def rys7_eval(n, T, thr=65.0, strict=False):
+    """The f classes' Rys roots/weights, n = 1..7 (host evaluation of their table)."""
+    u = np.zeros(n)
+    w = np.zeros(n)
+    _check(lib().liberi_c_rys7_eval(n, T, thr, int(strict), u.ctypes.data_as(_F64P), w.ctypes.data_as(_F64P)))
+    return u, w
+
+
 def rys_eval_f32(n, T, thr=60.0, strict=False):
     """FP32-tier Rys roots/weights (host evaluation in single precision)."""
     u = np.zeros(n, dtype=np.float32)
@@ -488,7 +518,7 @@ def setup_bytes(basis, schwarz_cut=5.00000000000000018e-11):
     out = ctypes.c_int64()
     _check(lib().liberi_c_setup_bytes(nsh, natoms, nbf, mx, _i32(ang, k), _i32(cn, k), _i32(sl, k), _i32(an, k),
                                       _i32(al, k), _f64(ex, k), _f64(cs, k), _f64(cp, k), _f64(cd, k),
-                                      _f64(xyz, k), _f64(basis["schwrz"], k), float(schwarz_cut),
+                                      _f64(cf, k), _f64(xyz, k), _f64(basis["schwrz"], k), float(schwarz_cut),
                                       ctypes.byref(out)))
     return int(out.value)
 

@@ -13,8 +13,10 @@
  *     n(n+1)/2, element (i,j), i>=j, 1-based, at ia(i)+j with ia(i)=i(i-1)/2
  *     (src/liberi_shell_pair.F90:131-133, src/rhf/rot_axis/int0000.F90:273-283);
  *   - schwrz_int is packed the same way over shells;
- *   - sh_loc, atom_num, atom_loc are 1-based; ang_mom 1=s 2=p 3=d;
- *     Cartesian d order xx,yy,zz,xy,xz,yz with sqrt(3) on xy,xz,yz.
+ *   - sh_loc, atom_num, atom_loc are 1-based; ang_mom 1=s 2=p 3=d 4=f;
+ *     Cartesian d order xx,yy,zz,xy,xz,yz with sqrt(3) on xy,xz,yz; f order
+ *     xxx,yyy,zzz,xxy,xxz,xyy,yyz,xzz,yzz,xyz with sqrt(5) on the six mixed
+ *     components and sqrt(15) on xyz (src/rhf/rys/int3011_rysgen.F90).
  * All integer arguments are int32_t (the reference requires c_int at the
  * boundary), all real arrays double.
  */
@@ -36,7 +38,7 @@ enum {
     LIBERI_E_SIZE = -3,       /* matrix_size != num_bas(num_bas+1)/2 */
     LIBERI_E_DEVICE = -4,     /* CUDA error */
     LIBERI_E_NOMEM = -5,      /* device allocation failed or over limit */
-    LIBERI_E_UNSUPPORTED = -6 /* f shells (ang_mom 4) are not built; num_bas > 65535 */
+    LIBERI_E_UNSUPPORTED = -6 /* num_bas > 65535; f shells in the Schwarz generator or a batch; NCCL absent */
 };
 
 /* ---- handle API: src/interface/liberi_interface.F90 --------------------- */
@@ -159,7 +161,8 @@ int liberi_c_fock_build_uhf_device(liberi_handle handle, const double *d_density
 
 /* Schwarz table generator: schwrz_out[ia(max)+min] = sqrt(max_components
  * |(ab|ab)|) over shell pairs, computed on the device (GAMESS supplies this
- * table to the reference, liberi_interface.F90:128-129). */
+ * table to the reference, liberi_interface.F90:128-129).  s/p/d shells; a
+ * basis with f shells is rejected with LIBERI_E_UNSUPPORTED. */
 int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot,
                      const int32_t *ang_mom, const int32_t *contr_num, const int32_t *sh_loc,
                      const int32_t *atom_num, const int32_t *atom_loc, const double *exponents,
@@ -184,8 +187,9 @@ int liberi_c_schwarz_noalloc(int32_t nsh, int32_t natoms, int32_t num_bas, int32
                              const double *contr_coef_s, const double *contr_coef_p,
                              const double *contr_coef_d, const double *coords, double *schwrz_out);
 
-/* Per-kernel statistics of the last build, 21 rows in the reference driver
- * order (liberi_driver.F90:69-102):
+/* Per-kernel statistics of the last build, the 21 s/p/d rows in the reference
+ * driver order (liberi_driver.F90:69-102; the f classes through
+ * liberi_c_get_class_stats):
  *   quartets[k]     screened shell quartets owned by this rank
  *   fp32_quartets[k] of those, evaluated in FP32
  *   prim_quartets[k] primitive quartets (after mu*R^2 > 50 pair removal)
@@ -199,6 +203,11 @@ typedef struct {
     int64_t device_bytes;
 } liberi_stats;
 int liberi_c_get_stats(liberi_handle handle, liberi_stats *stats);
+/* Class k of all 55 (0..20 the s/p/d kernels, 21..54 the f block in the
+ * driver's order, liberi_driver.F90:103-160): out[0] screened shell quartets
+ * owned by this rank, out[1] primitive quartets.  No counterpart in the
+ * reference. */
+int liberi_c_get_class_stats(liberi_handle handle, int32_t k, int64_t *out);
 
 /* Fingerprint of the screened-quartet set, for parity checks.  No counterpart
  * in the reference (its kernels enumerate the set implicitly: pre-screen and
@@ -215,6 +224,9 @@ int liberi_c_get_stats(liberi_handle handle, liberi_stats *stats);
  * Runs on the device, synchronous; fails if options changed since the last
  * build (the plan would be rebuilt first). */
 int liberi_c_quartet_fingerprint(liberi_handle handle, uint64_t *out);
+/* The same for all 55 classes (out[3*55]; the f classes always evaluate their
+ * static FP64 lists). */
+int liberi_c_quartet_fingerprint_all(liberi_handle handle, uint64_t *out);
 
 /* Device bytes liberi_c_setup would allocate for this basis at this Schwarz
  * cut (host-only dry run of the pair and plan construction, no device
@@ -223,13 +235,14 @@ int liberi_c_quartet_fingerprint(liberi_handle handle, uint64_t *out);
 int liberi_c_setup_bytes(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot, const int32_t *ang_mom,
                          const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
                          const int32_t *atom_loc, const double *exponents, const double *contr_coef_s,
-                         const double *contr_coef_p, const double *contr_coef_d, const double *coords,
-                         const double *schwrz_int, double schwarz_cut, int64_t *bytes);
+                         const double *contr_coef_p, const double *contr_coef_d, const double *contr_coef_f,
+                         const double *coords, const double *schwrz_int, double schwarz_cut, int64_t *bytes);
 
 /* Batched Fock builds over several set-up handles (one molecule each): one
  * launch per quartet class covers every molecule (a persistent multi-molecule
  * work list), preceded by one launch that zeroes every F.  No counterpart in
- * the reference.  Handles must share device, cuts and precision (FP64, or
+ * the reference.  Handles must have s/p/d bases (f shells: LIBERI_E_UNSUPPORTED)
+ * and share device, cuts and precision (FP64, or
  * mixed with one fp32_cut: each iteration then splits every molecule's work
  * at its own max|D| on the device, inside the captured graph) and use one rank.
  *   bind:     device density / Fock buffer of every molecule (kept by address);
@@ -272,6 +285,9 @@ int liberi_c_rys_eval(int32_t n, double T, double thr, int32_t strict, double *u
  * single precision exactly as the device does.  No counterpart in the
  * reference. */
 int liberi_c_rys_eval_f32(int32_t n, float T, float thr, int32_t strict, float *u, float *w);
+/* The f classes' tables (n = 1..7 roots on [0, 65)), evaluated as the f
+ * kernel does.  No counterpart in the reference. */
+int liberi_c_rys7_eval(int32_t n, double T, double thr, int32_t strict, double *u, double *w);
 
 /* Device microbenchmarks on the current device (roofline denominators):
  *   kind 0: FP64 FMA throughput, TFLOP/s
@@ -282,7 +298,8 @@ int liberi_c_rys_eval_f32(int32_t n, float T, float thr, int32_t strict, float *
  *           array, random addresses), Gatomic/s */
 int liberi_c_microbench(int32_t kind, double *result);
 
-/* Name of kernel class k (0..20), e.g. "int2222"; NULL if out of range. */
+/* Name of kernel class k (0..54: the 21 s/p/d classes, then the f block),
+ * e.g. "int2222"; NULL if out of range. */
 const char *liberi_c_kernel_name(int32_t k);
 
 /* ---- MDI plugin command set (liberi_mdi_api.F90:194-428), transport-free ----

@@ -25,9 +25,11 @@ def test_header_symbols_exported():
 
 def test_kernel_names_in_driver_order():
     L = liberi.lib()
-    names = [L.liberi_c_kernel_name(i).decode() for i in range(21)]
-    assert names == liberi.KERNELS
-    assert L.liberi_c_kernel_name(21) is None
+    names = [L.liberi_c_kernel_name(i).decode() for i in range(55)]
+    assert names == liberi.KERNELS_ALL  # the s/p/d kernels, then the f block
+    assert L.liberi_c_kernel_name(55) is None
+    from oracle import oracle
+    assert liberi.KERNELS_ALL == oracle.KERNELS + oracle.KERNELS_F
 
 
 def test_fock_before_setup_is_state_error():
@@ -79,13 +81,16 @@ def test_launch_options_round_trip():
     liberi.liberi_destroy(h)
 
 
-@pytest.mark.parametrize("bad", ["fshell", "rank", "sizes", "num_bas"])
+@pytest.mark.parametrize("bad", ["gshell", "fshell_size", "rank", "sizes", "num_bas"])
 def test_setup_rejects_bad_input(bad):
     h = liberi.liberi_create()
     args = dict(nsh=1, natoms=1, num_bas=1, mxgtot=1, ang=[1], rank=0, nproc=1)
-    if bad == "fshell":
+    if bad == "gshell":  # ang_mom 5 (g) is beyond the reference's kernels
+        args["ang"] = [5]
+        code = -1
+    elif bad == "fshell_size":  # an f shell's ten functions do not fit num_bas = 1
         args["ang"] = [4]
-        code = -6
+        code = -1
     elif bad == "num_bas":
         # n(n+1)/2 of 65536 functions exceeds the int32 matrix_size
         args["num_bas"] = 65536
@@ -106,16 +111,39 @@ def test_setup_rejects_bad_input(bad):
 
 @pytest.mark.parametrize("n", [1, 2, 3, 4, 5])
 def test_engine_rys_tables_match_oracle(n):
-    # the piecewise tables reproduce the reference's 35-point Stieltjes roots
+    # the piecewise tables reproduce the Stieltjes roots: the oracle's 40-point
+    # rule on the whole table range, the reference's own grid for n roots
+    # (30 points up to 4, 35 for 5) below that class's threshold
     from oracle import oracle
     rng = np.random.default_rng(n)
+    thr_ref = {1: 43.0, 2: 43.0, 3: 43.0, 4: 49.0, 5: 55.0}[n]
     for T in np.concatenate([[0.0, 1e-9, 0.5, 24.999, 25.0, 42.99, 59.9], rng.uniform(0, 60, 40)]):
         ue, we = liberi.rys_eval(n, float(T), thr=60.0)
-        uo, wo = oracle.rys_roots(n, float(T), thr=60.0)
+        uo, wo = oracle.rys_roots(n, float(T), thr=60.0, ngrid=40)
         assert np.allclose(ue, uo, rtol=5e-13, atol=0), (n, T)
         assert np.allclose(we, wo, rtol=5e-13, atol=0), (n, T)
+        if T < thr_ref:
+            ur, wr = oracle.rys_roots(n, float(T), thr=thr_ref)
+            assert np.allclose(ue, ur, rtol=5e-13, atol=0), (n, T)
+            assert np.allclose(we, wr, rtol=5e-13, atol=0), (n, T)
     for T in [25.5, 70.0, 300.0]:
         ue, we = liberi.rys_eval(n, T, thr=25.0, strict=True)
+        uo, wo = oracle.rys_roots(n, T, thr=25.0, rot=True)
+        assert np.allclose(ue, uo, rtol=1e-14) and np.allclose(we, wo, rtol=1e-14)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7])
+def test_engine_rys7_tables_match_oracle(n):
+    # the f classes' table (1..7 roots on [0, 65)) against the oracle's 40-point rule
+    from oracle import oracle
+    rng = np.random.default_rng(100 + n)
+    for T in np.concatenate([[0.0, 1e-9, 0.5, 24.999, 25.0, 42.99, 59.9, 64.9], rng.uniform(0, 65, 40)]):
+        ue, we = liberi.rys7_eval(n, float(T), thr=65.0)
+        uo, wo = oracle.rys_roots(n, float(T), thr=65.0, ngrid=40)
+        assert np.allclose(ue, uo, rtol=5e-13, atol=0), (n, T, ue, uo)
+        assert np.allclose(we, wo, rtol=5e-13, atol=0), (n, T, we, wo)
+    for T in [25.5, 70.0, 300.0]:
+        ue, we = liberi.rys7_eval(n, T, thr=25.0, strict=True)
         uo, wo = oracle.rys_roots(n, T, thr=25.0, rot=True)
         assert np.allclose(ue, uo, rtol=1e-14) and np.allclose(we, wo, rtol=1e-14)
 

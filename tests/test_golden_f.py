@@ -1,9 +1,8 @@
 """The reference's f-shell known answer (H2O / cc-pVTZ: s, p, d and one f
 shell; 65 functions, 2145 packed Fock values at tol 1e-10, identity density,
-screening off), kept as a fixture for the f-shell classes, which this engine
-does not build yet.  Pinned here: the fixture is consistent, and setup through
-the C ABI rejects its f shell cleanly (LIBERI_E_UNSUPPORTED naming the shell)
-rather than building a partial F."""
+screening off), kept as a fixture.  Pinned here: the fixture is consistent
+with its basis, and the host half of setup plans the f classes for it (the
+value checks are in tests/test_oracle_f.py and tests/test_gpu_f.py)."""
 import numpy as np
 import pytest
 
@@ -27,13 +26,11 @@ def test_f_fixture_is_consistent():
     assert np.isfinite(d["fa_ref"]).all()
 
 
-def test_setup_rejects_the_f_shell():
+def test_setup_bytes_plan_the_f_classes():
+    # host-only dry run of setup: the f pair classes and the 34 f class plans
+    # add device bytes; the Schwarz generator still covers s/p/d only
     d = load_kat("h2o_ccpvtz")
-    h = liberi.liberi_create()
-    with pytest.raises(liberi.LiberiError) as e:
-        liberi.liberi_setup(h, d["nsh"], d["natoms"], d["num_bas"], d["mxgtot"], d["ang_mom"], d["contr_num"],
-                            d["sh_loc"], d["atom_num"], d["atom_loc"], d["start_bas"], d["end_bas"], d["exponents"],
-                            d["coef_s"], d["coef_p"], d["coef_d"], d["coef_f"], d["coords"], d["schwrz"], 0, 1)
-    assert e.value.code == -6
-    assert "shell 10" in str(e.value) and "f shell" in str(e.value)
-    liberi.liberi_destroy(h)
+    assert liberi.setup_bytes(d, 5e-11) > 0
+    with pytest.raises(liberi.LiberiError) as err:
+        liberi.schwarz(d)  # rejected on the host, before any device call
+    assert err.value.code == -6 and "f shell" in str(err.value)
