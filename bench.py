@@ -288,7 +288,7 @@ def run_ours(args):
             step()
             ev[s][1].record(stream)
             if per_class:
-                cls += h.stats()["kernel_ms"]
+                cls += h.stats()["kernel_ms"][:21]  # the s/p/d classes (C60 has no f shells)
         barrier()
         ms = [a.elapsed_time(b) for a, b in ev]
         return float(np.mean(ms)), cls / max(1, nsteps)
