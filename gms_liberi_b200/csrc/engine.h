@@ -271,6 +271,10 @@ cudaError_t launch_maxabs(const double *x, long long n, unsigned long long *out,
 cudaError_t launch_split_tasks(int nitems, const int4 *items, const double *bra_x, const double *ket_x,
                                const unsigned long long *maxd, double fp32_cut, int chunk,
                                int4 *tasks64, int4 *tasks32, int *counts, cudaStream_t stream);
+// Schwarz values of the f pair classes (sf, pf, df, ff) with the f classes'
+// shared-memory evaluation and the 1..7-root table (k_f.cu)
+cudaError_t launch_fschwarz(int pair_class, int npairs, int pair_off, const DevBasis &b, const double *rys_tab7,
+                            double *out, cudaStream_t stream);
 cudaError_t launch_schwarz(int pair_class, int npairs, int pair_off, const DevBasis &b,
                            const double *rys_tab, double *out_per_pair, cudaStream_t stream);
 // per primitive pair of one pair class: sqrt(max |(ab|ab)|) of the primitive alone, rounded up to float

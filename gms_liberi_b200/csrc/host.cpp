@@ -118,7 +118,7 @@ static int ncart_l(int l) { return (l + 1) * (l + 2) / 2; }
 static int default_chunk(int k) {
     const KernelDesc &d = KDESC[k];
     const int nc = ncart_l(d.la) * ncart_l(d.lb) * ncart_l(d.lc) * ncart_l(d.ld);
-    if (k >= NKERN) return nc >= 1000 ? 2 : (nc >= 200 ? 4 : 16);
+    if (k >= NKERN) return nc >= 1000 ? 1 : (nc >= 200 ? 2 : 8);
     const int qpt = nc >= 216 ? 1 : (nc >= 54 ? 2 : 4);
     return CLASS_CTA_THREADS * qpt;
 }
@@ -2004,18 +2004,14 @@ int liberi_c_quartet_fingerprint_all(liberi_handle h, uint64_t *out) { return qu
 int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot, const int32_t *ang_mom,
                      const int32_t *contr_num, const int32_t *sh_loc, const int32_t *atom_num,
                      const int32_t *atom_loc, const double *exponents, const double *contr_coef_s,
-                     const double *contr_coef_p, const double *contr_coef_d, const double *coords,
-                     double *schwrz_out) {
+                     const double *contr_coef_p, const double *contr_coef_d, const double *contr_coef_f,
+                     const double *coords, double *schwrz_out) {
     if (!schwrz_out) return fail(LIBERI_E_ARG, "liberi_schwarz: null output");
-    if (ang_mom && nsh > 0)
-        for (int s = 0; s < nsh; s++)
-            if (ang_mom[s] == 4)
-                return fail(LIBERI_E_UNSUPPORTED, "liberi_schwarz: shell %d is an f shell; the generator covers s/p/d", s + 1);
     liberi_handle_s tmp;
     std::vector<double> ones((size_t)(nsh > 0 ? nsh : 0) * (nsh + 1) / 2, 1.0);
     int rc = copy_basis(tmp.basis, nsh, natoms, num_bas, mxgtot, ang_mom, contr_num, sh_loc, atom_num,
                         atom_loc, nullptr, nullptr, exponents, contr_coef_s, contr_coef_p, contr_coef_d,
-                        nullptr, coords, ones.data());
+                        contr_coef_f, coords, ones.data());
     if (rc) return rc;
     rc = validate_basis(tmp.basis);
     if (rc) return rc;
@@ -2034,7 +2030,9 @@ int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgto
         DevBasis db = dev_basis(&tmp);
         for (int c = 0; c < NPC && !rc; c++) {
             int off = tmp.pairs.class_off[c], n = tmp.pairs.class_off[c + 1] - off;
-            cudaError_t e = launch_schwarz(c, n, off, db, tmp.d_tab, d_out + off, tmp.stream);
+            // s/p/d pair classes by their Rys kernels, f ones by the f classes' evaluation
+            cudaError_t e = c < NPC_SPD ? launch_schwarz(c, n, off, db, tmp.d_tab, d_out + off, tmp.stream)
+                                        : launch_fschwarz(c, n, off, db, tmp.d_tab7, d_out, tmp.stream);
             if (e != cudaSuccess) rc = fail(LIBERI_E_DEVICE, "liberi_schwarz: %s", cudaGetErrorString(e));
         }
     }

@@ -3,9 +3,11 @@
 // the generated Rys kernels, src/rhf/eric, src/rhf/rys).
 //
 // An f quartet is too large for the thread-per-quartet class kernels ((ff|ff)
-// holds 10,000 integrals and 7 roots), so one CTA evaluates one shell quartet
-// at a time, everything in shared memory, with the class's angular momenta as
-// run-time parameters (one kernel serves all 34 classes):
+// holds 10,000 integrals and 7 roots), so a group of threads evaluates one
+// shell quartet at a time, everything in shared memory, with the class's
+// angular momenta as run-time parameters (one kernel serves all 34 classes).
+// The group is one warp (four tasks per CTA, warp barriers only) where the
+// quartet's working set fits 24 KB, else the whole 128-thread CTA:
 //   1. 3 n threads per primitive quartet (one per root and Cartesian axis)
 //      take the root and weight from the 7-root table and run the 2D vertical
 //      recurrence g[e][f], e <= la+lb, f <= lc+ld (prefactor and weight folded
@@ -35,6 +37,7 @@ struct FShape {
     int e1, f1;          // VRR extents la+lb+1, lc+ld+1
     int nab2, ncd2;      // 2D index extents (la+1)(lb+1), (lc+1)(ld+1)
     int npq;             // primitive quartets per round
+    int group_doubles;   // shared memory of one group (doubles, 16-byte multiple)
 };
 
 namespace {
@@ -94,151 +97,204 @@ __device__ __forceinline__ void rys7_root(int n, int r, double T, double thr, bo
 
 }  // namespace
 
-__global__ void __launch_bounds__(FCLASS_THREADS) fclass_kernel(ClassArgs a, const double *__restrict__ tab7,
-                                                                FShape s) {
-    if ((int)blockIdx.x >= a.ntasks) return;
-    extern __shared__ __align__(16) double fsm[];
-    const int tid = threadIdx.x;
-    const int n = s.nroot, nrx = 3 * n;
-    const int gsz = s.e1 * s.f1;          // one VRR table
-    const int Gsz = s.nab2 * s.ncd2;      // one 2D-integral table
-    double *acc = fsm;                          // [ncomp]
-    double *g = acc + s.ncomp;                  // [npq][3n][e1*f1]
-    double *G = g + (size_t)s.npq * nrx * gsz;  // [npq][3n][nab2*ncd2]
-    // component -> 2D index per axis: AB part (a*(lb+1)+b), CD part (c*(ld+1)+d)
-    unsigned char *gab = reinterpret_cast<unsigned char *>(G + (size_t)s.npq * nrx * Gsz);  // [3][na*nb]
-    const int nab = s.ncomp / s.ncd;
-    unsigned char *gcd = gab + 3 * nab;  // [3][ncd]
-    for (int i = tid; i < nab; i += FCLASS_THREADS) {
+// A group of NT threads evaluates one quartet at a time: a whole CTA (NT = 128)
+// for the classes with large blocks, one warp (NT = 32) for the others, four
+// warps of a CTA then working on four tasks with their own shared memory and
+// warp barriers only.
+template <int NT>
+__device__ __forceinline__ int group_rank() { return NT == 32 ? (int)(threadIdx.x & 31) : (int)threadIdx.x; }
+template <int NT>
+__device__ __forceinline__ void group_sync() {
+    if constexpr (NT == 32) __syncwarp();
+    else __syncthreads();
+}
+
+// Shared-memory layout of one group: the quartet's block, the VRR tables and
+// the 2D-integral tables of a round, and per component the 2D index on each axis.
+struct FSmem {
+    double *acc;         // [ncomp]
+    double *g;           // [npq][3n][e1*f1]
+    double *G;           // [npq][3n][nab2*ncd2]
+    unsigned char *gab;  // [3][na*nb]: a*(lb+1)+b per axis
+    unsigned char *gcd;  // [3][ncd]: c*(ld+1)+d per axis
+    int nab;
+};
+
+// Carves the layout, fills the index tables and zeroes the block (the caller
+// synchronises the group before use).
+template <int NT>
+__device__ __forceinline__ FSmem fsmem_setup(const FShape &s, double *fsm) {
+    FSmem m;
+    const int tid = group_rank<NT>(), nrx = 3 * s.nroot;
+    m.acc = fsm;
+    m.g = m.acc + s.ncomp;
+    m.G = m.g + (size_t)s.npq * nrx * s.e1 * s.f1;
+    m.gab = reinterpret_cast<unsigned char *>(m.G + (size_t)s.npq * nrx * s.nab2 * s.ncd2);
+    m.nab = s.ncomp / s.ncd;
+    m.gcd = m.gab + 3 * m.nab;
+    for (int i = tid; i < m.nab; i += NT) {
         int ax, ay, az, bx, by, bz;
         cart3(s.la, i / s.nb, ax, ay, az);
         cart3(s.lb, i % s.nb, bx, by, bz);
-        gab[i] = (unsigned char)(ax * (s.lb + 1) + bx);
-        gab[nab + i] = (unsigned char)(ay * (s.lb + 1) + by);
-        gab[2 * nab + i] = (unsigned char)(az * (s.lb + 1) + bz);
+        m.gab[i] = (unsigned char)(ax * (s.lb + 1) + bx);
+        m.gab[m.nab + i] = (unsigned char)(ay * (s.lb + 1) + by);
+        m.gab[2 * m.nab + i] = (unsigned char)(az * (s.lb + 1) + bz);
     }
-    for (int i = tid; i < s.ncd; i += FCLASS_THREADS) {
+    for (int i = tid; i < s.ncd; i += NT) {
         int cx, cy, cz, dx, dy, dz;
         cart3(s.lc, i / s.nd, cx, cy, cz);
         cart3(s.ld, i % s.nd, dx, dy, dz);
-        gcd[i] = (unsigned char)(cx * (s.ld + 1) + dx);
-        gcd[s.ncd + i] = (unsigned char)(cy * (s.ld + 1) + dy);
-        gcd[2 * s.ncd + i] = (unsigned char)(cz * (s.ld + 1) + dz);
+        m.gcd[i] = (unsigned char)(cx * (s.ld + 1) + dx);
+        m.gcd[s.ncd + i] = (unsigned char)(cy * (s.ld + 1) + dy);
+        m.gcd[2 * s.ncd + i] = (unsigned char)(cz * (s.ld + 1) + dz);
     }
-    for (int c = tid; c < s.ncomp; c += FCLASS_THREADS) acc[c] = 0.0;
-    __syncthreads();
+    for (int c = tid; c < s.ncomp; c += NT) m.acc[c] = 0.0;
+    return m;
+}
 
-    const int4 t = a.tasks[blockIdx.x];
+// Adds the contracted block of the quartet (P|Q) (pair P = (A,B), Q = (C,D))
+// to m.acc: every thread keeps its own components c = rank + k * NT.  Called
+// by the whole group; every round of primitive quartets ends with a group
+// barrier, so the tables may be reused on return.
+template <int NT>
+__device__ __forceinline__ void fquartet_block(const FShape &s, const FSmem &m, const DevBasis &b, int P, int Q,
+                                               double thr, bool strict, const double *__restrict__ tab7) {
+    const int tid = group_rank<NT>();
+    const int n = s.nroot, nrx = 3 * n;
+    const int gsz = s.e1 * s.f1;      // one VRR table
+    const int Gsz = s.nab2 * s.ncd2;  // one 2D-integral table
+    double *g = m.g, *G = m.G;
+    const int nab = m.nab;
+    const unsigned char *gab = m.gab, *gcd = m.gcd;
+    const int2 sab = b.pair_shell[P], scd = b.pair_shell[Q];
+    const double4 A = b.shell_xyz[sab.x], B = b.shell_xyz[sab.y];
+    const double4 C = b.shell_xyz[scd.x], D = b.shell_xyz[scd.y];
+    const int p0 = b.pair_prim0[P], np = b.pair_nprim[P];
+    const int q0 = b.pair_prim0[Q], nq = b.pair_nprim[Q];
+    const double AB[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+    const double CD[3] = {C.x - D.x, C.y - D.y, C.z - D.z};
+    const int npq_total = np * nq;
+    for (int pq0 = 0; pq0 < npq_total; pq0 += s.npq) {
+        // 1. roots and the vertical recurrence, one thread per (slot, root, axis)
+        if (tid < s.npq * nrx) {
+            const int slot = tid / nrx, rx = tid - slot * nrx;
+            const int r = rx / 3, x = rx - 3 * r;
+            const int pq = pq0 + slot;
+            double *gs = g + (size_t)(slot * nrx + rx) * gsz;
+            if (pq < npq_total) {
+                const int ip = pq / nq, iq = pq - ip * nq;
+                const double4 Pp = b.prim_P[p0 + ip], Qp = b.prim_P[q0 + iq];
+                const double2 Xp = b.prim_X[p0 + ip], Xq = b.prim_X[q0 + iq];
+                const double p = Pp.w, q = Qp.w, ipq = 1.0 / (p + q);
+                const double dx = Pp.x - Qp.x, dy = Pp.y - Qp.y, dz = Pp.z - Qp.z;
+                const double T = p * q * ipq * (dx * dx + dy * dy + dz * dz);
+                double u, w;
+                rys7_root(n, r, T, thr, strict, tab7, u, w);
+                const double B00 = 0.5 * u * ipq;
+                const double B10 = 0.5 / p * (1.0 - q * u * ipq);
+                const double B01 = 0.5 / q * (1.0 - p * u * ipq);
+                const double PA = x == 0 ? Pp.x - A.x : (x == 1 ? Pp.y - A.y : Pp.z - A.z);
+                const double QC = x == 0 ? Qp.x - C.x : (x == 1 ? Qp.y - C.y : Qp.z - C.z);
+                const double PQ = x == 0 ? dx : (x == 1 ? dy : dz);
+                const double C00 = PA - q * u * ipq * PQ;
+                const double Cp00 = QC + p * u * ipq * PQ;
+                const double g00 = x == 0 ? Xp.x * Xq.x * sqrt(ipq) * w : 1.0;
+                const int e1 = s.e1, f1 = s.f1;
+                gs[0] = g00;
+                for (int e = 0; e + 1 < e1; e++) {
+                    double v = C00 * gs[e * f1];
+                    if (e > 0) v += (double)e * B10 * gs[(e - 1) * f1];
+                    gs[(e + 1) * f1] = v;
+                }
+                for (int f = 0; f + 1 < f1; f++)
+                    for (int e = 0; e < e1; e++) {
+                        double v = Cp00 * gs[e * f1 + f];
+                        if (f > 0) v += (double)f * B01 * gs[e * f1 + f - 1];
+                        if (e > 0) v += (double)e * B00 * gs[(e - 1) * f1 + f];
+                        gs[e * f1 + f + 1] = v;
+                    }
+            } else {
+                for (int i = 0; i < gsz; i++) gs[i] = 0.0;  // empty slot contributes nothing
+            }
+        }
+        group_sync<NT>();
+        // 2. transfer to the 2D integrals of every (slot, root, axis)
+        const int nG = s.npq * nrx * Gsz;
+        for (int idx = tid; idx < nG; idx += NT) {
+            const int tab_i = idx / Gsz, rem = idx - tab_i * Gsz;
+            const int x = tab_i % 3;
+            const int iab = rem / s.ncd2, icd = rem - iab * s.ncd2;
+            const int ia = iab / (s.lb + 1), ib = iab - ia * (s.lb + 1);
+            const int ic = icd / (s.ld + 1), id = icd - ic * (s.ld + 1);
+            const double ab = AB[x], cd = CD[x];
+            const double *gs = g + (size_t)tab_i * gsz;
+            // i, k from the top: weights C(ib,i) AB^(ib-i) and C(id,k) CD^(id-k),
+            // the binomial updated as C(n,m-1) = C(n,m) m / (n-m+1)
+            double sum = 0.0, wb = 1.0;
+            for (int i = ib; i >= 0; i--) {
+                double inner = 0.0, wd = 1.0;
+                for (int k = id; k >= 0; k--) {
+                    inner = fma(wd, gs[(ia + i) * s.f1 + ic + k], inner);
+                    wd *= cd * (double)k / (double)(id - k + 1);
+                }
+                sum = fma(wb, inner, sum);
+                wb *= ab * (double)i / (double)(ib - i + 1);
+            }
+            G[idx] = sum;
+        }
+        group_sync<NT>();
+        // 3. assembly: every thread its own components
+        for (int c = tid; c < s.ncomp; c += NT) {
+            const int iab = c / s.ncd, icd = c - iab * s.ncd;
+            const int ix = gab[iab] * s.ncd2 + gcd[icd];
+            const int iy = gab[nab + iab] * s.ncd2 + gcd[s.ncd + icd];
+            const int iz = gab[2 * nab + iab] * s.ncd2 + gcd[2 * s.ncd + icd];
+            double v = 0.0;
+            const int ntab = s.npq * n;
+            for (int tr = 0; tr < ntab; tr++) {
+                const double *Gt = G + (size_t)tr * 3 * Gsz;
+                v = fma(Gt[ix] * Gt[Gsz + iy], Gt[2 * Gsz + iz], v);
+            }
+            m.acc[c] += v;
+        }
+        group_sync<NT>();
+    }
+}
+
+// NT = 128: one task per CTA; NT = 32: one task per warp (four per CTA).
+template <int NT>
+__global__ void __launch_bounds__(FCLASS_THREADS) fclass_kernel(ClassArgs a, const double *__restrict__ tab7,
+                                                                FShape s) {
+    constexpr int GROUPS = FCLASS_THREADS / NT;
+    const int grp = NT == 32 ? (int)(threadIdx.x >> 5) : 0;
+    const int task = (int)blockIdx.x * GROUPS + grp;
+    if (task >= a.ntasks) return;  // the whole group (only warp barriers follow in warp mode)
+    extern __shared__ __align__(16) double fsm[];
+    const int tid = group_rank<NT>();
+    const FSmem m = fsmem_setup<NT>(s, fsm + (size_t)grp * s.group_doubles);
+    double *acc = m.acc;
+    group_sync<NT>();
+
+    const int4 t = a.tasks[task];
     const DevBasis &b = a.b;
     const int P = a.bra_ids[t.x];
     const int2 sab = b.pair_shell[P];
-    const double4 A = b.shell_xyz[sab.x], B = b.shell_xyz[sab.y];
     const int bfA = b.shell_bf0[sab.x], bfB = b.shell_bf0[sab.y];
-    const int p0 = b.pair_prim0[P], np = b.pair_nprim[P];
-    const double AB[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
     const unsigned nbf = (unsigned)a.nbf;
     const double *Dm = a.Dm, *Dk = a.Dm + a.k_offset;
 
     for (int qi = 0; qi < t.z; qi++) {
         const int j = t.y + qi;
-        if (a.rs.nsize > 1 && !quartet_owned(a, t.x, j)) continue;  // uniform over the CTA
+        if (a.rs.nsize > 1 && !quartet_owned(a, t.x, j)) continue;  // uniform over the group
         const int Q = a.ket_ids[j];
         const int2 scd = b.pair_shell[Q];
-        const double4 C = b.shell_xyz[scd.x], D = b.shell_xyz[scd.y];
         const int bfC = b.shell_bf0[scd.x], bfD = b.shell_bf0[scd.y];
-        const int q0 = b.pair_prim0[Q], nq = b.pair_nprim[Q];
-        const double CD[3] = {C.x - D.x, C.y - D.y, C.z - D.z};
-        const int npq_total = np * nq;
-        for (int pq0 = 0; pq0 < npq_total; pq0 += s.npq) {
-            // 1. roots and the vertical recurrence, one thread per (slot, root, axis)
-            if (tid < s.npq * nrx) {
-                const int slot = tid / nrx, rx = tid - slot * nrx;
-                const int r = rx / 3, x = rx - 3 * r;
-                const int pq = pq0 + slot;
-                double *gs = g + (size_t)(slot * nrx + rx) * gsz;
-                if (pq < npq_total) {
-                    const int ip = pq / nq, iq = pq - ip * nq;
-                    const double4 Pp = b.prim_P[p0 + ip], Qp = b.prim_P[q0 + iq];
-                    const double2 Xp = b.prim_X[p0 + ip], Xq = b.prim_X[q0 + iq];
-                    const double p = Pp.w, q = Qp.w, ipq = 1.0 / (p + q);
-                    const double dx = Pp.x - Qp.x, dy = Pp.y - Qp.y, dz = Pp.z - Qp.z;
-                    const double T = p * q * ipq * (dx * dx + dy * dy + dz * dz);
-                    double u, w;
-                    rys7_root(n, r, T, a.thr, a.strict, tab7, u, w);
-                    const double B00 = 0.5 * u * ipq;
-                    const double B10 = 0.5 / p * (1.0 - q * u * ipq);
-                    const double B01 = 0.5 / q * (1.0 - p * u * ipq);
-                    const double PA = x == 0 ? Pp.x - A.x : (x == 1 ? Pp.y - A.y : Pp.z - A.z);
-                    const double QC = x == 0 ? Qp.x - C.x : (x == 1 ? Qp.y - C.y : Qp.z - C.z);
-                    const double PQ = x == 0 ? dx : (x == 1 ? dy : dz);
-                    const double C00 = PA - q * u * ipq * PQ;
-                    const double Cp00 = QC + p * u * ipq * PQ;
-                    const double g00 = x == 0 ? Xp.x * Xq.x * sqrt(ipq) * w : 1.0;
-                    const int e1 = s.e1, f1 = s.f1;
-                    gs[0] = g00;
-                    for (int e = 0; e + 1 < e1; e++) {
-                        double v = C00 * gs[e * f1];
-                        if (e > 0) v += (double)e * B10 * gs[(e - 1) * f1];
-                        gs[(e + 1) * f1] = v;
-                    }
-                    for (int f = 0; f + 1 < f1; f++)
-                        for (int e = 0; e < e1; e++) {
-                            double v = Cp00 * gs[e * f1 + f];
-                            if (f > 0) v += (double)f * B01 * gs[e * f1 + f - 1];
-                            if (e > 0) v += (double)e * B00 * gs[(e - 1) * f1 + f];
-                            gs[e * f1 + f + 1] = v;
-                        }
-                } else {
-                    for (int i = 0; i < gsz; i++) gs[i] = 0.0;  // empty slot contributes nothing
-                }
-            }
-            __syncthreads();
-            // 2. transfer to the 2D integrals of every (slot, root, axis)
-            const int nG = s.npq * nrx * Gsz;
-            for (int idx = tid; idx < nG; idx += FCLASS_THREADS) {
-                const int tab_i = idx / Gsz, rem = idx - tab_i * Gsz;
-                const int x = tab_i % 3;
-                const int iab = rem / s.ncd2, icd = rem - iab * s.ncd2;
-                const int ia = iab / (s.lb + 1), ib = iab - ia * (s.lb + 1);
-                const int ic = icd / (s.ld + 1), id = icd - ic * (s.ld + 1);
-                const double ab = AB[x], cd = CD[x];
-                const double *gs = g + (size_t)tab_i * gsz;
-                // i, k from the top: weights C(ib,i) AB^(ib-i) and C(id,k) CD^(id-k),
-                // the binomial updated as C(n,m-1) = C(n,m) m / (n-m+1)
-                double sum = 0.0, wb = 1.0;
-                for (int i = ib; i >= 0; i--) {
-                    double inner = 0.0, wd = 1.0;
-                    for (int k = id; k >= 0; k--) {
-                        inner = fma(wd, gs[(ia + i) * s.f1 + ic + k], inner);
-                        wd *= cd * (double)k / (double)(id - k + 1);
-                    }
-                    sum = fma(wb, inner, sum);
-                    wb *= ab * (double)i / (double)(ib - i + 1);
-                }
-                G[idx] = sum;
-            }
-            __syncthreads();
-            // 3. assembly: every thread its own components
-            for (int c = tid; c < s.ncomp; c += FCLASS_THREADS) {
-                const int iab = c / s.ncd, icd = c - iab * s.ncd;
-                const int ix = gab[iab] * s.ncd2 + gcd[icd];
-                const int iy = gab[nab + iab] * s.ncd2 + gcd[s.ncd + icd];
-                const int iz = gab[2 * nab + iab] * s.ncd2 + gcd[2 * s.ncd + icd];
-                double v = 0.0;
-                const int ntab = s.npq * n;
-                for (int tr = 0; tr < ntab; tr++) {
-                    const double *Gt = G + (size_t)tr * 3 * Gsz;
-                    v = fma(Gt[ix] * Gt[Gsz + iy], Gt[2 * Gsz + iz], v);
-                }
-                acc[c] += v;
-            }
-            __syncthreads();
-        }
+        fquartet_block<NT>(s, m, b, P, Q, a.thr, a.strict, tab7);
         // digestion of this thread's components (the same components it
         // accumulated: no barrier needed before the reads)
         const bool iandj = sab.x == sab.y, kandl = scd.x == scd.y;
         const bool same = sab.x == scd.x && sab.y == scd.y;
-        for (int c = tid; c < s.ncomp; c += FCLASS_THREADS) {
+        for (int c = tid; c < s.ncomp; c += NT) {
             double val = acc[c];
             acc[c] = 0.0;
             const int iab = c / s.ncd, icd = c - iab * s.ncd;
@@ -279,12 +335,14 @@ static size_t fclass_smem(const FShape &s) {
            3 * (nab + s.ncd) + 16;
 }
 
-static FShape fshape_of(const KernelDesc &kd) {
+// nt: threads of a group; shared-memory budget 96 KB per CTA group (two CTAs
+// per SM) or 24 KB per warp group
+static FShape fshape_make(int la, int lb, int lc, int ld, int nt) {
     FShape s;
-    s.la = kd.la;
-    s.lb = kd.lb;
-    s.lc = kd.lc;
-    s.ld = kd.ld;
+    s.la = la;
+    s.lb = lb;
+    s.lc = lc;
+    s.ld = ld;
     s.nroot = (s.la + s.lb + s.lc + s.ld) / 2 + 1;
     const int na = (s.la + 1) * (s.la + 2) / 2;
     s.nb = (s.lb + 1) * (s.lb + 2) / 2;
@@ -296,24 +354,73 @@ static FShape fshape_of(const KernelDesc &kd) {
     s.f1 = s.lc + s.ld + 1;
     s.nab2 = (s.la + 1) * (s.lb + 1);
     s.ncd2 = (s.lc + 1) * (s.ld + 1);
-    // as many primitive quartets per round as the threads of step 1 and a
-    // 96 KB shared-memory budget allow (two CTAs per SM)
-    s.npq = FCLASS_THREADS / (3 * s.nroot);
-    while (s.npq > 1) {
-        if (fclass_smem(s) <= 96 * 1024) break;
-        s.npq--;
-    }
+    // as many primitive quartets per round as the group's threads in step 1
+    // and the shared-memory budget allow
+    const size_t budget = nt == 32 ? 24 * 1024 : 96 * 1024;
+    s.npq = nt / (3 * s.nroot);
+    if (s.npq < 1) s.npq = 1;
+    while (s.npq > 1 && fclass_smem(s) > budget) s.npq--;
+    s.group_doubles = (int)((fclass_smem(s) + 15) / 16 * 2);
     return s;
 }
 
-size_t fclass_smem_bytes(int k) { return fclass_smem(fshape_of(KDESC[k])); }
+// warp groups where one warp's working set fits 24 KB, else CTA groups
+static bool fclass_warp_mode(const KernelDesc &kd) {
+    return fclass_smem(fshape_make(kd.la, kd.lb, kd.lc, kd.ld, 32)) <= 24 * 1024;
+}
+
+// Schwarz values of f pairs: one CTA per pair P of one class, the (P|P) block
+// as in the class kernel, then sqrt(max over components |(ab|ab)|) of the
+// normalised integrals into out[P] (global pair index).
+__global__ void __launch_bounds__(FCLASS_THREADS) fschwarz_kernel(DevBasis b, int pair_off, int npairs,
+                                                                  const double *__restrict__ tab7, FShape s,
+                                                                  double *out) {
+    if ((int)blockIdx.x >= npairs) return;
+    extern __shared__ __align__(16) double fsm[];
+    __shared__ double wmax[FCLASS_THREADS / 32];
+    const FSmem m = fsmem_setup<FCLASS_THREADS>(s, fsm);
+    __syncthreads();
+    const int P = pair_off + (int)blockIdx.x;
+    fquartet_block<FCLASS_THREADS>(s, m, b, P, P, RYS7_TMAX, false, tab7);
+    // diagonal components (a b|a b): icd == iab
+    double mx = 0.0;
+    for (int iab = threadIdx.x; iab < m.nab; iab += FCLASS_THREADS) {
+        const int ia = iab / s.nb, ib = iab - ia * s.nb;
+        const double nrm = cnorm(s.la, ia) * cnorm(s.lb, ib);
+        mx = fmax(mx, fabs(m.acc[iab * s.ncd + iab]) * nrm * nrm);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < FCLASS_THREADS / 32; w++) mx = fmax(mx, wmax[w]);
+        out[P] = sqrt(mx);
+    }
+}
+
+cudaError_t launch_fschwarz(int pair_class, int npairs, int pair_off, const DevBasis &b, const double *rys_tab7,
+                            double *out, cudaStream_t stream) {
+    if (npairs <= 0) return cudaSuccess;
+    if (pair_class < NPC_SPD || pair_class >= NPC || !rys_tab7) return cudaErrorInvalidValue;
+    const int lf = pair_class - NPC_SPD;  // sf, pf, df, ff: the lower-L shell s, p, d, f
+    const FShape s = fshape_make(3, lf, 3, lf, FCLASS_THREADS);
+    const size_t smem = fclass_smem(s);
+    cudaError_t e = cudaFuncSetAttribute(fschwarz_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    fschwarz_kernel<<<(unsigned)npairs, FCLASS_THREADS, smem, stream>>>(b, pair_off, npairs, rys_tab7, s, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_fclass(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs, int nbf) {
     if (plan.ntasks <= 0) return cudaSuccess;
     const KernelDesc &kd = KDESC[k];
-    const FShape s = fshape_of(kd);
-    const size_t smem = fclass_smem(s);
-    cudaError_t e = cudaFuncSetAttribute(fclass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const bool warp = fclass_warp_mode(kd);
+    const int nt = warp ? 32 : FCLASS_THREADS, groups = FCLASS_THREADS / nt;
+    const FShape s = fshape_make(kd.la, kd.lb, kd.lc, kd.ld, nt);
+    const size_t smem = (size_t)groups * s.group_doubles * sizeof(double);
+    cudaError_t e = warp ? cudaFuncSetAttribute(fclass_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                         : cudaFuncSetAttribute(fclass_kernel<FCLASS_THREADS>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     ClassArgs a{};
     a.b = ctx.basis;
@@ -334,7 +441,9 @@ cudaError_t launch_fclass(int k, const LaunchCtx &ctx, const DevPlan &plan, cons
     a.swapped = plan.swapped;
     a.rs = rs;
     a.k_offset = ctx.k_offset;
-    fclass_kernel<<<(unsigned)plan.ntasks, FCLASS_THREADS, smem, ctx.stream>>>(a, ctx.rys_tab7, s);
+    const unsigned grid = (unsigned)((plan.ntasks + groups - 1) / groups);
+    if (warp) fclass_kernel<32><<<grid, FCLASS_THREADS, smem, ctx.stream>>>(a, ctx.rys_tab7, s);
+    else fclass_kernel<FCLASS_THREADS><<<grid, FCLASS_THREADS, smem, ctx.stream>>>(a, ctx.rys_tab7, s);
     return cudaGetLastError();
 }
 

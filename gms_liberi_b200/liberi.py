@@ -99,7 +99,7 @@ def lib():
         L.liberi_c_get_option.argtypes = [H, ctypes.c_char_p, _F64P]
         L.liberi_c_schwarz.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                        _I32P, _I32P, _I32P, _I32P, _I32P,
-                                       _F64P, _F64P, _F64P, _F64P, _F64P, _F64P]
+                                       _F64P, _F64P, _F64P, _F64P, _F64P, _F64P, _F64P]
         L.liberi_c_get_stats.argtypes = [H, ctypes.POINTER(Stats)]
         L.liberi_c_quartet_fingerprint.argtypes = [H, ctypes.POINTER(ctypes.c_uint64)]
         L.liberi_c_fock_build_uhf.argtypes = [H, _F64P, _F64P, _F64P, _F64P, ctypes.c_int32]
@@ -120,7 +120,9 @@ def lib():
         L.liberi_c_quartet_fingerprint_all.argtypes = [H, ctypes.POINTER(ctypes.c_uint64)]
         L.liberi_c_rys7_eval.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                          _F64P, _F64P]
-        L.liberi_c_schwarz_noalloc.argtypes = L.liberi_c_schwarz.argtypes
+        L.liberi_c_schwarz_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                               _I32P, _I32P, _I32P, _I32P, _I32P,
+                                               _F64P, _F64P, _F64P, _F64P, _F64P, _F64P]
         L.liberi_c_rys_eval.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                         _F64P, _F64P]
         L.liberi_c_microbench.argtypes = [ctypes.c_int32, _F64P]
@@ -530,7 +532,7 @@ def schwarz(basis):
     out = np.zeros(nsh * (nsh + 1) // 2)
     _check(lib().liberi_c_schwarz(nsh, natoms, nbf, mx, _i32(ang, k), _i32(cn, k), _i32(sl, k),
                                   _i32(an, k), _i32(al, k), _f64(ex, k), _f64(cs, k), _f64(cp, k),
-                                  _f64(cd, k), _f64(xyz, k), out.ctypes.data_as(_F64P)))
+                                  _f64(cd, k), _f64(cf, k), _f64(xyz, k), out.ctypes.data_as(_F64P)))
     return out
 
 

@@ -161,16 +161,17 @@ int liberi_c_fock_build_uhf_device(liberi_handle handle, const double *d_density
 
 /* Schwarz table generator: schwrz_out[ia(max)+min] = sqrt(max_components
  * |(ab|ab)|) over shell pairs, computed on the device (GAMESS supplies this
- * table to the reference, liberi_interface.F90:128-129).  s/p/d shells; a
- * basis with f shells is rejected with LIBERI_E_UNSUPPORTED. */
+ * table to the reference, liberi_interface.F90:128-129).  s/p/d/f shells;
+ * contr_coef_f may be NULL for bases without f shells. */
 int liberi_c_schwarz(int32_t nsh, int32_t natoms, int32_t num_bas, int32_t mxgtot,
                      const int32_t *ang_mom, const int32_t *contr_num, const int32_t *sh_loc,
                      const int32_t *atom_num, const int32_t *atom_loc, const double *exponents,
-                     const double *contr_coef_s, const double *contr_coef_p,
-                     const double *contr_coef_d, const double *coords, double *schwrz_out);
+                     const double *contr_coef_s, const double *contr_coef_p, const double *contr_coef_d,
+                     const double *contr_coef_f, const double *coords, double *schwrz_out);
 
 /* Schwarz table without device allocation.  No counterpart in the reference:
- * same inputs and output as liberi_c_schwarz, for callers that cannot call
+ * the inputs and output of liberi_c_schwarz for s/p/d bases (no f
+ * coefficients; f shells are rejected), for callers that cannot call
  * cudaMalloc (their device memory is already committed to their own pool, or
  * their allocation policy forbids ad-hoc cudaMalloc/cudaFree).  Its device
  * scratch is one static array of LIBERI_NOALLOC_SCRATCH_BYTES that every GPU

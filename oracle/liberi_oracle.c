@@ -688,6 +688,17 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
                            const pairs_t *pb, int64_t eb_, const pairs_t *pk, int64_t ek_,
                            const kdesc_t *kd, real_t *out) {
     const oracle_basis *b = c->b;
+    /* out keeps the (A B|C D) order of the call; the evaluation puts the
+     * higher-L shell of each pair first, as the reference's Rys kernels order
+     * their pairs (int3011_rysgen.F90: ish the f shell of an sf pair): the
+     * transfer relation then moves angular momentum onto the lower-L shell,
+     * which stays accurate when a tight high-L shell meets a distant diffuse
+     * partner (the other way round loses digits to cancellation) */
+    const int la0 = b->ang_mom[A] - 1, lb0 = b->ang_mom[B] - 1, lc0 = b->ang_mom[C] - 1, ld0 = b->ang_mom[D] - 1;
+    const int nb0 = NCART[lb0], nc0 = NCART[lc0], nd0 = NCART[ld0];
+    const int sab = lb0 > la0, scd = ld0 > lc0;
+    if (sab) { const int t = A; A = B; B = t; }
+    if (scd) { const int t = C; C = D; D = t; }
     int la = b->ang_mom[A] - 1, lb = b->ang_mom[B] - 1, lc = b->ang_mom[C] - 1, ld = b->ang_mom[D] - 1;
     int na = NCART[la], nb = NCART[lb], nc = NCART[lc], nd = NCART[ld];
     int n = (la + lb + lc + ld) / 2 + 1;
@@ -703,13 +714,13 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
     int64_t nprim = 0;
     const double twopi52 = 2.0 * PI_D * PI_D * sqrt(PI_D);
     for (int64_t kq = pk->loc[ek_]; kq < pk->loc[ek_ + 1]; kq++) {
-        real_t gc = pk->ea[kq], gd = pk->eb[kq], q = gc + gd;
+        real_t gc = scd ? pk->eb[kq] : pk->ea[kq], gd = scd ? pk->ea[kq] : pk->eb[kq], q = gc + gd;
         real_t Q[3];
         for (int x = 0; x < 3; x++) Q[x] = (gc * Cr[x] + gd * Dr[x]) / q;
         real_t ecd = exp(-gc * gd / q * rcd2);
         for (int64_t bq = pb->loc[eb_]; bq < pb->loc[eb_ + 1]; bq++) {
             if (kd->skip && (pb->ismlp[bq] + pk->ismlp[kq] >= 2)) continue;
-            real_t ga = pb->ea[bq], gb = pb->eb[bq], p = ga + gb;
+            real_t ga = sab ? pb->eb[bq] : pb->ea[bq], gb = sab ? pb->ea[bq] : pb->eb[bq], p = ga + gb;
             real_t P[3], PQ2 = 0.0;
             for (int x = 0; x < 3; x++) {
                 P[x] = (ga * Ar[x] + gb * Br[x]) / p;
@@ -777,18 +788,20 @@ static int64_t eri_quartet(const ctx_t *c, int A, int B, int C, int D,
                 real_t acc = 0.0;
                 for (int r = 0; r < n; r++)
                     acc += w[r] * I2[r][0][ax][bx][cx][dx] * I2[r][1][ay][by][cy][dy] * I2[r][2][az][bz][cz][dz];
-                out[((ia * nb + ib) * nc + ic) * nd + id] += pref * acc;
+                const int i0 = sab ? ib : ia, j0 = sab ? ia : ib, k0 = scd ? id : ic, l0 = scd ? ic : id;
+                out[((i0 * nb0 + j0) * nc0 + k0) * nd0 + l0] += pref * acc;
             }
         }
     }
     ORACLE_MARK();  /* op-counting build: end of the primitive-quartet work */
-    /* component normalisation (sqrt3 on xy,xz,yz of d; sqrt5 / sqrt15 on f) */
-    for (int ia = 0; ia < na; ia++)
-    for (int ib = 0; ib < nb; ib++)
-    for (int ic = 0; ic < nc; ic++)
-    for (int id = 0; id < nd; id++)
-        out[((ia * nb + ib) * nc + ic) * nd + id] *=
-            CNORM[la][ia] * CNORM[lb][ib] * CNORM[lc][ic] * CNORM[ld][id];
+    /* component normalisation (sqrt3 on xy,xz,yz of d; sqrt5 / sqrt15 on f),
+     * in the call's order */
+    for (int ia = 0; ia < NCART[la0]; ia++)
+    for (int ib = 0; ib < nb0; ib++)
+    for (int ic = 0; ic < nc0; ic++)
+    for (int id = 0; id < nd0; id++)
+        out[((ia * nb0 + ib) * nc0 + ic) * nd0 + id] *=
+            CNORM[la0][ia] * CNORM[lb0][ib] * CNORM[lc0][ic] * CNORM[ld0][id];
     return nprim;
 }
 

@@ -28,9 +28,11 @@ def test_f_fixture_is_consistent():
 
 def test_setup_bytes_plan_the_f_classes():
     # host-only dry run of setup: the f pair classes and the 34 f class plans
-    # add device bytes; the Schwarz generator still covers s/p/d only
     d = load_kat("h2o_ccpvtz")
-    assert liberi.setup_bytes(d, 5e-11) > 0
-    with pytest.raises(liberi.LiberiError) as err:
-        liberi.schwarz(d)  # rejected on the host, before any device call
-    assert err.value.code == -6 and "f shell" in str(err.value)
+    full = liberi.setup_bytes(d, 5e-11)
+    e = dict(d)
+    e["ang_mom"] = [l if l != 4 else 3 for l in d["ang_mom"]]  # the f shell as a d shell
+    e["coef_d"] = d["coef_d"] + d["coef_f"]
+    e["num_bas"] = d["num_bas"] - 4
+    e["atom_loc"] = [a if a <= 26 else a - 4 for a in d["atom_loc"]]
+    assert full > liberi.setup_bytes(e, 5e-11) > 0

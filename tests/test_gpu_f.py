@@ -135,3 +135,13 @@ def test_f_mixed_precision_energy(f_mols):
     F, st = gpu_fock(b, D, schwarz_cut=1e-10, precision=1, fp32_cut=1e-5)
     assert st["fp32_quartets"][:21].sum() > 0 and st["fp32_quartets"][21:].sum() == 0
     assert abs(energy(D, F) - energy(D, Fo)) <= 1e-6
+
+
+@pytest.mark.parametrize("name", ["triatomic", "cluster_14"])
+def test_f_schwarz_generator_matches_oracle(f_mols, name):
+    # the device generator covers f pairs with the f classes' evaluation
+    b, _ = f_mols[name]
+    sg, so = liberi.schwarz(b), oracle.schwarz(b)
+    err = np.abs(sg - so) / (1e-14 + 1e-10 * np.abs(so))
+    i = int(np.argmax(err))
+    assert err[i] <= 1.0, (i, sg[i], so[i])

@@ -118,3 +118,25 @@ def test_oracle_f_rank_partials_sum_to_full(nsize):
     full = oracle.fock_build(b, D, schwarz_cut=1e-10)
     parts = sum(oracle.fock_build(b, D, schwarz_cut=1e-10, my_rank=r, num_procs=nsize) for r in range(nsize))
     assert np.abs(parts - full).max() < 1e-12
+
+
+def test_oracle_tight_f_beside_distant_diffuse_shells():
+    # a tight f shell (exponent 588) 6.2 bohr from a diffuse p shell: evaluated
+    # from the p shell, the transfer relation cancels to a few digits; the
+    # oracle orients every pair with its higher-L shell first, as the
+    # reference's Rys kernels do, and matches the independent integrals
+    shells = {"C": [(3, [587.77], M._contracted(3, [587.77], [1.0])), (0, [1.3], M._contracted(0, [1.3], [1.0]))],
+              "H": [(1, [0.2175], M._contracted(1, [0.2175], [1.0])), (0, [0.4], M._contracted(0, [0.4], [1.0]))]}
+    b = M.build_basis(["C", "H"], np.array([[0.0, 0.0, 0.0], [1.1, -3.9, 4.7]]), lambda s: shells[s])
+    b["schwrz"] = np.full(b["nsh"] * (b["nsh"] + 1) // 2, 1e10)
+    sh = md_eri.shells_of(b)
+    S = oracle.schwarz(b)
+    for i in range(len(sh)):
+        for j in range(i + 1):
+            v = md_eri.shell_quartet(sh[i], sh[j], sh[i], sh[j])
+            m = max(abs(v[a, c, a, c]) for a in range(v.shape[0]) for c in range(v.shape[1]))
+            assert abs(np.sqrt(m) - S[i * (i + 1) // 2 + j]) <= 1e-12 * np.sqrt(m), (i, j)
+    G = md_eri.eri_tensor(b)
+    D = M.density(b["num_bas"], 4, seed=3)
+    F = oracle.fock_build(b, D, schwarz_cut=0.0, eri_cut=0.0)
+    assert np.abs(F - md_eri.fock_from_eri(G, D)).max() <= 1e-12 * max(1.0, np.abs(F).max())
