@@ -27,9 +27,12 @@ _SHAPE_631GD_HEAVY = [("s", 6), ("sp", 3), ("sp", 1), ("d", 1)]
 _SHAPE_631GD_H = [("s", 3), ("s", 1)]
 _SHAPE_STO3G_HEAVY = [("s", 3), ("sp", 3)]
 _SHAPE_STO3G_H = [("s", 3)]
-# f-bearing shapes: a polarised heavy-atom set with one f shell, H with a p
-_SHAPE_F_HEAVY = [("s", 6), ("sp", 3), ("sp", 1), ("d", 1), ("f", 1)]
-_SHAPE_F_H = [("s", 3), ("s", 1), ("p", 1)]
+# f-bearing shapes: a polarised heavy-atom set with one d and one f
+# polarisation shell, H with a p; polarisation exponents ("dpol", "fpol",
+# "ppol") in the range of correlation-consistent sets, [0.3, 3]
+_SHAPE_F_HEAVY = [("s", 6), ("sp", 3), ("sp", 1), ("dpol", 1), ("fpol", 1)]
+_SHAPE_F_H = [("s", 3), ("s", 1), ("ppol", 1)]
+_POL_RANGE = (0.3, 3.0)
 
 
 def _prim_norm(l, a):
@@ -72,7 +75,9 @@ def element_basis(elem, shape, lo, hi, seed=0):
     rng = np.random.default_rng([seed, _ELEM_Z[elem]])
     shells = []
     for kind, K in shape:
-        exps = np.sort(np.exp(rng.uniform(math.log(lo), math.log(hi), K)))[::-1].tolist()
+        elo, ehi = _POL_RANGE if kind.endswith("pol") else (lo, hi)
+        kind = kind[0] if kind.endswith("pol") else kind
+        exps = np.sort(np.exp(rng.uniform(math.log(elo), math.log(ehi), K)))[::-1].tolist()
         if kind == "s":
             shells.append((0, exps, _contracted(0, exps, rng.uniform(0.1, 1.0, K).tolist())))
         elif kind == "sp":
