@@ -29,15 +29,41 @@ namespace liberi {
 
 constexpr int FCLASS_THREADS = 128;
 
-struct FShape {
-    int la, lb, lc, ld;  // engine orientation (la >= lb, lc >= ld)
-    int nroot;
-    int nb, nc, nd;      // Cartesian components of B, C, D
-    int ncd, ncomp;      // nc * nd, na * nb * nc * nd
-    int e1, f1;          // VRR extents la+lb+1, lc+ld+1
-    int nab2, ncd2;      // 2D index extents (la+1)(lb+1), (lc+1)(ld+1)
-    int npq;             // primitive quartets per round
-    int group_doubles;   // shared memory of one group (doubles, 16-byte multiple)
+// Shared-memory bytes of one group of a class: the quartet's block, npq
+// rounds' VRR and 2D-integral tables, the component index tables.
+__host__ __device__ constexpr int fnc(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr size_t fgroup_bytes(int la, int lb, int lc, int ld, int npq) {
+    return sizeof(double) * ((size_t)fnc(la) * fnc(lb) * fnc(lc) * fnc(ld) +
+                             (size_t)npq * 3 * ((la + lb + lc + ld) / 2 + 1) *
+                                 ((la + lb + 1) * (lc + ld + 1) + (la + 1) * (lb + 1) * (lc + 1) * (ld + 1))) +
+           3 * (size_t)(fnc(la) * fnc(lb) + fnc(lc) * fnc(ld)) + 16;
+}
+// One warp per quartet where the working set of one primitive quartet per
+// round fits 24 KB, else the whole CTA.
+__host__ __device__ constexpr bool fwarp_mode(int la, int lb, int lc, int ld) {
+    return fgroup_bytes(la, lb, lc, ld, 1) <= 24 * 1024;
+}
+// Primitive quartets per round: as many as the group's threads take in step 1
+// (3 n each) within 12 KB per warp group (four CTAs of four warps per SM) or
+// 96 KB per CTA group.
+__host__ __device__ constexpr int fnpq(int la, int lb, int lc, int ld, int nt) {
+    int npq = nt / (3 * ((la + lb + lc + ld) / 2 + 1));
+    while (npq > 1 && fgroup_bytes(la, lb, lc, ld, npq) > (nt == 32 ? 12 * 1024 : 96 * 1024)) npq--;
+    return npq < 1 ? 1 : npq;
+}
+
+// Compile-time shape of one class (engine orientation, la >= lb, lc >= ld) for
+// groups of NT threads.
+template <int LA, int LB, int LC, int LD, int NT>
+struct FS {
+    static constexpr int la = LA, lb = LB, lc = LC, ld = LD, nt = NT;
+    static constexpr int nroot = (LA + LB + LC + LD) / 2 + 1;
+    static constexpr int nb = fnc(LB), nc = fnc(LC), nd = fnc(LD);
+    static constexpr int ncd = nc * nd, ncomp = fnc(LA) * nb * ncd;
+    static constexpr int e1 = LA + LB + 1, f1 = LC + LD + 1;              // VRR extents
+    static constexpr int nab2 = (LA + 1) * (LB + 1), ncd2 = (LC + 1) * (LD + 1);  // 2D index extents
+    static constexpr int npq = fnpq(LA, LB, LC, LD, NT);
+    static constexpr int group_doubles = (int)((fgroup_bytes(LA, LB, LC, LD, npq) + 15) / 16 * 2);
 };
 
 namespace {
@@ -122,8 +148,9 @@ struct FSmem {
 
 // Carves the layout, fills the index tables and zeroes the block (the caller
 // synchronises the group before use).
-template <int NT>
-__device__ __forceinline__ FSmem fsmem_setup(const FShape &s, double *fsm) {
+template <typename S>
+__device__ __forceinline__ FSmem fsmem_setup(const S &s, double *fsm) {
+    constexpr int NT = S::nt;
     FSmem m;
     const int tid = group_rank<NT>(), nrx = 3 * s.nroot;
     m.acc = fsm;
@@ -156,9 +183,10 @@ __device__ __forceinline__ FSmem fsmem_setup(const FShape &s, double *fsm) {
 // to m.acc: every thread keeps its own components c = rank + k * NT.  Called
 // by the whole group; every round of primitive quartets ends with a group
 // barrier, so the tables may be reused on return.
-template <int NT>
-__device__ __forceinline__ void fquartet_block(const FShape &s, const FSmem &m, const DevBasis &b, int P, int Q,
+template <typename S>
+__device__ __forceinline__ void fquartet_block(const S &s, const FSmem &m, const DevBasis &b, int P, int Q,
                                                double thr, bool strict, const double *__restrict__ tab7) {
+    constexpr int NT = S::nt;
     const int tid = group_rank<NT>();
     const int n = s.nroot, nrx = 3 * n;
     const int gsz = s.e1 * s.f1;      // one VRR table
@@ -262,16 +290,17 @@ __device__ __forceinline__ void fquartet_block(const FShape &s, const FSmem &m, 
 }
 
 // NT = 128: one task per CTA; NT = 32: one task per warp (four per CTA).
-template <int NT>
-__global__ void __launch_bounds__(FCLASS_THREADS) fclass_kernel(ClassArgs a, const double *__restrict__ tab7,
-                                                                FShape s) {
+template <typename S>
+__global__ void __launch_bounds__(FCLASS_THREADS) fclass_kernel(ClassArgs a, const double *__restrict__ tab7) {
+    constexpr int NT = S::nt;
+    constexpr S s{};
     constexpr int GROUPS = FCLASS_THREADS / NT;
     const int grp = NT == 32 ? (int)(threadIdx.x >> 5) : 0;
     const int task = (int)blockIdx.x * GROUPS + grp;
     if (task >= a.ntasks) return;  // the whole group (only warp barriers follow in warp mode)
     extern __shared__ __align__(16) double fsm[];
     const int tid = group_rank<NT>();
-    const FSmem m = fsmem_setup<NT>(s, fsm + (size_t)grp * s.group_doubles);
+    const FSmem m = fsmem_setup(s, fsm + (size_t)grp * s.group_doubles);
     double *acc = m.acc;
     group_sync<NT>();
 
@@ -289,7 +318,7 @@ __global__ void __launch_bounds__(FCLASS_THREADS) fclass_kernel(ClassArgs a, con
         const int Q = a.ket_ids[j];
         const int2 scd = b.pair_shell[Q];
         const int bfC = b.shell_bf0[scd.x], bfD = b.shell_bf0[scd.y];
-        fquartet_block<NT>(s, m, b, P, Q, a.thr, a.strict, tab7);
+        fquartet_block(s, m, b, P, Q, a.thr, a.strict, tab7);
         // digestion of this thread's components (the same components it
         // accumulated: no barrier needed before the reads)
         const bool iandj = sab.x == sab.y, kandl = scd.x == scd.y;
@@ -328,60 +357,21 @@ __global__ void __launch_bounds__(FCLASS_THREADS) fclass_kernel(ClassArgs a, con
     }
 }
 
-// shared-memory bytes of one CTA of this shape
-static size_t fclass_smem(const FShape &s) {
-    const size_t nab = (size_t)s.ncomp / s.ncd;
-    return sizeof(double) * ((size_t)s.ncomp + (size_t)s.npq * 3 * s.nroot * (s.e1 * s.f1 + s.nab2 * s.ncd2)) +
-           3 * (nab + s.ncd) + 16;
-}
-
-// nt: threads of a group; shared-memory budget 96 KB per CTA group (two CTAs
-// per SM) or 24 KB per warp group
-static FShape fshape_make(int la, int lb, int lc, int ld, int nt) {
-    FShape s;
-    s.la = la;
-    s.lb = lb;
-    s.lc = lc;
-    s.ld = ld;
-    s.nroot = (s.la + s.lb + s.lc + s.ld) / 2 + 1;
-    const int na = (s.la + 1) * (s.la + 2) / 2;
-    s.nb = (s.lb + 1) * (s.lb + 2) / 2;
-    s.nc = (s.lc + 1) * (s.lc + 2) / 2;
-    s.nd = (s.ld + 1) * (s.ld + 2) / 2;
-    s.ncd = s.nc * s.nd;
-    s.ncomp = na * s.nb * s.ncd;
-    s.e1 = s.la + s.lb + 1;
-    s.f1 = s.lc + s.ld + 1;
-    s.nab2 = (s.la + 1) * (s.lb + 1);
-    s.ncd2 = (s.lc + 1) * (s.ld + 1);
-    // as many primitive quartets per round as the group's threads in step 1
-    // and the shared-memory budget allow
-    const size_t budget = nt == 32 ? 24 * 1024 : 96 * 1024;
-    s.npq = nt / (3 * s.nroot);
-    if (s.npq < 1) s.npq = 1;
-    while (s.npq > 1 && fclass_smem(s) > budget) s.npq--;
-    s.group_doubles = (int)((fclass_smem(s) + 15) / 16 * 2);
-    return s;
-}
-
-// warp groups where one warp's working set fits 24 KB, else CTA groups
-static bool fclass_warp_mode(const KernelDesc &kd) {
-    return fclass_smem(fshape_make(kd.la, kd.lb, kd.lc, kd.ld, 32)) <= 24 * 1024;
-}
-
 // Schwarz values of f pairs: one CTA per pair P of one class, the (P|P) block
 // as in the class kernel, then sqrt(max over components |(ab|ab)|) of the
 // normalised integrals into out[P] (global pair index).
+template <typename S>
 __global__ void __launch_bounds__(FCLASS_THREADS) fschwarz_kernel(DevBasis b, int pair_off, int npairs,
-                                                                  const double *__restrict__ tab7, FShape s,
-                                                                  double *out) {
+                                                                  const double *__restrict__ tab7, double *out) {
     if ((int)blockIdx.x >= npairs) return;
+    constexpr S s{};
+    static_assert(S::nt == FCLASS_THREADS, "one pair per CTA");
     extern __shared__ __align__(16) double fsm[];
     __shared__ double wmax[FCLASS_THREADS / 32];
-    const FSmem m = fsmem_setup<FCLASS_THREADS>(s, fsm);
+    const FSmem m = fsmem_setup(s, fsm);
     __syncthreads();
     const int P = pair_off + (int)blockIdx.x;
-    fquartet_block<FCLASS_THREADS>(s, m, b, P, P, RYS7_TMAX, false, tab7);
+    fquartet_block(s, m, b, P, P, RYS7_TMAX, false, tab7);
     // diagonal components (a b|a b): icd == iab
     double mx = 0.0;
     for (int iab = threadIdx.x; iab < m.nab; iab += FCLASS_THREADS) {
@@ -398,30 +388,47 @@ __global__ void __launch_bounds__(FCLASS_THREADS) fschwarz_kernel(DevBasis b, in
     }
 }
 
+template <int LF>
+static cudaError_t fschwarz_t(int npairs, int pair_off, const DevBasis &b, const double *tab7, double *out,
+                              cudaStream_t stream) {
+    using S = FS<3, LF, 3, LF, FCLASS_THREADS>;
+    const size_t smem = (size_t)S::group_doubles * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(fschwarz_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    fschwarz_kernel<S><<<(unsigned)npairs, FCLASS_THREADS, smem, stream>>>(b, pair_off, npairs, tab7, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fschwarz(int pair_class, int npairs, int pair_off, const DevBasis &b, const double *rys_tab7,
                             double *out, cudaStream_t stream) {
     if (npairs <= 0) return cudaSuccess;
-    if (pair_class < NPC_SPD || pair_class >= NPC || !rys_tab7) return cudaErrorInvalidValue;
-    const int lf = pair_class - NPC_SPD;  // sf, pf, df, ff: the lower-L shell s, p, d, f
-    const FShape s = fshape_make(3, lf, 3, lf, FCLASS_THREADS);
-    const size_t smem = fclass_smem(s);
-    cudaError_t e = cudaFuncSetAttribute(fschwarz_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (!rys_tab7) return cudaErrorInvalidValue;
+    switch (pair_class) {  // sf, pf, df, ff: the lower-L shell s, p, d, f
+        case SF: return fschwarz_t<0>(npairs, pair_off, b, rys_tab7, out, stream);
+        case PF: return fschwarz_t<1>(npairs, pair_off, b, rys_tab7, out, stream);
+        case DF: return fschwarz_t<2>(npairs, pair_off, b, rys_tab7, out, stream);
+        case FF: return fschwarz_t<3>(npairs, pair_off, b, rys_tab7, out, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// one class: warp or CTA groups by its shape, one launch over the plan's tasks
+template <int LA, int LB, int LC, int LD>
+static cudaError_t fclass_t(const ClassArgs &a, const double *tab7, cudaStream_t stream) {
+    constexpr bool W = fwarp_mode(LA, LB, LC, LD);
+    using S = FS<LA, LB, LC, LD, W ? 32 : FCLASS_THREADS>;
+    constexpr int groups = FCLASS_THREADS / S::nt;
+    const size_t smem = (size_t)groups * S::group_doubles * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(fclass_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    fschwarz_kernel<<<(unsigned)npairs, FCLASS_THREADS, smem, stream>>>(b, pair_off, npairs, rys_tab7, s, out);
+    const unsigned grid = (unsigned)((a.ntasks + groups - 1) / groups);
+    fclass_kernel<S><<<grid, FCLASS_THREADS, smem, stream>>>(a, tab7);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fclass(int k, const LaunchCtx &ctx, const DevPlan &plan, const RankSplit &rs, int nbf) {
     if (plan.ntasks <= 0) return cudaSuccess;
     const KernelDesc &kd = KDESC[k];
-    const bool warp = fclass_warp_mode(kd);
-    const int nt = warp ? 32 : FCLASS_THREADS, groups = FCLASS_THREADS / nt;
-    const FShape s = fshape_make(kd.la, kd.lb, kd.lc, kd.ld, nt);
-    const size_t smem = (size_t)groups * s.group_doubles * sizeof(double);
-    cudaError_t e = warp ? cudaFuncSetAttribute(fclass_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                         : cudaFuncSetAttribute(fclass_kernel<FCLASS_THREADS>,
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
     ClassArgs a{};
     a.b = ctx.basis;
     a.Dm = ctx.D;
@@ -441,10 +448,22 @@ cudaError_t launch_fclass(int k, const LaunchCtx &ctx, const DevPlan &plan, cons
     a.swapped = plan.swapped;
     a.rs = rs;
     a.k_offset = ctx.k_offset;
-    const unsigned grid = (unsigned)((plan.ntasks + groups - 1) / groups);
-    if (warp) fclass_kernel<32><<<grid, FCLASS_THREADS, smem, ctx.stream>>>(a, ctx.rys_tab7, s);
-    else fclass_kernel<FCLASS_THREADS><<<grid, FCLASS_THREADS, smem, ctx.stream>>>(a, ctx.rys_tab7, s);
-    return cudaGetLastError();
+    // the engine orientation (la lb lc ld) of classes 21..54, KDESC order
+#define LIBERI_F(kk, A, B, C, D) \
+    case kk: return fclass_t<A, B, C, D>(a, ctx.rys_tab7, ctx.stream);
+    switch (k) {
+        LIBERI_F(21, 3, 3, 3, 3) LIBERI_F(22, 0, 0, 3, 0) LIBERI_F(23, 0, 0, 3, 1) LIBERI_F(24, 0, 0, 3, 2)
+        LIBERI_F(25, 1, 0, 3, 0) LIBERI_F(26, 3, 3, 3, 0) LIBERI_F(27, 3, 0, 1, 1) LIBERI_F(28, 3, 0, 2, 0)
+        LIBERI_F(29, 2, 1, 3, 0) LIBERI_F(30, 2, 2, 3, 0) LIBERI_F(31, 3, 0, 3, 0) LIBERI_F(32, 3, 1, 1, 0)
+        LIBERI_F(33, 3, 1, 1, 1) LIBERI_F(34, 3, 1, 2, 0) LIBERI_F(35, 3, 1, 2, 1) LIBERI_F(36, 2, 2, 3, 1)
+        LIBERI_F(37, 3, 1, 3, 0) LIBERI_F(38, 3, 1, 3, 1) LIBERI_F(39, 3, 2, 1, 0) LIBERI_F(40, 3, 3, 3, 1)
+        LIBERI_F(41, 3, 2, 1, 1) LIBERI_F(42, 3, 2, 2, 0) LIBERI_F(43, 3, 2, 2, 1) LIBERI_F(44, 3, 2, 2, 2)
+        LIBERI_F(45, 3, 2, 3, 0) LIBERI_F(46, 3, 2, 3, 1) LIBERI_F(47, 3, 2, 3, 2) LIBERI_F(48, 3, 3, 0, 0)
+        LIBERI_F(49, 3, 3, 1, 0) LIBERI_F(50, 3, 3, 1, 1) LIBERI_F(51, 3, 3, 2, 0) LIBERI_F(52, 3, 3, 2, 1)
+        LIBERI_F(53, 3, 3, 2, 2) LIBERI_F(54, 3, 3, 3, 2)
+        default: return cudaErrorInvalidValue;
+    }
+#undef LIBERI_F
 }
 
 }  // namespace liberi
