@@ -118,7 +118,7 @@ static int ncart_l(int l) { return (l + 1) * (l + 2) / 2; }
 static int default_chunk(int k) {
     const KernelDesc &d = KDESC[k];
     const int nc = ncart_l(d.la) * ncart_l(d.lb) * ncart_l(d.lc) * ncart_l(d.ld);
-    if (k >= NKERN) return nc >= 1000 ? 1 : (nc >= 200 ? 2 : 8);
+    if (k >= NKERN) return 1;  // an f quartet is a group's work: one ket per task keeps every SM busy
     const int qpt = nc >= 216 ? 1 : (nc >= 54 ? 2 : 4);
     return CLASS_CTA_THREADS * qpt;
 }
