@@ -51,6 +51,7 @@ def parse_args():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-molecule batched SCF section")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop section")
+    ap.add_argument("--no-fshells", action="store_true", help="skip the f-shell workload section")
     ap.add_argument("--serve-rates", type=str, default="10,20,50,100,200,500",
                     help="Poisson build-request rates (req/s) of the serving capacity curve; the configured "
                          "50-500 and two rates below the GPU's capacity for this pool")
@@ -446,6 +447,9 @@ def run_ours(args):
         batched["mixed"]["max_dE_vs_fp64_batch"] = float(np.abs(emx - e64).max())
         batched["mixed_speedup_vs_fp64_batch"] = round(batched["fp64"]["ms_per_iteration_graph"] /
                                                        batched["mixed"]["ms_per_iteration_graph"], 3)
+    fshells = None
+    if world == 1 and not args.no_fshells:
+        fshells = run_fshells(dev, stream, cpu=not args.no_cpu_baseline)
     serve = None
     if world == 1 and not args.no_serve:
         curve = [run_serve(local, float(r), args.serve_sessions if float(r) >= 50 else max(1, args.serve_sessions // 2))
@@ -464,7 +468,7 @@ def run_ours(args):
                 "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 8 * ntri,
                         "d2h_bytes_per_step": 8 * ntri},
                 "gpu_launches": launched * args.steps, "roofline": roofline, "cpu_baseline": cpu,
-                "mixed": mixed, "batched": batched, "serve": serve,
+                "mixed": mixed, "batched": batched, "serve": serve, "f_shells": fshells,
                 "quartets": int(st0["quartets"].sum()), "prim_quartets": int(st0["prim_quartets"].sum())}
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -581,6 +585,56 @@ def run_batched(dev, stream, precision=0):
             "timing": "CUDA events per iteration (D update + build), inputs resident, no L2 flush "
                       "(all molecules' data fits in L2 as it would across SCF iterations)",
             "_energies": energies}
+
+
+def run_fshells(dev, stream, cpu=True):
+    """The f-shell classes on a 30-atom C/N/O/H cluster with a d and an f
+    polarisation shell on every heavy atom and a p shell on every H (470
+    functions; FP64, Schwarz table from the device generator, cut 1e-10),
+    device-resident D/F, CUDA events on the build's stream, median of 5 builds
+    after 2 (the working set stays in L2 between builds).  cpu_baseline: one
+    complete oracle build of the same inputs on every host core."""
+    import torch
+    from gms_liberi_b200 import liberi
+    from gms_liberi_b200 import molecules as M
+    b = M.f_cluster(30, seed=5)
+    b["schwrz"] = liberi.schwarz(b)
+    D = M.density(b["num_bas"], M.nocc_of(b), seed=1)
+    n = b["num_bas"]
+    ntri = n * (n + 1) // 2
+    dD = torch.tensor(D, device=dev)
+    dF = torch.zeros(ntri, dtype=torch.float64, device=dev)
+    h = liberi.liberi_create()
+    h.set_option("schwarz_cut", SCHWARZ_CUT)
+    liberi.setup_from_basis(h, b)
+    ts = []
+    for it in range(7):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        liberi.fock_build_device(h, dD.data_ptr(), dF.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if it >= 2:
+            ts.append(e0.elapsed_time(e1))
+    st = h.stats()
+    liberi.liberi_destroy(h)
+    ms = float(np.median(ts))
+    out = {"workload": "30-atom C/N/O/H cluster, 6-31G(d)-shaped s/p with one d and one f polarisation shell per "
+                       "heavy atom and a p shell per H (polarisation exponents in [0.3, 3]), Schwarz cut 1e-10",
+           "functions": n, "dtype": "f64", "ms": round(ms, 3),
+           "quartets_spd": int(st["quartets"][:21].sum()), "quartets_f": int(st["quartets"][21:].sum()),
+           "prim_quartets_f": int(st["prim_quartets"][21:].sum()),
+           "timing": "CUDA events, median of 5 builds after 2, no L2 flush (working set L2-resident)"}
+    if cpu:
+        from oracle import oracle
+        t0 = time.time()
+        _, info = oracle.fock_build(b, D, schwarz_cut=SCHWARZ_CUT, nthreads=os.cpu_count(), return_info=True)
+        wall = time.time() - t0
+        out["cpu_baseline"] = {"value": round(wall * 1e3, 1), "unit": "ms", "cores": int(info["nthreads"]),
+                               "kind": "port", "sample": "one complete build of the same inputs",
+                               "f_classes_ms": round(float(info["t_wall"][21:].sum()) * 1e3, 1)}
+        out["speedup_vs_cpu_baseline"] = round(wall * 1e3 / ms, 1)
+    return out
 
 
 _SERVE_POOL = None
