@@ -5,9 +5,9 @@
 // An f quartet is too large for the thread-per-quartet class kernels ((ff|ff)
 // holds 10,000 integrals and 7 roots), so a group of threads evaluates one
 // shell quartet at a time, everything in shared memory, with the class's
-// angular momenta as run-time parameters (one kernel serves all 34 classes).
+// angular momenta as compile-time parameters (one instantiation per class).
 // The group is one warp (four tasks per CTA, warp barriers only) where the
-// quartet's working set fits 24 KB, else the whole 128-thread CTA:
+// quartet's working set fits 24 KB, else a whole 256-thread CTA:
 //   1. 3 n threads per primitive quartet (one per root and Cartesian axis)
 //      take the root and weight from the 7-root table and run the 2D vertical
 //      recurrence g[e][f], e <= la+lb, f <= lc+ld (prefactor and weight folded
@@ -45,7 +45,7 @@ __host__ __device__ constexpr bool fwarp_mode(int la, int lb, int lc, int ld) {
 }
 // Primitive quartets per round: as many as the group's threads take in step 1
 // (3 n each) within 12 KB per warp group (four CTAs of four warps per SM) or
-// 96 KB per CTA group.
+// 96 KB per CTA group (two CTAs of eight warps per SM).
 __host__ __device__ constexpr int fnpq(int la, int lb, int lc, int ld, int nt) {
     int npq = nt / (3 * ((la + lb + lc + ld) / 2 + 1));
     while (npq > 1 && fgroup_bytes(la, lb, lc, ld, npq) > (nt == 32 ? 12 * 1024 : 96 * 1024)) npq--;
@@ -53,10 +53,11 @@ __host__ __device__ constexpr int fnpq(int la, int lb, int lc, int ld, int nt) {
 }
 
 // Compile-time shape of one class (engine orientation, la >= lb, lc >= ld) for
-// groups of NT threads.
+// groups of NT threads: one warp (CTAs of four warps) or a whole CTA of NT.
 template <int LA, int LB, int LC, int LD, int NT>
 struct FS {
     static constexpr int la = LA, lb = LB, lc = LC, ld = LD, nt = NT;
+    static constexpr int block = NT == 32 ? FCLASS_THREADS : NT;
     static constexpr int nroot = (LA + LB + LC + LD) / 2 + 1;
     static constexpr int nb = fnc(LB), nc = fnc(LC), nd = fnc(LD);
     static constexpr int ncd = nc * nd, ncomp = fnc(LA) * nb * ncd;
@@ -289,12 +290,12 @@ __device__ __forceinline__ void fquartet_block(const S &s, const FSmem &m, const
     }
 }
 
-// NT = 128: one task per CTA; NT = 32: one task per warp (four per CTA).
+// NT = 256: one task per CTA; NT = 32: one task per warp (four per CTA).
 template <typename S>
-__global__ void __launch_bounds__(FCLASS_THREADS) fclass_kernel(ClassArgs a, const double *__restrict__ tab7) {
+__global__ void __launch_bounds__(S::block) fclass_kernel(ClassArgs a, const double *__restrict__ tab7) {
     constexpr int NT = S::nt;
     constexpr S s{};
-    constexpr int GROUPS = FCLASS_THREADS / NT;
+    constexpr int GROUPS = S::block / NT;
     const int grp = NT == 32 ? (int)(threadIdx.x >> 5) : 0;
     const int task = (int)blockIdx.x * GROUPS + grp;
     if (task >= a.ntasks) return;  // the whole group (only warp barriers follow in warp mode)
@@ -416,13 +417,13 @@ cudaError_t launch_fschwarz(int pair_class, int npairs, int pair_off, const DevB
 template <int LA, int LB, int LC, int LD>
 static cudaError_t fclass_t(const ClassArgs &a, const double *tab7, cudaStream_t stream) {
     constexpr bool W = fwarp_mode(LA, LB, LC, LD);
-    using S = FS<LA, LB, LC, LD, W ? 32 : FCLASS_THREADS>;
-    constexpr int groups = FCLASS_THREADS / S::nt;
+    using S = FS<LA, LB, LC, LD, W ? 32 : 2 * FCLASS_THREADS>;
+    constexpr int groups = S::block / S::nt;
     const size_t smem = (size_t)groups * S::group_doubles * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(fclass_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned grid = (unsigned)((a.ntasks + groups - 1) / groups);
-    fclass_kernel<S><<<grid, FCLASS_THREADS, smem, stream>>>(a, tab7);
+    fclass_kernel<S><<<grid, S::block, smem, stream>>>(a, tab7);
     return cudaGetLastError();
 }
 
