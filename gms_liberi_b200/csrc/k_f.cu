@@ -204,8 +204,12 @@ __device__ __forceinline__ void fquartet_block(const S &s, const FSmem &m, const
     const double CD[3] = {C.x - D.x, C.y - D.y, C.z - D.z};
     const int npq_total = np * nq;
     for (int pq0 = 0; pq0 < npq_total; pq0 += s.npq) {
+        // slots of this round that hold a primitive quartet (uncontracted
+        // polarisation shells leave most of them empty): steps 2 and 3 cover
+        // only these
+        const int nslot = min(s.npq, npq_total - pq0);
         // 1. roots and the vertical recurrence, one thread per (slot, root, axis)
-        if (tid < s.npq * nrx) {
+        if (tid < nslot * nrx) {
             const int slot = tid / nrx, rx = tid - slot * nrx;
             const int r = rx / 3, x = rx - 3 * r;
             const int pq = pq0 + slot;
@@ -242,13 +246,11 @@ __device__ __forceinline__ void fquartet_block(const S &s, const FSmem &m, const
                         if (e > 0) v += (double)e * B00 * gs[(e - 1) * f1 + f];
                         gs[e * f1 + f + 1] = v;
                     }
-            } else {
-                for (int i = 0; i < gsz; i++) gs[i] = 0.0;  // empty slot contributes nothing
             }
         }
         group_sync<NT>();
         // 2. transfer to the 2D integrals of every (slot, root, axis)
-        const int nG = s.npq * nrx * Gsz;
+        const int nG = nslot * nrx * Gsz;
         for (int idx = tid; idx < nG; idx += NT) {
             const int tab_i = idx / Gsz, rem = idx - tab_i * Gsz;
             const int x = tab_i % 3;
@@ -279,7 +281,7 @@ __device__ __forceinline__ void fquartet_block(const S &s, const FSmem &m, const
             const int iy = gab[nab + iab] * s.ncd2 + gcd[s.ncd + icd];
             const int iz = gab[2 * nab + iab] * s.ncd2 + gcd[2 * s.ncd + icd];
             double v = 0.0;
-            const int ntab = s.npq * n;
+            const int ntab = nslot * n;
             for (int tr = 0; tr < ntab; tr++) {
                 const double *Gt = G + (size_t)tr * 3 * Gsz;
                 v = fma(Gt[ix] * Gt[Gsz + iy], Gt[2 * Gsz + iz], v);
