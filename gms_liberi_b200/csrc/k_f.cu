@@ -45,10 +45,12 @@ __host__ __device__ constexpr bool fwarp_mode(int la, int lb, int lc, int ld) {
 }
 // Primitive quartets per round: as many as the group's threads take in step 1
 // (3 n each) within 12 KB per warp group (four CTAs of four warps per SM) or
-// 96 KB per CTA group (two CTAs of eight warps per SM).
+// 48 KB per CTA group (four or more CTAs of eight warps per SM where the
+// block allows: a round rarely fills many slots, uncontracted polarisation
+// shells having one primitive each).
 __host__ __device__ constexpr int fnpq(int la, int lb, int lc, int ld, int nt) {
     int npq = nt / (3 * ((la + lb + lc + ld) / 2 + 1));
-    while (npq > 1 && fgroup_bytes(la, lb, lc, ld, npq) > (nt == 32 ? 12 * 1024 : 96 * 1024)) npq--;
+    while (npq > 1 && fgroup_bytes(la, lb, lc, ld, npq) > (nt == 32 ? 12 * 1024 : 48 * 1024)) npq--;
     return npq < 1 ? 1 : npq;
 }
 
