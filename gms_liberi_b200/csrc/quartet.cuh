@@ -1477,6 +1477,15 @@ cudaError_t launch_shape(const ClassArgs &a, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, R, BATCH, V>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, CLASS_DYN_SMEM_MAX);
     if (e != cudaSuccess) return e;
+    // the rest of the SM's 256 KB stays L1 (the class's Rys table rows, pair
+    // data and D): a shared-memory carveout of what MINB resident CTAs use
+    {
+        const size_t need = smem * (size_t)MINB;
+        const int carve = need == 0 ? 0 : (int)std::min<size_t>(100, (need * 100 + 228 * 1024 - 1) / (228 * 1024));
+        e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, R, BATCH, V>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        if (e != cudaSuccess) return e;
+    }
     class_kernel<LA, LB, LC, LD, R, BATCH, V><<<(unsigned)a.ntasks, CLASS_THREADS, smem, st>>>(args);
     return cudaGetLastError();
 }
