@@ -753,7 +753,7 @@ constexpr int tuned_minb(int key) {
     switch (key) {
         case 0: return 6;
         case 1000: return 6;
-        case 1010: return 4;
+        case 1010: return 6;  // with the L1-sized carveout its spills stay in L1: 14.19 -> 14.00 ms on C60
         case 1100: return 5;
         case 1110: return 4;
         case 1111: return 3;
@@ -885,7 +885,7 @@ constexpr int alt_minb(int key, bool f32, int v) {
     switch (key * 10 + v) {
         case 10001: return 8;
         case 10101: return 5;
-        case 10102: return 6;
+        case 10102: return 4;
         case 11001: return 5;
         case 11002: return 6;
         case 11101: return 3;
