@@ -106,6 +106,60 @@ __device__ __forceinline__ void rys_eval(double T, double thr, bool strict,
     }
 }
 
+// Table rows staged in shared memory: the classes with the large-T form from
+// T = 25 (the reference's t_max) need intervals 0..100 only; a CTA copies its
+// class's rows at start, each row padded by 16 bytes (stride 16N+2 doubles)
+// so that lanes reading different rows spread over the banks, and reads them
+// with 128-bit shared loads.  Measured per class on C60 (FP64): (ss|pp)
+// 6.17 -> 5.91 ms, (sp|sp) 14.21 -> 14.11, (ss|dd) 0.353 -> 0.336; slower in
+// the other classes ((ss|ss) 2.78 -> 3.14, (pp|pp) 9.63 -> 10.48, (ss|sd)
+// 1.91 -> 2.22 ms): the copy and the random-row bank conflicts cost more than
+// the L1 misses they save, so only those three stage their rows.
+constexpr int STAB_NINT = 25 * RYS_PER_UNIT + 1;
+__host__ __device__ constexpr int stab_stride(int n) { return 16 * n + 2; }
+template <int N>
+__device__ __forceinline__ void rys_eval_staged(double T, double thr, bool strict, const double *__restrict__ tab,
+                                                const double *stab, double *u, double *w) {
+    bool asym = strict ? (T > thr) : (T >= thr);
+    if (asym) {
+        double it = 1.0 / T, sq = sqrt(it);
+        const double *hr = tab + rys_herm_off(N);
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            u[i] = __ldg(hr + i) * it;
+            w[i] = __ldg(hr + MAXROOT + i) * sq;
+        }
+        return;
+    }
+    const double t4 = T * (double)RYS_PER_UNIT;
+    const int k = (int)t4;
+    const double x = 2.0 * (t4 - (double)k) - 1.0;
+    const double *base = stab + k * stab_stride(N);
+    const double x2 = x * x, x4 = x2 * x2;
+#pragma unroll
+    for (int f = 0; f < 2 * N; f++) {
+        const double2 q0 = *reinterpret_cast<const double2 *>(base + f * RYS_NCOEF);
+        const double2 q1 = *reinterpret_cast<const double2 *>(base + f * RYS_NCOEF + 2);
+        const double2 q2 = *reinterpret_cast<const double2 *>(base + f * RYS_NCOEF + 4);
+        const double2 q3 = *reinterpret_cast<const double2 *>(base + f * RYS_NCOEF + 6);
+        const double a0 = fma(q0.y, x, q0.x), a1 = fma(q1.y, x, q1.x);
+        const double a2 = fma(q2.y, x, q2.x), a3 = fma(q3.y, x, q3.x);
+        const double b0 = fma(a1, x2, a0), b1 = fma(a3, x2, a2);
+        const double v = fma(b1, x4, b0);
+        if (f < N) u[f] = v; else w[f - N] = v;
+    }
+}
+// the classes that stage their rows (FP64 (ss|pp), (sp|sp), (ss|dd))
+template <int LA, int LB, int LC, int LD, typename R>
+constexpr bool stab_class() {
+    constexpr int key = LA * 1000 + LB * 100 + LC * 10 + LD;
+    return std::is_same<R, double>::value && (key == 1100 || key == 1010 || key == 2200);
+}
+template <int LA, int LB, int LC, int LD, typename R>
+constexpr size_t stab_bytes() {
+    return stab_class<LA, LB, LC, LD, R>() ? (size_t)STAB_NINT * stab_stride((LA + LB + LC + LD) / 2 + 1) * 8 : 0;
+}
+
 // FP32 tier: width-1/8 intervals, degree 3 (two functions per 256-bit load);
 // the large-T limit as in FP64.
 template <int N>
@@ -510,7 +564,7 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                                            R cdx, R cdy, R cdz, double thr, bool strict,
                                            const double *__restrict__ tab, const float *__restrict__ tabf,
                                            int mu0, ACC &acc, R *cache_u, R *cache_w, int cache,
-                                           float pthr = 0.f, float bpmax = 0.f) {
+                                           float pthr = 0.f, float bpmax = 0.f, const double *stab = nullptr) {
     constexpr int NA = ncart(LA);
     constexpr int LAB = LA + LB, LCD = LC + LD;
     constexpr int NR = (LAB + LCD) / 2 + 1;
@@ -561,7 +615,10 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                     const double rs = rsqrt(p + q);
                     const double ipq = rs * rs;
                     const double T = p * q * ipq * (pqx * pqx + pqy * pqy + pqz * pqz);
-                    rys_eval<NR>(T, thr, strict, tab, u, w);
+                    if (stab_class<LA, LB, LC, LD, R>() && stab != nullptr)
+                        rys_eval_staged<NR>(T, thr, strict, tab, stab, u, w);
+                    else
+                        rys_eval<NR>(T, thr, strict, tab, u, w);
                     const double pref = Px.x * Qx.x * rs;
 #pragma unroll
                     for (int i = 0; i < NR; i++) {
@@ -1167,7 +1224,8 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
                                            const double4 &C, R abx, R aby, R abz, R cdx, R cdy, R cdz,
                                            double thr, bool strict, const double *__restrict__ tab,
                                            const float *__restrict__ tabf, const QuartetCtx<R> &qc,
-                                           const Rows<R> &rows, KB &kb, float pthr, float bpmax) {
+                                           const Rows<R> &rows, KB &kb, float pthr, float bpmax,
+                                           const double *stab) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     using PS = PassShape<LA, LB, LC, LD, R, V>;
     constexpr int M = PS::NMU;
@@ -1193,7 +1251,7 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
             Acc acc;
             eval_block<LA, LB, LC, LD, R, M, HGP>(b, p0, np, q0, nq, A, C, abx, aby, abz, cdx, cdy, cdz, thr, strict,
                                                   tab, tabf, mu0, acc, cache_u, cache_w,
-                                                  cache_ok ? (pass == 0 ? 1 : 2) : 0, pthr, bpmax);
+                                                  cache_ok ? (pass == 0 ? 1 : 2) : 0, pthr, bpmax, stab);
             digest_pass<LA, LB, LC, LD, R, M, HGP, 1>(acc, mu0, true, abx, aby, abz, qc, rows, kb);
         }
     } else {
@@ -1209,7 +1267,7 @@ __device__ __forceinline__ void run_passes(const DevBasis &b, int p0, int np, in
             Acc acc;
             eval_block<LA, LB, LC, LD, R, M, HGP>(b, p0, np, q0, live ? nq : 0, A, C, abx, aby, abz, cdx, cdy, cdz,
                                                   thr, strict, tab, tabf, mu0, acc, cache_u, cache_w,
-                                                  cache_ok ? (trip == 0 ? 1 : 2) : 0, pthr, bpmax);
+                                                  cache_ok ? (trip == 0 ? 1 : 2) : 0, pthr, bpmax, stab);
             digest_pass<LA, LB, LC, LD, R, M, HGP, G>(acc, mu0, live, abx, aby, abz, qc, rows, kb);
         }
     }
@@ -1314,7 +1372,23 @@ template <int LA, int LB, int LC, int LD, typename R, bool BATCH, int V>
 __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     extern __shared__ __align__(16) unsigned char class_smem[];
-    R *tile = reinterpret_cast<R *>(class_smem);  // the digestion type: FP32 tile for the FP32 tier
+    // the class's staged table rows come first (16-byte aligned), then the
+    // F-row tile and the per-thread slots
+    constexpr size_t STB = stab_bytes<LA, LB, LC, LD, R>();
+    const double *stab = nullptr;
+    if constexpr (STB > 0) {
+        constexpr int NRt = (LA + LB + LC + LD) / 2 + 1;
+        double *st = reinterpret_cast<double *>(class_smem);
+        const double *g = a.tab + rys_table_off(NRt);
+        for (int i = threadIdx.x; i < STAB_NINT * 16 * NRt; i += CLASS_THREADS) {
+            const int kk = i / (16 * NRt), j = i - kk * 16 * NRt;
+            st[kk * stab_stride(NRt) + j] = __ldg(g + i);
+        }
+        __syncthreads();
+        // rows 0..100 cover T <= 25: the class's large-T form takes every T above
+        if (a.thr <= 25.0) stab = st;
+    }
+    R *tile = reinterpret_cast<R *>(class_smem + STB);  // the digestion type: FP32 tile for the FP32 tier
     const int ibra = t.x, k0 = t.y, cnt = t.z;
     const DevBasis &bas = mol_basis<BATCH>(a, t.w);
 #define LIBERI_D mol_D<BATCH, R>(a, t.w)
@@ -1382,7 +1456,7 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
 #pragma unroll
         for (int i = 0; i < KBuf<NB, NC, ND, SM, R>::N; i++) kb.at(i) = R(0);
         run_passes<LA, LB, LC, LD, R, V>(bas, p0, np, (int)(unsigned)kpr, act ? (int)(unsigned)(kpr >> 32) : 0, A, C, abx, aby,
-                                      abz, cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb, pthr, bpmax);
+                                      abz, cdx, cdy, cdz, a.thr, a.strict, a.tab, a.tabf, qc, rowsA, kb, pthr, bpmax, stab);
         if constexpr (G > 1) {
             // the group's lanes hold partial sums over their passes: combine
             // them, the group's first lane adds them to F
@@ -1470,8 +1544,9 @@ cudaError_t launch_shape(const ClassArgs &a, cudaStream_t st) {
     // the global atomics it saves.
     constexpr int MINB = PassShape<LA, LB, LC, LD, R, V>::MINB;
     ClassArgs args = a;
-    args.tile_rows = (a.tile_rows && (tile_bytes + slot_bytes) * MINB <= CLASS_DYN_SMEM_MAX) ? 1 : 0;
-    const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes;
+    constexpr size_t STB = stab_bytes<LA, LB, LC, LD, R>();
+    args.tile_rows = (a.tile_rows && (tile_bytes + slot_bytes + STB) * MINB <= CLASS_DYN_SMEM_MAX) ? 1 : 0;
+    const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes + STB;
     // the opt-in limit is raised to the per-CTA maximum, not to this launch's
     // size: a captured graph may hold a larger launch
     cudaError_t e = cudaFuncSetAttribute(class_kernel<LA, LB, LC, LD, R, BATCH, V>,
