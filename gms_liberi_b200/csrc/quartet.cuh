@@ -192,6 +192,40 @@ __device__ __forceinline__ void rys_eval(float T, float thr, bool strict, const 
     }
 }
 
+// ---- two Rys roots in one packed FP32 pair (FP32 tier) ------------------------
+// F2 holds one quantity for two roots of a primitive quartet; its arithmetic
+// is the paired single-precision instructions of sm_100 (__fmul2_rn,
+// __fadd2_rn, __ffma2_rn), so the recurrences and transfers of two roots
+// issue as one.  A product is kept unrounded (F2P) until it meets an addition,
+// which then becomes one fused multiply-add, as the compiler contracts the
+// scalar code.
+struct F2 {
+    float2 v;
+    F2() = default;
+    __device__ __forceinline__ explicit F2(float s) : v(make_float2(s, s)) {}
+    __device__ __forceinline__ F2(float a, float b) : v(make_float2(a, b)) {}
+    __device__ __forceinline__ explicit F2(float2 x) : v(x) {}
+};
+struct F2P {
+    float2 a, b;
+    __device__ __forceinline__ operator F2() const { return F2(__fmul2_rn(a, b)); }
+};
+__device__ __forceinline__ F2P operator*(F2 x, F2 y) { return F2P{x.v, y.v}; }
+__device__ __forceinline__ F2P operator*(F2P x, F2 y) { return F2P{__fmul2_rn(x.a, x.b), y.v}; }
+__device__ __forceinline__ F2 operator+(F2 x, F2 y) { return F2(__fadd2_rn(x.v, y.v)); }
+__device__ __forceinline__ F2 operator+(F2 x, F2P y) { return F2(__ffma2_rn(y.a, y.b, x.v)); }
+__device__ __forceinline__ F2 operator+(F2P x, F2 y) { return F2(__ffma2_rn(x.a, x.b, y.v)); }
+__device__ __forceinline__ F2 operator+(F2P x, F2P y) { return F2(__ffma2_rn(x.a, x.b, __fmul2_rn(y.a, y.b))); }
+__device__ __forceinline__ F2 &operator+=(F2 &x, F2P y) { x = F2(__ffma2_rn(y.a, y.b, x.v)); return x; }
+__device__ __forceinline__ F2 &operator+=(F2 &x, F2 y) { x = F2(__fadd2_rn(x.v, y.v)); return x; }
+// FP32 classes that run their roots in pairs.  Measured per class on C60
+// (mixed builds, every FP32 class with two or more roots paired): (pd|pd)
+// 3.05 -> 2.91 ms at cut 1e-2 and 3.36 -> 3.22 ms at 1e-5; the others lost or
+// did not change ((pd|pp) 6.17 -> 6.71, (sp|pd) 5.16 -> 5.47, all paired:
+// 49.3 -> 50.7 ms at cut 1e-2), the packing moves costing what the paired
+// instructions save.
+constexpr bool pair_roots_class(int key) { return key == 2121; }
+
 // ---- recurrences -------------------------------------------------------------
 template <int LAB, int LCD, typename R>
 __device__ __forceinline__ void vrr(R (&g)[LAB + 1][LCD + 1], R c00, R cp00, R b10, R b01,
@@ -552,6 +586,73 @@ __device__ __forceinline__ void contract_root(const R (&gx)[LA + LB + 1][LC + LD
     }
 }
 
+// contract_root for a pair of roots (FP32 tier): the transfers run on the
+// packed pair, each integral adds its two roots' products to the scalar
+// accumulator (one paired multiply and two fused multiply-adds)
+__device__ __forceinline__ float acc_pair(F2 x, F2 y, F2 z, float acc) {
+    const float2 t = __fmul2_rn(x.v, y.v);
+    return fmaf(t.y, z.v.y, fmaf(t.x, z.v.x, acc));
+}
+template <int LA, int LB, int LC, int LD, int NMU>
+__device__ __forceinline__ void contract_root_pair(const F2 (&gx)[LA + LB + 1][LC + LD + 1],
+                                                   const F2 (&gy)[LA + LB + 1][LC + LD + 1],
+                                                   const F2 (&gz)[LA + LB + 1][LC + LD + 1], F2 abx, F2 aby, F2 abz,
+                                                   F2 cdx, F2 cdy, F2 cdz, const int (&ex)[NMU], const int (&ey)[NMU],
+                                                   const int (&ez)[NMU],
+                                                   float (&acc)[NMU][ncart(LB)][ncart(LC)][ncart(LD)]) {
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    constexpr bool FULL = (NMU == NA);
+    if constexpr (FULL) {
+        F2 ix[LA + 1][LB + 1][LC + 1][LD + 1], iy[LA + 1][LB + 1][LC + 1][LD + 1],
+            iz[LA + 1][LB + 1][LC + 1][LD + 1];
+        hrr<LA, LB, LC, LD, F2>(gx, abx, cdx, ix);
+        hrr<LA, LB, LC, LD, F2>(gy, aby, cdy, iy);
+        hrr<LA, LB, LC, LD, F2>(gz, abz, cdz, iz);
+#pragma unroll
+        for (int m = 0; m < NMU; m++)
+#pragma unroll
+            for (int ib = 0; ib < NB; ib++)
+#pragma unroll
+                for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                    for (int id = 0; id < ND; id++)
+                        acc[m][ib][ic][id] = acc_pair(ix[cxp(LA, m)][cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)],
+                                                      iy[cyp(LA, m)][cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)],
+                                                      iz[czp(LA, m)][czp(LB, ib)][czp(LC, ic)][czp(LD, id)],
+                                                      acc[m][ib][ic][id]);
+    } else {
+#pragma unroll
+        for (int m = 0; m < NMU; m++) {
+            F2 sx[LB + 1][LC + 1][LD + 1], sy[LB + 1][LC + 1][LD + 1], sz[LB + 1][LC + 1][LD + 1];
+            hrr_slice<LA, LB, LC, LD, F2>(gx, ex[m], abx, cdx, sx);
+            hrr_slice<LA, LB, LC, LD, F2>(gy, ey[m], aby, cdy, sy);
+            hrr_slice<LA, LB, LC, LD, F2>(gz, ez[m], abz, cdz, sz);
+#pragma unroll
+            for (int ib = 0; ib < NB; ib++)
+#pragma unroll
+                for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                    for (int id = 0; id < ND; id++)
+                        acc[m][ib][ic][id] = acc_pair(sx[cxp(LB, ib)][cxp(LC, ic)][cxp(LD, id)],
+                                                      sy[cyp(LB, ib)][cyp(LC, ic)][cyp(LD, id)],
+                                                      sz[czp(LB, ib)][czp(LC, ic)][czp(LD, id)], acc[m][ib][ic][id]);
+        }
+    }
+}
+template <int LA, int LB, int LC>
+__device__ __forceinline__ void contract_hgp_pair(const F2 (&gx)[LA + LB + 1][LC + 1], const F2 (&gy)[LA + LB + 1][LC + 1],
+                                                  const F2 (&gz)[LA + LB + 1][LC + 1],
+                                                  float (&acc)[nrange(LA, LA + LB)][ncart(LC)]) {
+#pragma unroll
+    for (int e = 0; e < nrange(LA, LA + LB); e++) {
+        const int le = range_l(LA, e), ie = range_i(LA, e);
+#pragma unroll
+        for (int ic = 0; ic < ncart(LC); ic++)
+            acc[e][ic] = acc_pair(gx[cart_x(le, ie)][cxp(LC, ic)], gy[cart_y(le, ie)][cyp(LC, ic)],
+                                  gz[cart_z(le, ie)][czp(LC, ic)], acc[e][ic]);
+    }
+}
+
 // acc[m][ib][ic][id] for A components ia = mu0 + m (m < NMU, ia < NA), all of
 // B, C, D.  A single pass (NMU == NA) uses compile-time component indices; a
 // multi-pass class selects the A exponent at run time, so one copy of the
@@ -698,6 +799,35 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                     }
                 }
                 slot++;
+                if constexpr (NR >= 2 && pair_roots_class(LA * 1000 + LB * 100 + LC * 10 + LD)) {
+                    // roots in pairs (a last odd root pairs with a zero weight)
+                    constexpr int NP = (NR + 1) / 2;
+                    float u2[2 * NP], w2[2 * NP];
+#pragma unroll
+                    for (int i = 0; i < 2 * NP; i++) {
+                        u2[i] = i < NR ? u[i] : 0.f;
+                        w2[i] = i < NR ? w[i] : 0.f;
+                    }
+#pragma unroll(FULL ? NP : 1)
+                    for (int r = 0; r < NP; r++) {
+                        const F2 ui(u2[0], u2[1]), wr(w2[0], w2[1]);
+#pragma unroll
+                        for (int i = 0; i + 2 < 2 * NP; i++) {  // rotate the next pair to the front
+                            u2[i] = u2[i + 2];
+                            w2[i] = w2[i + 2];
+                        }
+                        const F2 fq = F2(q) * ui, fp = F2(p) * ui;
+                        const F2 b00 = F2(0.5f) * ui;
+                        const F2 b10 = F2(hp) * (F2(1.0f) + F2(-q) * ui), b01 = F2(hq) * (F2(1.0f) + F2(-p) * ui);
+                        F2 gx[LAB + 1][LCD + 1], gy[LAB + 1][LCD + 1], gz[LAB + 1][LCD + 1];
+                        vrr<LAB, LCD, F2>(gx, F2(Pa.x) + F2(-pqx) * fq, F2(Qa.x) + F2(pqx) * fp, b10, b01, b00, F2(1.0f));
+                        vrr<LAB, LCD, F2>(gy, F2(Pa.y) + F2(-pqy) * fq, F2(Qa.y) + F2(pqy) * fp, b10, b01, b00, F2(1.0f));
+                        vrr<LAB, LCD, F2>(gz, F2(Pa.z) + F2(-pqz) * fq, F2(Qa.z) + F2(pqz) * fp, b10, b01, b00, wr);
+                        if constexpr (HGP) contract_hgp_pair<LA, LB, LC>(gx, gy, gz, acc);
+                        else contract_root_pair<LA, LB, LC, LD, NMU>(gx, gy, gz, F2(abx), F2(aby), F2(abz), F2(cdx),
+                                                                    F2(cdy), F2(cdz), ex, ey, ez, acc);
+                    }
+                } else {
 #pragma unroll(FULL ? NR : 1)
                 for (int r = 0; r < NR; r++) {
                     const float ui = u[0], wr = w[0];
@@ -714,6 +844,7 @@ __device__ __forceinline__ void eval_block(const DevBasis &b, int p0, int np, in
                     vrr<LAB, LCD, R>(gz, Pa.z - fq * pqz, Qa.z + fp * pqz, b10, b01, b00, wr);
                     if constexpr (HGP) contract_hgp<LA, LB, LC, R>(gx, gy, gz, acc);
                     else contract_root<LA, LB, LC, LD, R, NMU>(gx, gy, gz, abx, aby, abz, cdx, cdy, cdz, ex, ey, ez, acc);
+                }
                 }
             }
         }
