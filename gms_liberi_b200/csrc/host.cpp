@@ -1815,10 +1815,13 @@ int liberi_c_autotune(liberi_handle h, int32_t reps, int32_t *chunks_out) {
         if (rc) break;
         h->chunk[k] = best_c;
         h->variant[0][k] = best_v;
-        // FP32 tier shape (handles in mixed precision): all quartets in FP32
+        // FP32 tier shape (handles in mixed precision), timed on the class's
+        // build at the handle's own cut (its FP32 primitive screening follows
+        // the cut: a cut that sent every quartet to FP32 would skip every
+        // primitive)
         if (prec0 == 1) {
             h->precision = 1;
-            h->fp32_cut = 1e300;
+            h->fp32_cut = cut0;
             float best32 = 1e30f;
             int best_v32 = h->variant[1][k];
             for (int v = 0; v < NVARIANT && !rc; v++) {

@@ -904,7 +904,13 @@ __device__ __forceinline__ T dget(const T *__restrict__ Dm, unsigned ld, unsigne
 // Per-class compile-time shape: A components per pass (bounds the contracted
 // block held in registers) and resident CTAs per SM requested from the
 // register allocator.  The table was tuned offline with ptxas register and
-// spill reports; LIBERI_TUNE_* override one class for that search.
+// spill reports; LIBERI_TUNE_* override one class for that search.  The FP64
+// resident-CTA counts were measured again, per class, on C60 with the
+// shared-memory carveout sized to the resident CTAs and the staged table
+// rows (every count from three below to one above the earlier choice):
+// (sp|sp) 6 -> 4 (14.10 -> 12.99 ms: no spills, and its table rows out of
+// L1), (sp|sd) 5 -> 4 (4.96 -> 4.14), (ss|sd) 6 -> 5 (1.91 -> 1.75), (sd|sd)
+// 2 -> 3 (0.73 -> 0.70), (dd|dd) 2 -> 1 (0.45 -> 0.33 ms).
 constexpr int class_key(int la, int lb, int lc, int ld) { return la * 1000 + lb * 100 + lc * 10 + ld; }
 constexpr int tuned_nmu(int key) {
 #ifdef LIBERI_TUNE_KEY
@@ -941,14 +947,14 @@ constexpr int tuned_minb(int key) {
     switch (key) {
         case 0: return 6;
         case 1000: return 6;
-        case 1010: return 6;  // with the L1-sized carveout its spills stay in L1: 14.19 -> 14.00 ms on C60
+        case 1010: return 4;
         case 1100: return 5;
         case 1110: return 4;
         case 1111: return 3;
         case 1120: return 2;
-        case 2000: return 6;
-        case 2010: return 5;
-        case 2020: return 2;
+        case 2000: return 5;
+        case 2010: return 4;
+        case 2020: return 3;
         case 2100: return 4;
         case 2110: return 2;
         case 2111: return 3;
@@ -959,13 +965,17 @@ constexpr int tuned_minb(int key) {
         case 2211: return 2;
         case 2220: return 2;
         case 2221: return 2;
-        case 2222: return 2;
+        case 2222: return 1;
         default: return 3;
     }
 }
 
 // FP32 tier shapes (half the register footprint per value); 0 / default
-// falls back to the FP64 choice.  LIBERI_TUNE_* with LIBERI_TUNE_F32 override
+// falls back to the FP64 choice.  Resident-CTA counts measured again per
+// class in the C60 mixed build at cut 1e-2 (every count from three below to
+// one above the earlier choice): one more CTA pays in (pp|pp) 3.99 -> 3.80,
+// (pd|pp) 6.20 -> 5.91, (ss|sp) 4.19 -> 4.11, (ss|sd) 1.13 -> 1.10 and (pd|sd)
+// 2.06 -> 2.02 ms.  LIBERI_TUNE_* with LIBERI_TUNE_F32 override
 // one class of this table for the offline search.
 constexpr int tuned_nmu_f32(int key) {
 #ifdef LIBERI_TUNE_KEY
@@ -1000,24 +1010,25 @@ constexpr int tuned_minb_f32(int key) {
 #endif
     switch (key) {
         case 0: return 8;
-        case 1000: return 8;
+        case 1000: return 9;
         case 1010: return 8;
         case 1100: return 8;
         case 1110: return 5;
-        case 1111: return 4;
+        case 1111: return 5;
         case 1120: return 3;
-        case 2000: return 6;
+        case 2000: return 7;
         case 2010: return 6;
         case 2020: return 4;
         case 2100: return 5;
         case 2110: return 3;
-        case 2111: return 4;
-        case 2120: return 3;
+        case 2111: return 5;
+        case 2120: return 4;
         case 2121: return 2;
         case 2200: return 3;
         case 2210: return 3;
         case 2211: return 2;
         case 2220: return 2;
+        case 2222: return 2;
         default: return tuned_minb(key);
     }
 }
@@ -1073,7 +1084,7 @@ constexpr int alt_minb(int key, bool f32, int v) {
     switch (key * 10 + v) {
         case 10001: return 8;
         case 10101: return 5;
-        case 10102: return 4;
+        case 10102: return 6;
         case 11001: return 5;
         case 11002: return 6;
         case 11101: return 3;
@@ -1504,8 +1515,8 @@ __device__ __forceinline__ void class_task(const ClassArgs &a, const int4 t) {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     extern __shared__ __align__(16) unsigned char class_smem[];
     // the class's staged table rows come first (16-byte aligned), then the
-    // F-row tile and the per-thread slots
-    constexpr size_t STB = stab_bytes<LA, LB, LC, LD, R>();
+    // F-row tile and the per-thread slots (batched launches do not stage)
+    constexpr size_t STB = BATCH ? 0 : stab_bytes<LA, LB, LC, LD, R>();
     const double *stab = nullptr;
     if constexpr (STB > 0) {
         constexpr int NRt = (LA + LB + LC + LD) / 2 + 1;
@@ -1675,7 +1686,7 @@ cudaError_t launch_shape(const ClassArgs &a, cudaStream_t st) {
     // the global atomics it saves.
     constexpr int MINB = PassShape<LA, LB, LC, LD, R, V>::MINB;
     ClassArgs args = a;
-    constexpr size_t STB = stab_bytes<LA, LB, LC, LD, R>();
+    constexpr size_t STB = BATCH ? 0 : stab_bytes<LA, LB, LC, LD, R>();
     args.tile_rows = (a.tile_rows && (tile_bytes + slot_bytes + STB) * MINB <= CLASS_DYN_SMEM_MAX) ? 1 : 0;
     const size_t smem = (args.tile_rows ? tile_bytes : 0) + slot_bytes + STB;
     // the opt-in limit is raised to the per-CTA maximum, not to this launch's
