@@ -122,6 +122,17 @@ static int default_chunk(int k) {
     // (ss|dd) and (sp|dd): few kets per row pair survive the screening; short
     // tasks spread them (C60: 0.35 -> 0.32 and 1.12 -> 1.08 ms)
     if (k == 10 || k == 11) return CLASS_CTA_THREADS;
+    // measured on C60 (FP64, liberi_c_autotune): longer tasks for the low-L
+    // classes ((sp|sp) 13.00 -> 12.67 ms at 2048 kets, (ss|sp) 10.41 -> 10.32,
+    // (ss|pp) 5.93 -> 5.84, (pp|pp) 9.61 -> 9.53 at 1024), shorter ones for
+    // (sd|sd) (0.70 -> 0.68 ms at 128) and (pd|pd) (4.30 -> 4.25 ms at 256)
+    switch (k) {
+        case 1: case 4: return 2048;
+        case 2: case 3: case 5: return 1024;
+        case 13: return 128;
+        case 15: return 256;
+        default: break;
+    }
     const int qpt = nc >= 216 ? 1 : (nc >= 54 ? 2 : 4);
     return CLASS_CTA_THREADS * qpt;
 }
