@@ -203,6 +203,13 @@ struct liberi_handle_s {
     // tile's shared memory costs more L1, where tables and spills live, than
     // its atomics save; measured on C60 and the batched molecules)
     uint32_t tile_mask = 0;
+    // FP64 builds: classes launched on the side stream beside the others: the
+    // high-L classes of few long CTAs and the small low-occupancy ones
+    // ((ss|dd), (sp|dd), (sd|sd), (dd|pp), (pd|pd), (dd|sd), (dd|pd),
+    // (dd|dd)).  Measured on C60: 100.40 ms with (dd|dd) and (dd|pd) alone
+    // there, 99.64 ms with these eight.
+    uint32_t side_mask = (1u << 10) | (1u << 11) | (1u << 13) | (1u << 14) | (1u << 15) | (1u << 18) | (1u << 19) |
+                         (1u << 20);
     int chunk[NKALL] = {};  // kets per CTA task per class (0 = default)
     int variant[2][NKERN] = {};  // kernel shape variant per class, FP64 / FP32 tier
     bool timing = false;
@@ -966,7 +973,7 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
         if ((h->class_mask >> k) & 1u) nquart += h->stats.quartets[k];
     const bool fan = h->fan_out && h->overlap && !h->timing && nquart <= FAN_MAX_QUARTETS;
     const bool fork = h->overlap && !h->timing && !fan;
-    const uint32_t side64 = mixed ? 0u : (1u << 20) | (1u << 19);
+    const uint32_t side64 = mixed ? 0u : h->side_mask;
     if (fan) {
         if (mixed)
             for (int k = 0; k < NKERN; k++) {
@@ -1907,6 +1914,9 @@ int liberi_c_set_option(liberi_handle h, const char *name, double value) {
         if (value != 0 && value != 1) return fail(LIBERI_E_ARG, "rank_split must be 0 or 1");
         if (h->initialized) return fail(LIBERI_E_STATE, "rank_split must be chosen before setup");
         h->rank_split = (int)value;
+    } else if (n == "side_mask") {
+        if (!(value >= 0 && value < (double)(1u << NKERN))) return fail(LIBERI_E_ARG, "side_mask out of range");
+        h->side_mask = (uint32_t)value;
     } else if (n == "overlap") {
         h->overlap = value != 0;
     } else if (n == "fan") {
@@ -1934,6 +1944,7 @@ int liberi_c_get_option(liberi_handle h, const char *name, double *value) {
     else if (n == "device") *value = h->device;
     else if (n == "class_mask") *value = h->class_mask;
     else if (n == "tile_mask") *value = h->tile_mask;
+    else if (n == "side_mask") *value = h->side_mask;
     else if (n == "overlap") *value = h->overlap ? 1 : 0;
     else if (n == "fan") *value = h->fan_out ? 1 : 0;
     else if (n == "rank_split") *value = h->rank_split;

@@ -118,9 +118,12 @@ int liberi_c_last_error(char *buf, int32_t len);
  *                   build's stream: builds of at most 25 million screened
  *                   quartets spread their classes over 8 streams (while "fan"
  *                   is 1); larger ones run every class's FP64 task list beside
- *                   the FP32 lists (mixed precision) or the (dd|dd) and (dd|pd)
- *                   classes beside the others (FP64) on a second stream;
+ *                   the FP32 lists (mixed precision) or the classes of
+ *                   "side_mask" beside the others (FP64) on a second stream;
  *                   default 1; off while "timing")
+ *   "side_mask"    (bit k set = FP64 builds launch class k on the second
+ *                   stream; default the high-L and low-occupancy classes
+ *                   measured faster there on C60)
  *   "fan"          (1 = the 8-stream spread of small builds above, default 1;
  *                   set 0 where many handles build at once and already fill
  *                   the GPU, as the serving loop does)
