@@ -257,14 +257,16 @@ def test_calls_keep_the_callers_current_device():
 @pytest.mark.parametrize("mol", ["ethane", "random_9"])
 def test_launch_options_do_not_change_results(mol):
     # F-row tile on/off, side-stream overlap on/off, the multi-stream spread of
-    # small builds on/off, shape variants: the same F
+    # small builds on/off, the FP64 side-stream class set (none, all), shape
+    # variants: the same F
     # (up to the order of FP64 atomics), FP64 and mixed
     b, nocc = _molecule(mol)
     D = M.density(b["num_bas"], nocc, seed=12)
     Fo = oracle.fock_build(b, D, schwarz_cut=1e-10)
     for prec in (0, 1):
         base, _ = gpu_fock(b, D, schwarz_cut=1e-10, precision=prec, fp32_cut=1e-7)
-        variants = [dict(tile_mask=(1 << 21) - 1), dict(overlap=0), dict(fan=0)]
+        variants = [dict(tile_mask=(1 << 21) - 1), dict(overlap=0), dict(fan=0),
+                    dict(fan=0, side_mask=0), dict(fan=0, side_mask=(1 << 21) - 1)]
         for opts in variants:
             F, _ = gpu_fock(b, D, schwarz_cut=1e-10, precision=prec, fp32_cut=1e-7, **opts)
             assert np.abs(F - base).max() <= 1e-11, (prec, opts)
