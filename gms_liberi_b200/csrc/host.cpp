@@ -205,11 +205,11 @@ struct liberi_handle_s {
     uint32_t tile_mask = 0;
     // FP64 builds: classes launched on the side stream beside the others: the
     // high-L classes of few long CTAs and the small low-occupancy ones
-    // ((ss|dd), (sp|dd), (sd|sd), (dd|pp), (pd|pd), (dd|sd), (dd|pd),
-    // (dd|dd)).  Measured on C60: 100.40 ms with (dd|dd) and (dd|pd) alone
-    // there, 99.64 ms with these eight.
-    uint32_t side_mask = (1u << 10) | (1u << 11) | (1u << 13) | (1u << 14) | (1u << 15) | (1u << 18) | (1u << 19) |
-                         (1u << 20);
+    // ((ss|dd), (sp|dd), (sd|sd) and the seven Rys classes).  Measured on C60:
+    // 100.40 ms with (dd|dd) and (dd|pd) alone there, 99.37 ms with these ten
+    // (99.60 without (pd|sd) and (pd|pp), 99.51 with (pp|sd) added).
+    uint32_t side_mask = (1u << 10) | (1u << 11) | (1u << 13) | (1u << 14) | (1u << 15) | (1u << 16) | (1u << 17) |
+                         (1u << 18) | (1u << 19) | (1u << 20);
     int chunk[NKALL] = {};  // kets per CTA task per class (0 = default)
     int variant[2][NKERN] = {};  // kernel shape variant per class, FP64 / FP32 tier
     bool timing = false;

@@ -71,9 +71,9 @@ def test_launch_options_round_trip():
     h = liberi.liberi_create()
     assert h.get_option("overlap") == 1 and h.get_option("fan") == 1
     assert h.get_option("tile_mask") == 0 and h.get_option("rank_split") == 0
-    # FP64 side stream: (ss|dd), (sp|dd), (sd|sd), (dd|pp), (pd|pd), (dd|sd), (dd|pd), (dd|dd)
-    side = [liberi.KERNELS.index(n) for n in ("int0022", "int0122", "int0202", "int2211", "int2121", "int2220",
-                                               "int2221", "int2222")]
+    # FP64 side stream: (ss|dd), (sp|dd), (sd|sd) and the seven Rys classes
+    side = [liberi.KERNELS.index(n) for n in ("int0022", "int0122", "int0202", "int2211", "int2121", "int2120",
+                                               "int2111", "int2220", "int2221", "int2222")]
     assert h.get_option("side_mask") == sum(1 << k for k in side)
     for name, val in [("overlap", 0), ("fan", 0), ("tile_mask", 5), ("rank_split", 1), ("side_mask", 0)]:
         h.set_option(name, val)
