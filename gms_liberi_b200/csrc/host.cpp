@@ -231,8 +231,8 @@ struct liberi_handle_s {
     unsigned long long *d_maxd = nullptr;
     cudaStream_t stream = nullptr;
     // mixed builds run their FP64 task lists on a second stream beside the
-    // FP32 lists, FP64 builds the classes (dd|dd) and (dd|pd) (forked from and
-    // joined back into the build's stream)
+    // FP32 lists, FP64 builds the classes of side_mask (forked from and joined
+    // back into the build's stream)
     bool overlap = true;
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
@@ -959,10 +959,10 @@ static int build_on_device(liberi_handle h, const double *dD, double *dF, cudaSt
     // the side stream beside the FP32 lists on the build's stream.  Measured
     // on C60: 1.5 ms faster at cut 1e-2 than running them in turn, where
     // putting the high-L classes on the side instead gained 1 ms; FP64
-    // builds put only (dd|dd) and (dd|pd) there, two classes of few long
-    // CTAs at low occupancy (0.8 ms faster; more classes on the side crowd
-    // the large ones: the seven high-L classes cost 5 ms).  The task splits
-    // of every class come first; per-class timing keeps one stream.
+    // builds put the classes of side_mask there (the small low-occupancy
+    // classes and the seven Rys classes, measured against the kernel shapes
+    // of this build).  The task splits of every class come first; per-class
+    // timing keeps one stream.
     // Small builds (few quartets) are a sequence of class kernels each as long
     // as its costliest quartet's primitive loop: their classes are spread over
     // FAN_STREAMS streams instead (measured: 42 functions 2.9 -> 1.0 ms, 366
